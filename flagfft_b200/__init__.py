@@ -1,0 +1,236 @@
+"""flagfft_b200 -- Python binding of libflagfft.so, the sm_100a FFT engine behind
+the flagfft.h C ABI.
+
+The binding mirrors the C API one to one (``plan1d`` / ``plan2d`` / ``plan3d`` /
+``plan_many`` -> ``flagfftPlan*``, ``Plan.exec_*`` -> ``flagfftExec*``,
+``Plan.set_stream`` / ``Plan.destroy`` / ``Plan.description``), takes device
+pointers as integers or CUDA torch tensors, and raises ``FlagFFTError`` with the
+C status code on any non-success result.  There is no fallback: if the shared
+library is missing the import fails.
+"""
+from __future__ import annotations
+
+import ctypes
+import json
+import os
+from pathlib import Path
+
+__all__ = [
+    "FlagFFTError", "Plan", "plan1d", "plan2d", "plan3d", "plan_many", "planner_tree", "library_path",
+    "C2C", "Z2Z", "R2C", "D2Z", "C2R", "Z2D", "FORWARD", "INVERSE", "STATUS",
+]
+
+_PKG = Path(__file__).resolve().parent
+_LIB_PATH = Path(os.environ.get("FLAGFFT_B200_LIB", _PKG / "libflagfft.so"))
+
+C2C, Z2Z, R2C, D2Z, C2R, Z2D = 0x29, 0x69, 0x2A, 0x6A, 0x2C, 0x6C
+FORWARD, INVERSE = -1, 1
+STATUS = {
+    0: "FLAGFFT_SUCCESS", 1: "FLAGFFT_INVALID_PLAN", 2: "FLAGFFT_ALLOC_FAILED", 3: "FLAGFFT_INVALID_TYPE",
+    4: "FLAGFFT_INVALID_VALUE", 5: "FLAGFFT_INTERNAL_ERROR", 6: "FLAGFFT_EXEC_FAILED", 7: "FLAGFFT_SETUP_FAILED",
+    8: "FLAGFFT_INVALID_SIZE", 9: "FLAGFFT_UNALIGNED_DATA", 10: "FLAGFFT_INCOMPLETE_PARAMETER_LIST",
+    11: "FLAGFFT_INVALID_DEVICE", 12: "FLAGFFT_PARSE_ERROR", 13: "FLAGFFT_NO_WORKSPACE", 14: "FLAGFFT_NOT_SUPPORTED",
+}
+TYPE_NAMES = {C2C: "C2C", Z2Z: "Z2Z", R2C: "R2C", D2Z: "D2Z", C2R: "C2R", Z2D: "Z2D"}
+
+
+class FlagFFTError(RuntimeError):
+    def __init__(self, code: int, what: str):
+        self.code = code
+        super().__init__(f"{what}: {STATUS.get(code, code)}")
+
+
+def library_path() -> Path:
+    return _LIB_PATH
+
+
+def _load():
+    if not _LIB_PATH.exists():
+        raise ImportError(f"libflagfft.so not built at {_LIB_PATH}; run `python -m flagfft_b200.build`")
+    lib = ctypes.CDLL(str(_LIB_PATH))
+    H = ctypes.c_void_p
+    PH = ctypes.POINTER(ctypes.c_void_p)
+    i, vp, cp = ctypes.c_int, ctypes.c_void_p, ctypes.c_char_p
+    ip = ctypes.POINTER(ctypes.c_int)
+    sigs = {
+        "flagfftPlan1d": (i, [PH, i, i, i]),
+        "flagfftPlan2d": (i, [PH, i, i, i]),
+        "flagfftPlan3d": (i, [PH, i, i, i, i]),
+        "flagfftPlanMany": (i, [PH, i, ip, ip, i, i, ip, i, i, i, i]),
+        "flagfftExecC2C": (i, [H, vp, vp, i]),
+        "flagfftExecZ2Z": (i, [H, vp, vp, i]),
+        "flagfftExecR2C": (i, [H, vp, vp]),
+        "flagfftExecD2Z": (i, [H, vp, vp]),
+        "flagfftExecC2R": (i, [H, vp, vp]),
+        "flagfftExecZ2D": (i, [H, vp, vp]),
+        "flagfftSetStream": (i, [H, vp]),
+        "flagfftDestroy": (i, [H]),
+        "flagfftGetPlanDescription": (cp, [H]),
+        "flagfftB200Version": (cp, []),
+        "flagfftB200PlannerTree": (i, [i, i, ctypes.c_longlong, cp, i]),
+        "flagfftB200PlanJson": (cp, [H]),
+        "flagfftB200LaunchCount": (i, [H, i]),
+    }
+    for name, (res, args) in sigs.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+LIB = _load()
+
+
+def _check(code: int, what: str) -> None:
+    if code != 0:
+        raise FlagFFTError(code, what)
+
+
+def _ptr(x) -> int:
+    """Device address of a CUDA tensor, or an integer address as given."""
+    if x is None:
+        return 0
+    if isinstance(x, int):
+        return x
+    if hasattr(x, "data_ptr"):
+        if hasattr(x, "is_cuda") and not x.is_cuda:
+            raise ValueError("flagfft_b200 executes on device memory; got a host tensor")
+        return x.data_ptr()
+    raise TypeError(f"cannot take a device pointer of {type(x).__name__}")
+
+
+def _stream_handle(stream) -> int:
+    if stream is None:
+        return 0
+    if isinstance(stream, int):
+        return stream
+    return int(getattr(stream, "cuda_stream", stream))
+
+
+class Plan:
+    """A flagfftHandle.  Destroyed explicitly with destroy() or on garbage collection."""
+
+    def __init__(self, handle: int, ftype: int, shape: tuple[int, ...], batch: int):
+        self._h = ctypes.c_void_p(handle)
+        self.type = ftype
+        self.shape = shape
+        self.batch = batch
+
+    @property
+    def handle(self) -> int:
+        return self._h.value or 0
+
+    def _exec(self, fn: str, idata, odata, *extra) -> None:
+        _check(getattr(LIB, fn)(self._h, ctypes.c_void_p(_ptr(idata)), ctypes.c_void_p(_ptr(odata)), *extra), fn)
+
+    def exec_c2c(self, idata, odata, direction: int) -> None:
+        self._exec("flagfftExecC2C", idata, odata, direction)
+
+    def exec_z2z(self, idata, odata, direction: int) -> None:
+        self._exec("flagfftExecZ2Z", idata, odata, direction)
+
+    def exec_r2c(self, idata, odata) -> None:
+        self._exec("flagfftExecR2C", idata, odata)
+
+    def exec_d2z(self, idata, odata) -> None:
+        self._exec("flagfftExecD2Z", idata, odata)
+
+    def exec_c2r(self, idata, odata) -> None:
+        self._exec("flagfftExecC2R", idata, odata)
+
+    def exec_z2d(self, idata, odata) -> None:
+        self._exec("flagfftExecZ2D", idata, odata)
+
+    def execute(self, idata, odata, direction: int = FORWARD) -> None:
+        """Dispatch on the plan's type (direction only matters for C2C / Z2Z)."""
+        t = self.type
+        if t == C2C:
+            self.exec_c2c(idata, odata, direction)
+        elif t == Z2Z:
+            self.exec_z2z(idata, odata, direction)
+        elif t == R2C:
+            self.exec_r2c(idata, odata)
+        elif t == D2Z:
+            self.exec_d2z(idata, odata)
+        elif t == C2R:
+            self.exec_c2r(idata, odata)
+        else:
+            self.exec_z2d(idata, odata)
+
+    def set_stream(self, stream) -> None:
+        _check(LIB.flagfftSetStream(self._h, ctypes.c_void_p(_stream_handle(stream))), "flagfftSetStream")
+
+    def description(self) -> str:
+        s = LIB.flagfftGetPlanDescription(self._h)
+        if s is None:
+            raise FlagFFTError(1, "flagfftGetPlanDescription")
+        return s.decode()
+
+    def tree(self) -> dict:
+        s = LIB.flagfftB200PlanJson(self._h)
+        if s is None:
+            raise FlagFFTError(1, "flagfftB200PlanJson")
+        return json.loads(s.decode())
+
+    def launch_count(self, direction: int = FORWARD) -> int:
+        return int(LIB.flagfftB200LaunchCount(self._h, direction))
+
+    def destroy(self) -> None:
+        if self._h.value:
+            _check(LIB.flagfftDestroy(self._h), "flagfftDestroy")
+            self._h = ctypes.c_void_p(0)
+
+    def __del__(self):
+        try:
+            if self._h.value:
+                LIB.flagfftDestroy(self._h)
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.destroy()
+
+
+def plan1d(nx: int, ftype: int, batch: int = 1) -> Plan:
+    h = ctypes.c_void_p(0)
+    _check(LIB.flagfftPlan1d(ctypes.byref(h), nx, ftype, batch), "flagfftPlan1d")
+    return Plan(h.value, ftype, (nx,), batch)
+
+
+def plan2d(nx: int, ny: int, ftype: int) -> Plan:
+    h = ctypes.c_void_p(0)
+    _check(LIB.flagfftPlan2d(ctypes.byref(h), nx, ny, ftype), "flagfftPlan2d")
+    return Plan(h.value, ftype, (nx, ny), 1)
+
+
+def plan3d(nx: int, ny: int, nz: int, ftype: int) -> Plan:
+    h = ctypes.c_void_p(0)
+    _check(LIB.flagfftPlan3d(ctypes.byref(h), nx, ny, nz, ftype), "flagfftPlan3d")
+    return Plan(h.value, ftype, (nx, ny, nz), 1)
+
+
+def plan_many(n, inembed, istride: int, idist: int, onembed, ostride: int, odist: int, ftype: int,
+              batch: int) -> Plan:
+    rank = len(n)
+    arr = lambda v: None if v is None else (ctypes.c_int * rank)(*v)  # noqa: E731
+    h = ctypes.c_void_p(0)
+    _check(LIB.flagfftPlanMany(ctypes.byref(h), rank, arr(n), arr(inembed), istride, idist, arr(onembed), ostride,
+                               odist, ftype, batch), "flagfftPlanMany")
+    return Plan(h.value, ftype, tuple(n), batch)
+
+
+def planner_tree(n: int, is_double: bool = False, smem_bytes: int = 0) -> dict:
+    """Plan tree for a 1-D complex length, host only (no GPU)."""
+    need = LIB.flagfftB200PlannerTree(n, int(is_double), smem_bytes, None, 0)
+    if need < 0:
+        raise FlagFFTError(4, f"planner rejected length {n}")
+    buf = ctypes.create_string_buffer(need + 1)
+    LIB.flagfftB200PlannerTree(n, int(is_double), smem_bytes, buf, need + 1)
+    return json.loads(buf.value.decode())
+
+
+def version() -> str:
+    return LIB.flagfftB200Version().decode()

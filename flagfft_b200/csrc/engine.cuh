@@ -1,0 +1,428 @@
+// On-chip FFT engine for sm_100a: complex arithmetic, radix codelets, in-place
+// mixed-radix decimation stages over a shared-memory buffer.
+//
+// Design (B200-first, not a port of the reference's Triton leaf):
+//  * One transform of length L lives in one CTA's shared memory (up to 227 KB:
+//    29056 complex64 / 14528 complex128 points).  Stages run in place; each
+//    butterfly reads and writes the same R positions, so a stage needs no
+//    second buffer and a thread holds only one butterfly (R <= 19 values) in
+//    registers at a time -- any L that fits in shared memory runs at any
+//    thread count.
+//  * DIT stages consume a digit-reversed buffer and leave natural order; DIF
+//    stages consume natural order and leave it digit-reversed.  A DIF pass with
+//    radices (R0..Rk) followed by a DIT pass with the radices reversed needs no
+//    reordering in between: Bluestein and Rader convolutions multiply in that
+//    permuted order with a pre-permuted kernel spectrum.
+//  * Shared-memory positions are XOR-swizzled inside aligned 16-element
+//    (complex64) / 8-element (complex128) groups so the stride-R accesses of
+//    the early stages and the digit-reversed loads spread over the banks.
+//  * Twiddles W_L^m come from a per-length table built on the host in FP64 and
+//    rounded once (the reference also builds its stage twiddles in double and
+//    casts, src/codegen/tables.cpp:39-69); the inverse direction conjugates.
+//  * Codelets are the forward DFT; the inverse is conj(DFT(conj x)), the same
+//    convention the reference's codelets use (python/flagfft_codegen/kernels.py:493-512).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+// Every engine function is host+device: the host build runs the same code
+// sequentially (one "thread", barriers as no-ops) to check index arithmetic
+// without a GPU.
+#define FFB_HD __host__ __device__ __forceinline__
+
+namespace ffb {
+
+#include "roots.inc"
+
+template <typename T>
+struct alignas(2 * sizeof(T)) cpx {
+  T x, y;
+};
+
+template <typename T>
+FFB_HD cpx<T> mk(T x, T y) {
+  cpx<T> r;
+  r.x = x;
+  r.y = y;
+  return r;
+}
+template <typename T>
+FFB_HD cpx<T> operator+(cpx<T> a, cpx<T> b) { return mk(a.x + b.x, a.y + b.y); }
+template <typename T>
+FFB_HD cpx<T> operator-(cpx<T> a, cpx<T> b) { return mk(a.x - b.x, a.y - b.y); }
+template <typename T>
+FFB_HD cpx<T> cmul(cpx<T> a, cpx<T> b) {
+  return mk(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+template <typename T>
+FFB_HD cpx<T> cscale(cpx<T> a, T s) { return mk(a.x * s, a.y * s); }
+template <typename T>
+FFB_HD cpx<T> conjg(cpx<T> a) { return mk(a.x, -a.y); }
+// multiply by -i
+template <typename T>
+FFB_HD cpx<T> mul_mi(cpx<T> a) { return mk(a.y, -a.x); }
+
+// ---------------------------------------------------------------------------
+// Division by a runtime divisor d (1 <= d < 2^31) for dividends n < 2^31
+// (Granlund-Montgomery): l = ceil(log2 d), m = floor(2^32 (2^l - d) / d) + 1,
+// n / d == (umulhi(n, m) + n) >> l.  n < 2^31 keeps the sum below 2^32.
+// ---------------------------------------------------------------------------
+struct FastDiv {
+  uint32_t d, m, s;
+};
+
+inline FastDiv make_fastdiv(uint32_t d) {
+  FastDiv f;
+  f.d = d;
+  uint32_t l = 0;
+  while ((1ull << l) < d) ++l;
+  f.s = l;
+  f.m = (uint32_t)(((1ull << 32) * ((1ull << l) - d)) / d + 1);
+  return f;
+}
+
+FFB_HD uint32_t fdiv(uint32_t n, const FastDiv &f) {
+#ifdef __CUDA_ARCH__
+  return (__umulhi(n, f.m) + n) >> f.s;
+#else
+  return (uint32_t)((((uint64_t)n * f.m >> 32) + n) >> f.s);
+#endif
+}
+
+// ---------------------------------------------------------------------------
+// Codelets: forward DFT of R values held in registers, natural order in/out.
+// ---------------------------------------------------------------------------
+
+// Multiply by the compile-time root W_R^m = exp(-2*pi*i*m/R), skipping the
+// trivial ones.
+template <int R, typename T>
+FFB_HD cpx<T> twiddle_const(cpx<T> a, int m) {
+  m %= R;
+  if (m == 0) return a;
+  if (2 * m == R) return mk(-a.x, -a.y);
+  if (4 * m == R) return mul_mi(a);
+  if (4 * m == 3 * R) return mk(-a.y, a.x);
+  const T c = (T)RootTable<R>::c(m);
+  const T s = (T)RootTable<R>::s(m);
+  // exp(-i theta) = c - i s;  45-degree multiples need two multiplies
+  if (RootTable<R>::c(m) == RootTable<R>::s(m)) return mk(c * (a.x + a.y), c * (a.y - a.x));
+  if (RootTable<R>::c(m) == -RootTable<R>::s(m)) return mk(c * (a.x - a.y), c * (a.y + a.x));
+  return mk(a.x * c + a.y * s, a.y * c - a.x * s);
+}
+
+template <int R, typename T>
+struct Dft;
+
+template <typename T>
+struct Dft<1, T> {
+  static FFB_HD void run(cpx<T> *) {}
+};
+
+template <typename T>
+struct Dft<2, T> {
+  static FFB_HD void run(cpx<T> *v) {
+    cpx<T> a = v[0], b = v[1];
+    v[0] = a + b;
+    v[1] = a - b;
+  }
+};
+
+template <typename T>
+struct Dft<3, T> {
+  static FFB_HD void run(cpx<T> *v) {
+    const T c = (T)-0.5, s = (T)0.86602540378443864676;
+    cpx<T> t1 = v[1] + v[2], t2 = v[1] - v[2];
+    cpx<T> y0 = v[0] + t1;
+    cpx<T> m1 = mk(v[0].x + c * t1.x, v[0].y + c * t1.y);
+    // -i * s * t2
+    cpx<T> m2 = mk(s * t2.y, -s * t2.x);
+    v[0] = y0;
+    v[1] = m1 + m2;
+    v[2] = m1 - m2;
+  }
+};
+
+template <typename T>
+struct Dft<4, T> {
+  static FFB_HD void run(cpx<T> *v) {
+    cpx<T> a = v[0] + v[2], b = v[0] - v[2];
+    cpx<T> c = v[1] + v[3], d = mul_mi(v[1] - v[3]);
+    v[0] = a + c;
+    v[2] = a - c;
+    v[1] = b + d;
+    v[3] = b - d;
+  }
+};
+
+// Odd prime P: pair n with P-n.  y_k = x0 + sum_n a_n cos(2 pi n k/P)
+//                                  - i sum_n b_n sin(2 pi n k/P),
+// a_n = x_n + x_{P-n}, b_n = x_n - x_{P-n}; y_{P-k} flips the sine term.
+template <int P, typename T>
+struct DftPrime {
+  static FFB_HD void run(cpx<T> *v) {
+    constexpr int H = (P - 1) / 2;
+    cpx<T> a[H], b[H];
+#pragma unroll
+    for (int n = 1; n <= H; ++n) {
+      a[n - 1] = v[n] + v[P - n];
+      b[n - 1] = v[n] - v[P - n];
+    }
+    const cpx<T> x0 = v[0];
+    cpx<T> sum = x0;
+#pragma unroll
+    for (int n = 0; n < H; ++n) sum = sum + a[n];
+    v[0] = sum;
+#pragma unroll
+    for (int k = 1; k <= H; ++k) {
+      cpx<T> A = x0, B = mk((T)0, (T)0);
+#pragma unroll
+      for (int n = 1; n <= H; ++n) {
+        const int m = (n * k) % P;
+        const T c = (T)RootTable<P>::c(m);
+        const T s = (T)RootTable<P>::s(m);
+        A.x += a[n - 1].x * c;
+        A.y += a[n - 1].y * c;
+        B.x += b[n - 1].x * s;
+        B.y += b[n - 1].y * s;
+      }
+      // -i*B = (B.y, -B.x)
+      v[k] = mk(A.x + B.y, A.y - B.x);
+      v[P - k] = mk(A.x - B.y, A.y + B.x);
+    }
+  }
+};
+
+template <typename T> struct Dft<5, T> : DftPrime<5, T> {};
+template <typename T> struct Dft<7, T> : DftPrime<7, T> {};
+template <typename T> struct Dft<11, T> : DftPrime<11, T> {};
+template <typename T> struct Dft<13, T> : DftPrime<13, T> {};
+template <typename T> struct Dft<17, T> : DftPrime<17, T> {};
+template <typename T> struct Dft<19, T> : DftPrime<19, T> {};
+
+// Composite R = R1 * R2 (Cooley-Tukey inside the codelet):
+// X[k1 + R1 k2] = sum_n2 W_R2^{n2 k2} W_R^{n2 k1} sum_n1 x[R2 n1 + n2] W_R1^{n1 k1}
+template <int R1, int R2, typename T>
+struct DftSplit {
+  static FFB_HD void run(cpx<T> *v) {
+    constexpr int R = R1 * R2;
+    cpx<T> u[R];
+#pragma unroll
+    for (int n2 = 0; n2 < R2; ++n2) {
+      cpx<T> t[R1];
+#pragma unroll
+      for (int n1 = 0; n1 < R1; ++n1) t[n1] = v[R2 * n1 + n2];
+      Dft<R1, T>::run(t);
+#pragma unroll
+      for (int k1 = 0; k1 < R1; ++k1) u[n2 * R1 + k1] = twiddle_const<R, T>(t[k1], n2 * k1);
+    }
+#pragma unroll
+    for (int k1 = 0; k1 < R1; ++k1) {
+      cpx<T> t[R2];
+#pragma unroll
+      for (int n2 = 0; n2 < R2; ++n2) t[n2] = u[n2 * R1 + k1];
+      Dft<R2, T>::run(t);
+#pragma unroll
+      for (int k2 = 0; k2 < R2; ++k2) v[k1 + R1 * k2] = t[k2];
+    }
+  }
+};
+
+template <typename T> struct Dft<6, T> : DftSplit<2, 3, T> {};
+template <typename T> struct Dft<8, T> : DftSplit<2, 4, T> {};
+template <typename T> struct Dft<9, T> : DftSplit<3, 3, T> {};
+template <typename T> struct Dft<10, T> : DftSplit<2, 5, T> {};
+template <typename T> struct Dft<12, T> : DftSplit<4, 3, T> {};
+template <typename T> struct Dft<15, T> : DftSplit<3, 5, T> {};
+template <typename T> struct Dft<16, T> : DftSplit<4, 4, T> {};
+
+template <int R, typename T>
+FFB_HD void dft_dir(cpx<T> *v, bool inv) {
+  if (inv) {
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r].y = -v[r].y;
+  }
+  Dft<R, T>::run(v);
+  if (inv) {
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r].y = -v[r].y;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Shared-memory layout
+// ---------------------------------------------------------------------------
+
+// Swizzle inside aligned groups of G = 128 bytes / sizeof(cpx<T>) elements.
+template <typename T>
+struct Swz {
+  static constexpr int G = 128 / (2 * (int)sizeof(T));  // 16 (c64) or 8 (c128)
+  static constexpr int B = G == 16 ? 4 : 3;
+  static FFB_HD int phys(int p) { return p ^ (((p >> B) ^ (p >> (2 * B))) & (G - 1)); }
+  static FFB_HD int padded(int L) { return (L + G - 1) / G * G; }
+};
+
+constexpr int kMaxStages = 16;
+
+// One on-chip transform of length L as a sequence of radix stages.
+//   DIT stage s:  span[s] = R0*...*R(s-1)       (sub-transform length before it)
+//                 tws[s]  = L / (span[s]*R(s))  (twiddle index stride)
+//   DIF stage s:  span[s] = L / (R0*...*R(s-1)) (sub-length it splits)
+//                 tws[s]  = L / span[s]
+//   sdiv[s] divides the butterfly index by the inner block length
+//   (DIT: span[s]; DIF: span[s]/R(s)).
+//   rdiv[s] divides by R(s) (digit reversal).
+struct Core {
+  int L;
+  int nst;
+  int radix[kMaxStages];
+  int span[kMaxStages];
+  int tws[kMaxStages];
+  FastDiv sdiv[kMaxStages];
+  FastDiv rdiv[kMaxStages];
+};
+
+// Position of input element i for a DIT pass over `c` (digit reversal):
+// i = sum_s d_s * L/(R0..Rs)  ->  p = sum_s d_s * (R0..R(s-1)).
+FFB_HD int dit_position(int i, const Core &c) {
+  int p = 0;
+  int rem = i;
+  for (int s = c.nst - 1; s >= 0; --s) {
+    int q = (int)fdiv((uint32_t)rem, c.rdiv[s]);
+    int d = rem - q * c.radix[s];
+    rem = q;
+    p += d * c.span[s];
+  }
+  return p;
+}
+
+FFB_HD cpx<float> ldg_c(const cpx<float> *p) {
+#ifdef __CUDA_ARCH__
+  float2 v = __ldg(reinterpret_cast<const float2 *>(p));
+  return mk(v.x, v.y);
+#else
+  return *p;
+#endif
+}
+FFB_HD cpx<double> ldg_c(const cpx<double> *p) {
+#ifdef __CUDA_ARCH__
+  double2 v = __ldg(reinterpret_cast<const double2 *>(p));
+  return mk(v.x, v.y);
+#else
+  return *p;
+#endif
+}
+template <typename V>
+FFB_HD V ldg_v(const V *p) {
+#ifdef __CUDA_ARCH__
+  return __ldg(p);
+#else
+  return *p;
+#endif
+}
+
+// Twiddle W_L^{m} (forward) or its conjugate (inverse) from the length-L table.
+template <typename T>
+FFB_HD cpx<T> twiddle(const cpx<T> *__restrict__ tw, int m, bool inv) {
+  cpx<T> w = ldg_c(tw + m);
+  if (inv) w.y = -w.y;
+  return w;
+}
+
+// In-place DIT stage s: combine R sub-transforms of length Ls.
+template <int R, typename T>
+FFB_HD void dit_stage_r(cpx<T> *buf, const Core &c, int s, int tid, int nthr,
+                                            const cpx<T> *__restrict__ tw, bool inv) {
+  const int Ls = c.span[s];
+  const int tws = c.tws[s];
+  const int nb = c.L / R;
+  for (int u = tid; u < nb; u += nthr) {
+    const int b = (int)fdiv((uint32_t)u, c.sdiv[s]);
+    const int j = u - b * Ls;
+    const int base = b * Ls * R + j;
+    cpx<T> v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r] = buf[Swz<T>::phys(base + r * Ls)];
+    if (j != 0) {
+#pragma unroll
+      for (int r = 1; r < R; ++r) v[r] = cmul(v[r], twiddle(tw, r * j * tws, inv));
+    }
+    dft_dir<R, T>(v, inv);
+#pragma unroll
+    for (int q = 0; q < R; ++q) buf[Swz<T>::phys(base + q * Ls)] = v[q];
+  }
+}
+
+// In-place DIF stage s: split sub-transforms of length Ms into R interleaved
+// parts; outputs are multiplied by W_Ms^{q j} after the butterfly.
+template <int R, typename T>
+FFB_HD void dif_stage_r(cpx<T> *buf, const Core &c, int s, int tid, int nthr,
+                                            const cpx<T> *__restrict__ tw, bool inv) {
+  const int Ms = c.span[s];
+  const int stride = Ms / R;
+  const int tws = c.tws[s];
+  const int nb = c.L / R;
+  for (int u = tid; u < nb; u += nthr) {
+    const int b = (int)fdiv((uint32_t)u, c.sdiv[s]);
+    const int j = u - b * stride;
+    const int base = b * Ms + j;
+    cpx<T> v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r] = buf[Swz<T>::phys(base + r * stride)];
+    dft_dir<R, T>(v, inv);
+    if (j != 0) {
+#pragma unroll
+      for (int q = 1; q < R; ++q) v[q] = cmul(v[q], twiddle(tw, q * j * tws, inv));
+    }
+#pragma unroll
+    for (int q = 0; q < R; ++q) buf[Swz<T>::phys(base + q * stride)] = v[q];
+  }
+}
+
+#define FFB_RADIX_SWITCH(R_, CALL)                                     \
+  switch (R_) {                                                        \
+    case 2: CALL(2); break;                                            \
+    case 3: CALL(3); break;                                            \
+    case 4: CALL(4); break;                                            \
+    case 5: CALL(5); break;                                            \
+    case 6: CALL(6); break;                                            \
+    case 7: CALL(7); break;                                            \
+    case 8: CALL(8); break;                                            \
+    case 9: CALL(9); break;                                            \
+    case 10: CALL(10); break;                                          \
+    case 11: CALL(11); break;                                          \
+    case 12: CALL(12); break;                                          \
+    case 13: CALL(13); break;                                          \
+    case 15: CALL(15); break;                                          \
+    case 16: CALL(16); break;                                          \
+    case 17: CALL(17); break;                                          \
+    case 19: CALL(19); break;                                          \
+    default: break;                                                    \
+  }
+
+// All DIT stages (digit-reversed in, natural out).  Every thread of the
+// group calls this; `sync` is the barrier that covers the group's threads.
+template <typename T, typename Sync>
+FFB_HD void run_dit(cpx<T> *buf, const Core &c, int tid, int nthr,
+                                        const cpx<T> *__restrict__ tw, bool inv, Sync sync) {
+  for (int s = 0; s < c.nst; ++s) {
+#define FFB_DIT_CALL(R) dit_stage_r<R, T>(buf, c, s, tid, nthr, tw, inv)
+    FFB_RADIX_SWITCH(c.radix[s], FFB_DIT_CALL)
+#undef FFB_DIT_CALL
+    sync();
+  }
+}
+
+// All DIF stages (natural in, digit-reversed out).
+template <typename T, typename Sync>
+FFB_HD void run_dif(cpx<T> *buf, const Core &c, int tid, int nthr,
+                                        const cpx<T> *__restrict__ tw, bool inv, Sync sync) {
+  for (int s = 0; s < c.nst; ++s) {
+#define FFB_DIF_CALL(R) dif_stage_r<R, T>(buf, c, s, tid, nthr, tw, inv)
+    FFB_RADIX_SWITCH(c.radix[s], FFB_DIF_CALL)
+#undef FFB_DIF_CALL
+    sync();
+  }
+}
+
+}  // namespace ffb

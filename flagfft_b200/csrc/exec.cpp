@@ -1,0 +1,551 @@
+// Lowering of plan trees onto on-chip FFT passes.
+//
+// Node -> pass mapping (reference node shapes from src/exec/raw_nodes.cpp):
+//   leaf, or a four-step whose children flatten into radix lists, when the
+//   whole length fits one CTA              -> one pass (DIT core)
+//   Bluestein / Rader whose convolution fits one CTA
+//                                          -> one fused pass (chirp or
+//                                             permutation, forward FFT,
+//                                             kernel product, inverse FFT,
+//                                             unchirp / unpermute)
+//   four-step whose children each fit      -> two passes through a workspace:
+//                                             column FFTs with the W_N^{j2 k1}
+//                                             twiddle fused into their store,
+//                                             then row FFTs
+//   R2C / C2R of even n                    -> the n/2-point complex core with
+//                                             the pack / unpack fused into its
+//                                             load and store
+//   2-D RTRT                               -> a row pass and an in-place
+//                                             column-tile pass (no transposes)
+#include "exec.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <sstream>
+#include <stdexcept>
+
+#include "tables.hpp"
+
+namespace ffb {
+
+#ifndef FFB_HOST_EMULATION
+DevMem::DevMem(size_t n) : bytes(n) {
+  if (n == 0) return;
+  cudaError_t e = cudaMalloc(&ptr, n);
+  if (e != cudaSuccess) {
+    ptr = nullptr;
+    cudaGetLastError();
+    throw std::bad_alloc();
+  }
+}
+
+DevMem::~DevMem() {
+  if (ptr) cudaFree(ptr);
+}
+
+DevPtr upload(const void *host, size_t bytes) {
+  auto m = std::make_shared<DevMem>(bytes);
+  if (bytes && cudaMemcpy(m->ptr, host, bytes, cudaMemcpyHostToDevice) != cudaSuccess) {
+    cudaGetLastError();
+    throw std::runtime_error("table upload failed");
+  }
+  return m;
+}
+#else
+// Host-emulation build: "device" memory is host memory.
+DevMem::DevMem(size_t n) : bytes(n) {
+  if (n == 0) return;
+  ptr = std::malloc(n);
+  if (!ptr) throw std::bad_alloc();
+}
+
+DevMem::~DevMem() { std::free(ptr); }
+
+DevPtr upload(const void *host, size_t bytes) {
+  auto m = std::make_shared<DevMem>(bytes);
+  if (bytes) std::memcpy(m->ptr, host, bytes);
+  return m;
+}
+#endif
+
+cudaError_t Program::run(const void *in, void *out, cudaStream_t st) const {
+  void *s0 = scratch0 ? scratch0->ptr : nullptr;
+  void *s1 = scratch1 ? scratch1->ptr : nullptr;
+  for (const auto &p : passes) {
+    cudaError_t e = p->run(in, out, s0, s1, st);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+std::string Program::describe() const {
+  std::ostringstream o;
+  for (size_t i = 0; i < passes.size(); ++i) o << (i ? "\n" : "") << "  pass " << i << ": " << passes[i]->describe();
+  return o.str();
+}
+
+int Program::launches() const {
+  int n = 0;
+  for (const auto &p : passes) n += p->launches();
+  return n;
+}
+
+int64_t max_onchip_length(bool is_double) {
+  // (padded(L) + one spare group) complex elements within the 227 KB opt-in limit
+  const int64_t limit = 232448;
+  const int64_t elem = is_double ? 16 : 8;
+  const int64_t g = is_double ? 8 : 16;
+  return (limit / elem - g) / g * g;
+}
+
+namespace {
+
+const char *buf_name(Buf b) {
+  switch (b) {
+    case Buf::In: return "in";
+    case Buf::Out: return "out";
+    case Buf::Scratch0: return "ws0";
+    case Buf::Scratch1: return "ws1";
+  }
+  return "?";
+}
+
+const char *kind_name(CoreKind k) {
+  switch (k) {
+    case CoreKind::Dit: return "stockham-dit";
+    case CoreKind::Bluestein: return "bluestein-fused";
+    case CoreKind::Rader: return "rader-fused";
+  }
+  return "?";
+}
+
+const char *io_name(IoKind k) {
+  switch (k) {
+    case IoKind::C2C: return "c2c";
+    case IoKind::R2C: return "r2c-halfpack";
+    case IoKind::C2R: return "c2r-halfpack";
+    case IoKind::R2CFull: return "r2c-full";
+    case IoKind::C2RFull: return "c2r-full";
+  }
+  return "?";
+}
+
+template <typename T>
+struct TilePass final : PassBase {
+  TileArgs<T> a{};
+  CoreKind kind = CoreKind::Dit;
+  IoKind io = IoKind::C2C;
+  size_t smem = 0;
+  Buf src = Buf::In, dst = Buf::Out;
+  std::string note;
+
+  static void *pick(Buf b, const void *in, void *out, void *s0, void *s1) {
+    switch (b) {
+      case Buf::In: return const_cast<void *>(in);
+      case Buf::Out: return out;
+      case Buf::Scratch0: return s0;
+      case Buf::Scratch1: return s1;
+    }
+    return nullptr;
+  }
+
+  cudaError_t run(const void *in, void *out, void *s0, void *s1, cudaStream_t st) const override {
+    TileArgs<T> b = a;
+    b.in = pick(src, in, out, s0, s1);
+    b.out = pick(dst, in, out, s0, s1);
+    return launch_tile<T>(b, kind, io, smem, st);
+  }
+
+  std::string describe() const override {
+    std::ostringstream o;
+    o << kind_name(kind) << "/" << io_name(io) << " " << (sizeof(T) == 4 ? "f32" : "f64") << " L=" << a.core.L
+      << " radices=[";
+    for (int s = 0; s < a.core.nst; ++s) o << (s ? "," : "") << a.core.radix[s];
+    o << "] n=" << a.n << " transforms=" << a.nbatch << "x" << a.G << " per_cta=" << a.W
+      << " threads=" << a.W * a.tpt << " smem=" << smem << " " << buf_name(src) << "->" << buf_name(dst);
+    if (a.post_twiddle) o << " +twiddle";
+    if (!note.empty()) o << " (" << note << ")";
+    return o.str();
+  }
+};
+
+// What one CTA-resident transform needs.
+struct CoreSpec {
+  CoreKind kind = CoreKind::Dit;
+  int64_t n = 0;  // logical transform length
+  int64_t L = 0;  // buffer (core) length
+  std::vector<int> radices;
+  NodePtr node;
+};
+
+// Radix list of a node that runs as one chain of stages, or empty.
+static std::vector<int> flatten(const NodePtr &node) {
+  if (!node) return {};
+  if (node->kind == NodeKind::CtLeaf) {
+    std::vector<int> r;
+    for (int64_t f : node->factors) r.push_back((int)f);
+    return r;
+  }
+  if (node->kind == NodeKind::FourStep) {
+    auto a = flatten(node->row);
+    auto b = flatten(node->col);
+    if (a.empty() || b.empty()) return {};
+    a.insert(a.end(), b.begin(), b.end());
+    return a;
+  }
+  return {};
+}
+
+static Core make_dit_core(int64_t L, const std::vector<int> &r) {
+  if ((int)r.size() > kMaxStages) throw std::runtime_error("too many radix stages");
+  Core c{};
+  c.L = (int)L;
+  c.nst = (int)r.size();
+  int64_t span = 1;
+  for (size_t s = 0; s < r.size(); ++s) {
+    c.radix[s] = r[s];
+    c.span[s] = (int)span;
+    c.tws[s] = (int)(L / (span * r[s]));
+    c.sdiv[s] = make_fastdiv((uint32_t)span);
+    c.rdiv[s] = make_fastdiv((uint32_t)r[s]);
+    span *= r[s];
+  }
+  if (span != L) throw std::runtime_error("radices do not multiply to the core length");
+  return c;
+}
+
+static Core make_dif_core(int64_t L, const std::vector<int> &r) {
+  if ((int)r.size() > kMaxStages) throw std::runtime_error("too many radix stages");
+  Core c{};
+  c.L = (int)L;
+  c.nst = (int)r.size();
+  int64_t span = L;
+  for (size_t s = 0; s < r.size(); ++s) {
+    c.radix[s] = r[s];
+    c.span[s] = (int)span;
+    c.tws[s] = (int)(L / span);
+    c.sdiv[s] = make_fastdiv((uint32_t)(span / r[s]));
+    c.rdiv[s] = make_fastdiv((uint32_t)r[s]);
+    span /= r[s];
+  }
+  if (span != 1) throw std::runtime_error("radices do not multiply to the core length");
+  return c;
+}
+
+template <typename T>
+class Builder {
+ public:
+  Builder(Program &prog, Planner &planner) : prog_(prog), planner_(planner) {}
+
+  static constexpr int kMaxThreads = sizeof(T) == 4 ? 512 : 256;
+
+  // On-chip core for a complex transform node, if one exists.
+  bool core_for(const NodePtr &node, CoreSpec &spec) const {
+    const int64_t maxL = max_onchip_length(sizeof(T) == 8);
+    if (node->length == 1) {  // the half-length core of a 2-point real transform
+      spec = {CoreKind::Dit, 1, 1, {}, node};
+      return true;
+    }
+    auto r = flatten(node);
+    if (!r.empty() && node->length <= maxL) {
+      spec = {CoreKind::Dit, node->length, node->length, r, node};
+      return true;
+    }
+    if (node->kind == NodeKind::Bluestein) {
+      auto rc = flatten(node->child);
+      if (!rc.empty() && node->conv_length <= maxL) {
+        spec = {CoreKind::Bluestein, node->length, node->conv_length, rc, node};
+        return true;
+      }
+    }
+    if (node->kind == NodeKind::Rader) {
+      auto rc = flatten(node->child);
+      if (!rc.empty() && node->length - 1 <= maxL) {
+        spec = {CoreKind::Rader, node->length, node->length - 1, rc, node};
+        return true;
+      }
+    }
+    return false;
+  }
+
+  // Thread count per transform: one butterfly of the largest radix per thread.
+  static int choose_tpt(int64_t L, const std::vector<int> &r) {
+    if (r.empty()) return 1;
+    int rmax = *std::max_element(r.begin(), r.end());
+    int64_t t = (L + rmax - 1) / rmax;
+    if (t <= 32) {
+      int p = 1;
+      while (p < t) p <<= 1;
+      return p;
+    }
+    t = (t + 31) / 32 * 32;
+    return (int)std::min<int64_t>(t, kMaxThreads);
+  }
+
+  // Fill a tile pass for G transforms per outer batch.
+  TilePass<T> *add_pass(const CoreSpec &spec, IoKind io, bool inverse, int64_t nbatch, int64_t G, long long ib,
+                        long long ig, long long ii, long long ob, long long og, long long ok, Buf src, Buf dst,
+                        int64_t logical_n) {
+    auto p = std::make_unique<TilePass<T>>();
+    TileArgs<T> &a = p->a;
+    a = TileArgs<T>{};
+    a.nbatch = nbatch;
+    a.ib = ib;
+    a.ig = ig;
+    a.ii = ii;
+    a.ob = ob;
+    a.og = og;
+    a.ok = ok;
+    a.G = (int)G;
+    a.inv = inverse ? 1 : 0;
+    a.n = (int)logical_n;
+    const int64_t L = spec.L;
+    if (spec.kind == CoreKind::Dit) {
+      a.core = make_dit_core(L, spec.radices);
+    } else {
+      a.core = make_dif_core(L, spec.radices);
+      std::vector<int> rev(spec.radices.rbegin(), spec.radices.rend());
+      a.core2 = make_dit_core(L, rev);
+      fill_convolution(a, spec, inverse);
+    }
+    a.tw = table_tw(L);
+    // thread and tile shape
+    const bool strided = ig == 1 && ii != 1;
+    a.wfast = strided ? 1 : 0;
+    int tpt = choose_tpt(L, spec.radices);
+    const size_t per = tile_smem_per_transform<T>((int)L) + Swz<T>::G * sizeof(cpx<T>);
+    const size_t limit = 232448;
+    int64_t W;
+    if (strided) {
+      W = std::min<int64_t>({(int64_t)(limit / per), 8, G});
+    } else {
+      W = std::max<int64_t>(1, 256 / tpt);
+      W = std::min<int64_t>({W, (int64_t)(limit / per), G});
+      // keep at least ~2 CTAs per SM worth of work spread when the batch is small
+    }
+    W = std::max<int64_t>(W, 1);
+    if (W * tpt > kMaxThreads) tpt = std::max<int>(1, (int)(kMaxThreads / W));
+    a.W = (int)W;
+    a.tpt = tpt;
+    a.ldiv = make_fastdiv((uint32_t)L);
+    a.wdiv = make_fastdiv((uint32_t)W);
+    a.ndiv = make_fastdiv((uint32_t)std::max<int64_t>(1, logical_n));
+    a.hdiv = make_fastdiv((uint32_t)std::max<int64_t>(1, logical_n / 2));
+    p->kind = spec.kind;
+    p->io = io;
+    p->smem = per * (size_t)W;
+    p->src = src;
+    p->dst = dst;
+    TilePass<T> *raw = p.get();
+    prog_.passes.push_back(std::move(p));
+    return raw;
+  }
+
+  // W_L^m, m < L (forward sign).
+  const cpx<T> *table_tw(int64_t L) {
+    for (auto &e : tw_cache_)
+      if (e.first == L) return reinterpret_cast<const cpx<T> *>(e.second->ptr);
+    std::vector<cpx<T>> h((size_t)L);
+    for (int64_t m = 0; m < L; ++m) {
+      cld w = unit_root(m, L, -1);
+      h[(size_t)m] = mk((T)w.real(), (T)w.imag());
+    }
+    DevPtr d = upload(h.data(), h.size() * sizeof(cpx<T>));
+    prog_.owned.push_back(d);
+    tw_cache_.push_back({L, d});
+    return reinterpret_cast<const cpx<T> *>(d->ptr);
+  }
+
+  // Real-transform twiddles W_n^k, k <= n/2.
+  const cpx<T> *table_rtw(int64_t n) {
+    std::vector<cpx<T>> h((size_t)(n / 2 + 1));
+    for (int64_t k = 0; k <= n / 2; ++k) {
+      cld w = unit_root(k, n, -1);
+      h[(size_t)k] = mk((T)w.real(), (T)w.imag());
+    }
+    DevPtr d = upload(h.data(), h.size() * sizeof(cpx<T>));
+    prog_.owned.push_back(d);
+    return reinterpret_cast<const cpx<T> *>(d->ptr);
+  }
+
+  // Four-step post-twiddle W_N^m = hi[m / split] * lo[m % split].
+  void set_post_twiddle(TileArgs<T> &a, int64_t N) {
+    int64_t split = (int64_t)std::ceil(std::sqrt((double)N));
+    int64_t nhi = (N + split - 1) / split;
+    std::vector<cpx<T>> lo((size_t)split), hi((size_t)nhi);
+    for (int64_t m = 0; m < split; ++m) {
+      cld w = unit_root(m, N, -1);
+      lo[(size_t)m] = mk((T)w.real(), (T)w.imag());
+    }
+    for (int64_t m = 0; m < nhi; ++m) {
+      cld w = unit_root(m * split, N, -1);
+      hi[(size_t)m] = mk((T)w.real(), (T)w.imag());
+    }
+    DevPtr dl = upload(lo.data(), lo.size() * sizeof(cpx<T>));
+    DevPtr dh = upload(hi.data(), hi.size() * sizeof(cpx<T>));
+    prog_.owned.push_back(dl);
+    prog_.owned.push_back(dh);
+    a.post_twiddle = 1;
+    a.ptw_lo = reinterpret_cast<const cpx<T> *>(dl->ptr);
+    a.ptw_hi = reinterpret_cast<const cpx<T> *>(dh->ptr);
+    a.ptw_div = make_fastdiv((uint32_t)split);
+  }
+
+ private:
+  // Chirp, kernel spectrum and permutation tables of a Bluestein / Rader core.
+  void fill_convolution(TileArgs<T> &a, const CoreSpec &spec, bool inverse) {
+    const int sign = inverse ? 1 : -1;
+    const int64_t L = spec.L;
+    std::vector<cld> b((size_t)L, cld(0));
+    if (spec.kind == CoreKind::Bluestein) {
+      const int64_t n = spec.n;
+      std::vector<cpx<T>> ch((size_t)n);
+      for (int64_t k = 0; k < n; ++k) {
+        cld c = chirp_value(k, n, sign);
+        ch[(size_t)k] = mk((T)c.real(), (T)c.imag());
+        cld bc = chirp_value(k, n, -sign);
+        b[(size_t)k] = bc;
+        if (k) b[(size_t)(L - k)] = bc;
+      }
+      DevPtr d = upload(ch.data(), ch.size() * sizeof(cpx<T>));
+      prog_.owned.push_back(d);
+      a.chirp = reinterpret_cast<const cpx<T> *>(d->ptr);
+    } else {
+      const int64_t p = spec.n, m = p - 1;
+      const int64_t g = spec.node->root;
+      auto idx = rader_index_table(p, g);
+      // perm_in: q -> g^-q (m entries), then the log table k -> q (p entries)
+      std::vector<int> pin((size_t)(m + p), 0), pout((size_t)m);
+      for (int64_t q = 0; q < m; ++q) {
+        pin[(size_t)q] = (int)idx[(size_t)(q == 0 ? 0 : m - q)];
+        pout[(size_t)q] = (int)idx[(size_t)q];
+        pin[(size_t)(m + idx[(size_t)q])] = (int)q;
+      }
+      for (int64_t q = 0; q < m; ++q) b[(size_t)q] = unit_root(idx[(size_t)q], p, sign);
+      DevPtr di = upload(pin.data(), pin.size() * sizeof(int));
+      DevPtr dout = upload(pout.data(), pout.size() * sizeof(int));
+      prog_.owned.push_back(di);
+      prog_.owned.push_back(dout);
+      a.perm_in = reinterpret_cast<const int *>(di->ptr);
+      a.perm_out = reinterpret_cast<const int *>(dout->ptr);
+    }
+    host_fft(b, -1);
+    std::vector<cpx<T>> kern((size_t)L);
+    for (int64_t k = 0; k < L; ++k) {
+      cld v = b[(size_t)k] / (long double)L;
+      kern[(size_t)dif_position(k, spec.radices)] = mk((T)v.real(), (T)v.imag());
+    }
+    DevPtr dk = upload(kern.data(), kern.size() * sizeof(cpx<T>));
+    prog_.owned.push_back(dk);
+    a.kern = reinterpret_cast<const cpx<T> *>(dk->ptr);
+  }
+
+  Program &prog_;
+  Planner &planner_;
+  std::vector<std::pair<int64_t, DevPtr>> tw_cache_;
+};
+
+template <typename T>
+std::unique_ptr<Program> lower_t(const NodePtr &root, Planner &planner, Transform t, bool inverse, int64_t n,
+                                 const Layout &lay, bool in_place_real) {
+  auto prog = std::make_unique<Program>();
+  Builder<T> bld(*prog, planner);
+  CoreSpec spec;
+  const int64_t batch = lay.batch;
+
+  if (t == Transform::C2C) {
+    if (bld.core_for(root, spec)) {
+      bld.add_pass(spec, IoKind::C2C, inverse, 1, batch, 0, lay.idist, 1, 0, lay.odist, 1, Buf::In, Buf::Out, n);
+      return prog;
+    }
+    if (root->kind == NodeKind::FourStep) {
+      CoreSpec sa, sb;
+      if (bld.core_for(root->row, sa) && bld.core_for(root->col, sb)) {
+        const int64_t n1 = root->n1, n2 = root->n2;
+        if (batch > 65535) throw std::runtime_error("four-step batch above 65535");
+        prog->scratch0 = std::make_shared<DevMem>((size_t)(batch * n) * sizeof(cpx<T>));
+        // pass A: columns j2 (stride n2) of length n1, twiddle W_n^{j2 k1}, rows Y[j2][k1]
+        auto *pa = bld.add_pass(sa, IoKind::C2C, inverse, batch, n2, lay.idist, 1, n2, n, n1, 1, Buf::In,
+                                Buf::Scratch0, n1);
+        bld.set_post_twiddle(pa->a, n);
+        // pass B: for each k1, length n2 over Y[j2][k1] -> X[k1 + n1 k2]
+        bld.add_pass(sb, IoKind::C2C, inverse, batch, n1, n, 1, n1, lay.odist, 1, n1, Buf::Scratch0, Buf::Out, n2);
+        return prog;
+      }
+    }
+    throw std::runtime_error("plan tree has no lowering yet: " + root->key_repr());
+  }
+
+  // Real transforms.  Even n: half-length complex core with fused pack/unpack.
+  const bool even = (n % 2) == 0;
+  NodePtr core_node = root;
+  if (even) core_node = build_raw_root(planner, n / 2, nullptr, nullptr);
+  if (!bld.core_for(core_node, spec)) throw std::runtime_error("real transform length has no on-chip lowering yet");
+  if (t == Transform::R2C) {
+    const int64_t idist = in_place_real ? std::max<int64_t>(lay.idist, 2 * (n / 2 + 1)) : lay.idist;
+    auto *p = bld.add_pass(spec, even ? IoKind::R2C : IoKind::R2CFull, false, 1, batch, 0, idist, 1, 0, lay.odist, 1,
+                           Buf::In, Buf::Out, n);
+    if (even) p->a.rtw = bld.table_rtw(n);
+    p->note = even ? "n/2-point complex core" : "n-point complex core";
+  } else {
+    const int64_t odist = in_place_real ? std::max<int64_t>(lay.odist, 2 * (n / 2 + 1)) : lay.odist;
+    auto *p = bld.add_pass(spec, even ? IoKind::C2R : IoKind::C2RFull, true, 1, batch, 0, lay.idist, 1, 0, odist, 1,
+                           Buf::In, Buf::Out, n);
+    if (even) p->a.rtw = bld.table_rtw(n);
+    p->note = even ? "n/2-point complex core" : "n-point complex core";
+  }
+  return prog;
+}
+
+template <typename T>
+std::unique_ptr<Program> lower_2d_t(const NodePtr &root, Planner &planner, Transform t, bool inverse, int64_t n0,
+                                    int64_t n1, int64_t batch) {
+  auto prog = std::make_unique<Program>();
+  Builder<T> bld(*prog, planner);
+  CoreSpec rs, cs;
+  const int64_t h1 = n1 / 2 + 1;
+  if (batch > 65535) throw std::runtime_error("2-D batch above 65535");
+  if (t == Transform::C2C) {
+    if (!bld.core_for(root->row, rs) || !bld.core_for(root->col, cs))
+      throw std::runtime_error("2-D axis has no on-chip lowering yet");
+    bld.add_pass(rs, IoKind::C2C, inverse, 1, batch * n0, 0, n1, 1, 0, n1, 1, Buf::In, Buf::Out, n1);
+    bld.add_pass(cs, IoKind::C2C, inverse, batch, n1, n0 * n1, 1, n1, n0 * n1, 1, n1, Buf::Out, Buf::Out, n0);
+    return prog;
+  }
+  if (!bld.core_for(root->col, cs)) throw std::runtime_error("2-D column axis has no on-chip lowering yet");
+  const bool even = (n1 % 2) == 0;
+  NodePtr row_core = even ? build_raw_root(planner, n1 / 2, nullptr, nullptr) : root->row;
+  if (!bld.core_for(row_core, rs)) throw std::runtime_error("2-D row axis has no on-chip lowering yet");
+  prog->scratch0 = std::make_shared<DevMem>((size_t)(batch * n0 * h1) * sizeof(cpx<T>));
+  if (t == Transform::R2C) {
+    // rows into the workspace, then column tiles into the output (safe in place)
+    auto *p = bld.add_pass(rs, even ? IoKind::R2C : IoKind::R2CFull, false, 1, batch * n0, 0, n1, 1, 0, h1, 1,
+                           Buf::In, Buf::Scratch0, n1);
+    if (even) p->a.rtw = bld.table_rtw(n1);
+    bld.add_pass(cs, IoKind::C2C, false, batch, h1, n0 * h1, 1, h1, n0 * h1, 1, h1, Buf::Scratch0, Buf::Out, n0);
+  } else {
+    bld.add_pass(cs, IoKind::C2C, true, batch, h1, n0 * h1, 1, h1, n0 * h1, 1, h1, Buf::In, Buf::Scratch0, n0);
+    auto *p = bld.add_pass(rs, even ? IoKind::C2R : IoKind::C2RFull, true, 1, batch * n0, 0, h1, 1, 0, n1, 1,
+                           Buf::Scratch0, Buf::Out, n1);
+    if (even) p->a.rtw = bld.table_rtw(n1);
+  }
+  return prog;
+}
+
+}  // namespace
+
+std::unique_ptr<Program> lower(const NodePtr &root, Planner &planner, bool is_double, Transform t, bool inverse,
+                               int64_t n, const Layout &layout, bool in_place_real) {
+  return is_double ? lower_t<double>(root, planner, t, inverse, n, layout, in_place_real)
+                   : lower_t<float>(root, planner, t, inverse, n, layout, in_place_real);
+}
+
+std::unique_ptr<Program> lower_2d(const NodePtr &root, Planner &planner, bool is_double, Transform t, bool inverse,
+                                  int64_t n0, int64_t n1, int64_t batch) {
+  return is_double ? lower_2d_t<double>(root, planner, t, inverse, n0, n1, batch)
+                   : lower_2d_t<float>(root, planner, t, inverse, n0, n1, batch);
+}
+
+}  // namespace ffb

@@ -1,0 +1,69 @@
+// Executor: lowers a plan tree (plan.hpp) onto on-chip FFT passes (kernels.cu)
+// and owns the plan's device tables and workspaces.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "kernels.cuh"
+#include "plan.hpp"
+
+namespace ffb {
+
+// Device allocation owned by a plan.
+struct DevMem {
+  void *ptr = nullptr;
+  size_t bytes = 0;
+  explicit DevMem(size_t n);
+  ~DevMem();
+  DevMem(const DevMem &) = delete;
+  DevMem &operator=(const DevMem &) = delete;
+};
+using DevPtr = std::shared_ptr<DevMem>;
+
+DevPtr upload(const void *host, size_t bytes);
+
+enum class Transform { C2C, R2C, C2R };
+
+// Buffer a pass reads or writes.
+enum class Buf : int { In = 0, Out = 1, Scratch0 = 2, Scratch1 = 3 };
+
+struct PassBase {
+  virtual ~PassBase() = default;
+  virtual cudaError_t run(const void *in, void *out, void *s0, void *s1, cudaStream_t st) const = 0;
+  virtual std::string describe() const = 0;
+  virtual int launches() const { return 1; }
+};
+
+// One direction of one plan: a fixed sequence of passes.
+struct Program {
+  std::vector<std::unique_ptr<PassBase>> passes;
+  std::vector<DevPtr> owned;  // tables and workspaces
+  DevPtr scratch0, scratch1;
+  cudaError_t run(const void *in, void *out, cudaStream_t st) const;
+  std::string describe() const;
+  int launches() const;
+};
+
+// Layout of one batched 1-D or 2-D request in elements of its own types.
+struct Layout {
+  int64_t batch = 1;
+  int64_t idist = 0;  // input transform distance (input element type)
+  int64_t odist = 0;  // output transform distance (output element type)
+};
+
+// 1-D: `root` is the plan tree of the length-n complex transform (for R2C /
+// C2R the executor derives its own half-length tree with `planner` when n is
+// even).  2-D: `root` is a TwoDim node.
+std::unique_ptr<Program> lower(const NodePtr &root, Planner &planner, bool is_double, Transform t, bool inverse,
+                               int64_t n, const Layout &layout, bool in_place_real);
+std::unique_ptr<Program> lower_2d(const NodePtr &root, Planner &planner, bool is_double, Transform t, bool inverse,
+                                  int64_t n0, int64_t n1, int64_t batch);
+
+// Largest core length one CTA can hold.
+int64_t max_onchip_length(bool is_double);
+
+}  // namespace ffb

@@ -1,0 +1,74 @@
+// Host-visible kernel interface of the on-chip FFT passes (kernels.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "engine.cuh"
+
+namespace ffb {
+
+// What one CTA-resident transform computes.
+enum class CoreKind : int {
+  Dit = 0,        // plain C2C: digit-reversed load, DIT stages, natural store
+  Bluestein = 1,  // chirp * x zero-padded -> DIF fwd -> x kernel -> DIT inv -> x chirp
+  Rader = 2,      // permuted load -> DIF fwd -> x kernel -> DIT inv -> permuted store + x0
+};
+
+// How the pass reads its input and writes its output.
+enum class IoKind : int {
+  C2C = 0,  // complex in, complex out
+  R2C = 1,  // real in (n = 2L reals packed as L complex), half spectrum out (L+1 bins)
+  C2R = 2,  // half spectrum in (L+1 bins), real out (2L reals)
+  R2CFull = 3,  // real in, complex core of length n (imag 0), first n/2+1 bins out
+  C2RFull = 4,  // half spectrum in, Hermitian-expanded core of length n, real part out
+};
+
+// One pass = nbatch x G independent transforms, W of them per CTA.
+// Transform g of outer batch b reads element i at  in + b*ib + g*ig + i*ii
+// and writes element k at                          out + b*ob + g*og + k*ok
+// (units: elements of the pass's input / output type).
+template <typename T>
+struct TileArgs {
+  const void *in;
+  void *out;
+  long long nbatch;
+  long long ib, ig, ii;
+  long long ob, og, ok;
+  int G;
+  int W;
+  int tpt;    // threads per transform
+  int wfast;  // 1: consecutive threads take consecutive transforms (strided tiles)
+  int inv;    // direction of a Dit core
+  int n;      // logical length: Bluestein n, Rader p, real-transform n; else core.L
+  Core core;   // Dit stages, or the forward DIF stages of a convolution
+  Core core2;  // inverse DIT stages of a convolution (radices reversed)
+  const cpx<T> *tw;     // W_L^m, m < core.L
+  const cpx<T> *chirp;  // Bluestein chirp, n entries (direction folded in)
+  const cpx<T> *kern;   // convolution kernel spectrum / L, in DIF position order
+  const int *perm_in;   // Rader: q -> g^-q mod p
+  const int *perm_out;  // Rader: q -> g^q mod p
+  const cpx<T> *rtw;    // real-transform twiddles W_n^k, k <= n/2 (IoKind R2C / C2R)
+  // optional post-twiddle of a four-step column pass: output k of transform g
+  // is multiplied by W_N^{g*k} = hi[m / split] * lo[m % split], m = g*k < N
+  int post_twiddle;
+  const cpx<T> *ptw_lo;
+  const cpx<T> *ptw_hi;
+  FastDiv ptw_div;
+  FastDiv ldiv;  // / core.L
+  FastDiv wdiv;  // / W
+  FastDiv ndiv;  // / n
+  FastDiv hdiv;  // / (n / 2)
+};
+
+template <typename T>
+cudaError_t launch_tile(const TileArgs<T> &a, CoreKind kind, IoKind io, size_t smem_bytes, cudaStream_t stream);
+
+// Shared memory one transform of the pass occupies (bytes).
+template <typename T>
+inline size_t tile_smem_per_transform(int core_len) {
+  return (size_t)Swz<T>::padded(core_len) * sizeof(cpx<T>);
+}
+
+}  // namespace ffb

@@ -1,0 +1,163 @@
+/*
+ * ORACLE -- test infrastructure only.  Nothing in the product (the flagfft_b200
+ * package, libflagfft.so, bench.py's timed arm) links, imports or calls this
+ * file; tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg use it
+ * as the checker.
+ *
+ * A CPU restatement, in plain C, of the FFT algorithms the reference FlagFFT
+ * runs on its Exec path (flagfftExec* -> CompiledRaw*Node::execute), driven by
+ * the same plan trees its planner builds.  Built twice from ffo_impl.h:
+ *   *_d  FP64 arithmetic and tables -- the oracle proper;
+ *   *_f  float arithmetic with tables rounded from double as the reference's
+ *        src/codegen/tables.cpp does -- an estimate of the reference's own
+ *        FP32 output, used for "no worse than the reference" comparisons.
+ * Plus ffo_naive_dft: an O(n^2) long-double DFT used to pin the FP64 path.
+ *
+ * Plan encoding (int64 preorder, mirrors the node shapes of
+ * src/utils/include/flagfft/plan.hpp:14-98):
+ *   leaf       [0, n, nfactors, f0, f1, ...]
+ *   four_step  [1, n, n1, n2, <row n1>, <col n2>]
+ *   bluestein  [2, n, m, <child m>]
+ *   rader      [3, p, g, <child p-1>]
+ *   direct     [4, n]
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define FFO_PI 3.14159265358979323846264338327950288
+
+enum { FFO_LEAF = 0, FFO_FOUR_STEP = 1, FFO_BLUESTEIN = 2, FFO_RADER = 3, FFO_DIRECT = 4 };
+
+typedef struct ffo_node {
+  int kind;
+  int64_t length;
+  int64_t factors[64];
+  int nfactors;
+  int64_t n1, n2, m, root;
+  struct ffo_node *a, *b;
+} ffo_node;
+
+static void ffo_free(ffo_node *nd) {
+  if (!nd) return;
+  ffo_free(nd->a);
+  ffo_free(nd->b);
+  free(nd);
+}
+
+static ffo_node *ffo_parse(const int64_t *code, int64_t *pos) {
+  ffo_node *nd = (ffo_node *)calloc(1, sizeof(ffo_node));
+  nd->kind = (int)code[(*pos)++];
+  nd->length = code[(*pos)++];
+  switch (nd->kind) {
+    case FFO_LEAF: {
+      nd->nfactors = (int)code[(*pos)++];
+      int64_t prod = 1;
+      for (int i = 0; i < nd->nfactors; ++i) {
+        nd->factors[i] = code[(*pos)++];
+        prod *= nd->factors[i];
+        if (nd->factors[i] > 64) {
+          ffo_free(nd);
+          return NULL;
+        }
+      }
+      if (prod != nd->length || nd->nfactors < 1) {
+        ffo_free(nd);
+        return NULL;
+      }
+      break;
+    }
+    case FFO_FOUR_STEP:
+      nd->n1 = code[(*pos)++];
+      nd->n2 = code[(*pos)++];
+      nd->a = ffo_parse(code, pos);
+      nd->b = ffo_parse(code, pos);
+      if (!nd->a || !nd->b || nd->n1 * nd->n2 != nd->length) {
+        ffo_free(nd);
+        return NULL;
+      }
+      break;
+    case FFO_BLUESTEIN:
+      nd->m = code[(*pos)++];
+      nd->a = ffo_parse(code, pos);
+      if (!nd->a || nd->a->length != nd->m || nd->m < 2 * nd->length - 1) {
+        ffo_free(nd);
+        return NULL;
+      }
+      break;
+    case FFO_RADER:
+      nd->root = code[(*pos)++];
+      nd->a = ffo_parse(code, pos);
+      if (!nd->a || nd->a->length != nd->length - 1) {
+        ffo_free(nd);
+        return NULL;
+      }
+      break;
+    case FFO_DIRECT:
+      break;
+    default:
+      ffo_free(nd);
+      return NULL;
+  }
+  return nd;
+}
+
+/* Cache of cos/sin(2*pi*m/n), m < n, for n up to 2^20 (computed in double,
+ * the precision the reference builds its tables in).  The oracle is single-
+ * threaded per process. */
+#define FFO_ROOT_SLOTS 1024
+static int64_t ffo_root_n[FFO_ROOT_SLOTS];
+static double *ffo_root_tab[FFO_ROOT_SLOTS];
+
+static const double *ffo_unit_roots(int64_t n) {
+  if (n <= 0 || n > (1 << 20)) return NULL;
+  uint64_t h = ((uint64_t)n * 0x9e3779b97f4a7c15ULL) >> 54;
+  for (int probe = 0; probe < FFO_ROOT_SLOTS; ++probe) {
+    int slot = (int)((h + (uint64_t)probe) % FFO_ROOT_SLOTS);
+    if (ffo_root_n[slot] == n) return ffo_root_tab[slot];
+    if (ffo_root_n[slot] == 0) {
+      double *t = (double *)malloc(sizeof(double) * 2 * (size_t)n);
+      for (int64_t m = 0; m < n; ++m) {
+        double a = 2.0 * FFO_PI * (double)m / (double)n;
+        t[2 * m] = cos(a);
+        t[2 * m + 1] = sin(a);
+      }
+      ffo_root_n[slot] = n;
+      ffo_root_tab[slot] = t;
+      return t;
+    }
+  }
+  return NULL;
+}
+
+#define REAL double
+#define SFX(name) name##_d
+#include "ffo_impl.h"
+#undef REAL
+#undef SFX
+
+#define REAL float
+#define SFX(name) name##_f
+#include "ffo_impl.h"
+#undef REAL
+#undef SFX
+
+/* O(n^2) DFT accumulated in long double with the phase index j*k reduced
+ * exactly mod n: the independent pin for the FP64 restatement. */
+int ffo_naive_dft(const double *in, double *out, int64_t n, int direction) {
+  const long double pi = 3.14159265358979323846264338327950288L;
+  for (int64_t k = 0; k < n; ++k) {
+    long double re = 0, im = 0;
+    for (int64_t j = 0; j < n; ++j) {
+      int64_t m = (int64_t)(((__int128)j * k) % n);
+      long double a = (direction > 0 ? 2.0L : -2.0L) * pi * (long double)m / (long double)n;
+      long double c = cosl(a), s = sinl(a);
+      re += (long double)in[2 * j] * c - (long double)in[2 * j + 1] * s;
+      im += (long double)in[2 * j] * s + (long double)in[2 * j + 1] * c;
+    }
+    out[2 * k] = (double)re;
+    out[2 * k + 1] = (double)im;
+  }
+  return 0;
+}
