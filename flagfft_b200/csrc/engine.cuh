@@ -425,4 +425,91 @@ FFB_HD void run_dif(cpx<T> *buf, const Core &c, int tid, int nthr,
   }
 }
 
+// ---------------------------------------------------------------------------
+// Stockham autosort (out of place, natural order in and out).
+//
+// Stage s with radix R and Ns = R0*...*R(s-1): butterfly j (< L/R) reads
+// elements j + r*L/R, multiplies input r by W_{Ns R}^{r (j mod Ns)}, and writes
+// output q to (j - j mod Ns)*R + j mod Ns + q*Ns.  The first stage reads the
+// caller's source and the last writes the caller's sink directly, so global
+// memory is read and written in the coalesced j + r*L/R pattern and the
+// stages in between ping-pong between two shared-memory buffers.  Uses the
+// DIT core's fields (span = Ns, tws = L/(Ns R), sdiv = / Ns).
+// ---------------------------------------------------------------------------
+
+// Shared-memory position of element p in a ping-pong buffer: one pad element
+// per 16 spreads the stride-R writes of the early stages over the banks.
+FFB_HD int pp_pos(int p) { return p + (p >> 4); }
+FFB_HD int pp_size(int L) { return ((L + (L >> 4) + 1) + 1) & ~1; }
+
+template <int R, typename T, class Src, class Dst>
+FFB_HD void stockham_stage_r(const Core &c, int s, int tid, int nthr, const cpx<T> *__restrict__ tw, bool inv,
+                             Src &src, Dst &dst) {
+  const int Ns = c.span[s];
+  const int tws = c.tws[s];
+  const int nb = c.L / R;
+  for (int j = tid; j < nb; j += nthr) {
+    const int k = j - (int)fdiv((uint32_t)j, c.sdiv[s]) * Ns;
+    cpx<T> v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r] = src(j + r * nb);
+    if (k != 0) {
+#pragma unroll
+      for (int r = 1; r < R; ++r) v[r] = cmul(v[r], twiddle(tw, r * k * tws, inv));
+    }
+    dft_dir<R, T>(v, inv);
+    const int base = (j - k) * R + k;
+#pragma unroll
+    for (int q = 0; q < R; ++q) dst(base + q * Ns, v[q]);
+  }
+}
+
+// Shared-memory reader / writer of a ping-pong buffer.
+template <typename T>
+struct PPRead {
+  const cpx<T> *b;
+  FFB_HD cpx<T> operator()(int p) const { return b[pp_pos(p)]; }
+};
+template <typename T>
+struct PPWrite {
+  cpx<T> *b;
+  FFB_HD void operator()(int p, cpx<T> v) const { b[pp_pos(p)] = v; }
+};
+
+// Runs all stages of `c`: stage 0 reads `src`, the last stage writes `dst`,
+// the others go through b0 / b1 (stage s < last writes b0 for even s, b1 for
+// odd s).  A barrier follows every stage except the last.  The last stage
+// reads the buffer of parity (nst - 2), so the one of parity (nst - 1) is free
+// for the sink to write into.
+template <typename T, class Src, class Dst, class Sync>
+FFB_HD void run_stockham(const Core &c, cpx<T> *b0, cpx<T> *b1, int tid, int nthr, const cpx<T> *__restrict__ tw,
+                         bool inv, Src &src, Dst &dst, Sync sync) {
+  const int S = c.nst;
+  for (int s = 0; s < S; ++s) {
+    const bool first = s == 0, last = s == S - 1;
+    if (first && last) {
+#define FFB_SS(R) stockham_stage_r<R, T>(c, s, tid, nthr, tw, inv, src, dst)
+      FFB_RADIX_SWITCH(c.radix[s], FFB_SS)
+#undef FFB_SS
+    } else if (first) {
+      PPWrite<T> w{b0};
+#define FFB_SS(R) stockham_stage_r<R, T>(c, s, tid, nthr, tw, inv, src, w)
+      FFB_RADIX_SWITCH(c.radix[s], FFB_SS)
+#undef FFB_SS
+    } else if (last) {
+      PPRead<T> rd{((s - 1) & 1) ? b1 : b0};
+#define FFB_SS(R) stockham_stage_r<R, T>(c, s, tid, nthr, tw, inv, rd, dst)
+      FFB_RADIX_SWITCH(c.radix[s], FFB_SS)
+#undef FFB_SS
+    } else {
+      PPRead<T> rd{((s - 1) & 1) ? b1 : b0};
+      PPWrite<T> w{(s & 1) ? b1 : b0};
+#define FFB_SS(R) stockham_stage_r<R, T>(c, s, tid, nthr, tw, inv, rd, w)
+      FFB_RADIX_SWITCH(c.radix[s], FFB_SS)
+#undef FFB_SS
+    }
+    if (!last) sync();
+  }
+}
+
 }  // namespace ffb

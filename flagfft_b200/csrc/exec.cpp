@@ -117,6 +117,7 @@ const char *kind_name(CoreKind k) {
     case CoreKind::Dit: return "stockham-dit";
     case CoreKind::Bluestein: return "bluestein-fused";
     case CoreKind::Rader: return "rader-fused";
+    case CoreKind::Conv: return "convolution-rows";
   }
   return "?";
 }
@@ -128,6 +129,8 @@ const char *io_name(IoKind k) {
     case IoKind::C2R: return "c2r-halfpack";
     case IoKind::R2CFull: return "r2c-full";
     case IoKind::C2RFull: return "c2r-full";
+    case IoKind::PackC2C: return "real-pairs-in";
+    case IoKind::C2CUnpack: return "real-pairs-out";
   }
   return "?";
 }
@@ -167,6 +170,31 @@ struct TilePass final : PassBase {
       << " threads=" << a.W * a.tpt << " smem=" << smem << " " << buf_name(src) << "->" << buf_name(dst);
     if (a.post_twiddle) o << " +twiddle";
     if (!note.empty()) o << " (" << note << ")";
+    return o.str();
+  }
+};
+
+// Elementwise real-transform post (Z -> half spectrum) or pre (half spectrum
+// -> Z) processing between the passes of a multi-pass R2C / C2R.
+template <typename T>
+struct RealPass final : PassBase {
+  bool post;
+  Buf src, dst;
+  long long batch, sdist, ddist;
+  int L;
+  const cpx<T> *rtw;
+  RealPass(bool post_, Buf s, Buf d, long long b, long long sd, long long dd, int64_t L_, const cpx<T> *r)
+      : post(post_), src(s), dst(d), batch(b), sdist(sd), ddist(dd), L((int)L_), rtw(r) {}
+  cudaError_t run(const void *in, void *out, void *s0, void *s1, cudaStream_t st) const override {
+    auto *sp = reinterpret_cast<const cpx<T> *>(TilePass<T>::pick(src, in, out, s0, s1));
+    auto *dp = reinterpret_cast<cpx<T> *>(TilePass<T>::pick(dst, in, out, s0, s1));
+    return post ? launch_real_post<T>(sp, dp, batch, sdist, ddist, L, rtw, st)
+                : launch_real_pre<T>(sp, dp, batch, sdist, ddist, L, rtw, st);
+  }
+  std::string describe() const override {
+    std::ostringstream o;
+    o << (post ? "real-post" : "real-pre") << " " << (sizeof(T) == 4 ? "f32" : "f64") << " L=" << L
+      << " transforms=" << batch << " " << buf_name(src) << "->" << buf_name(dst);
     return o.str();
   }
 };
@@ -302,21 +330,26 @@ class Builder {
     a.inv = inverse ? 1 : 0;
     a.n = (int)logical_n;
     const int64_t L = spec.L;
+    const size_t limit = 232448;
+    // Stockham ping-pong when two buffers of the transform fit (C2C passes);
+    // the in-place DIT / DIF path otherwise.
+    const size_t pp_per = 2 * (size_t)pp_size((int)L) * sizeof(cpx<T>);
+    a.pp = (io == IoKind::C2C && L > 1 && pp_per <= limit) ? 1 : 0;
     if (spec.kind == CoreKind::Dit) {
       a.core = make_dit_core(L, spec.radices);
     } else {
-      a.core = make_dif_core(L, spec.radices);
+      a.core = a.pp ? make_dit_core(L, spec.radices) : make_dif_core(L, spec.radices);
       std::vector<int> rev(spec.radices.rbegin(), spec.radices.rend());
       a.core2 = make_dit_core(L, rev);
-      fill_convolution(a, spec, inverse);
+      if (spec.kind != CoreKind::Conv) fill_convolution(a, spec, inverse);  // Conv: caller supplies the kernel
     }
     a.tw = table_tw(L);
-    // thread and tile shape
-    const bool strided = ig == 1 && ii != 1;
+    // thread and tile shape: column tiles (transform index fastest in memory)
+    // take consecutive transforms on consecutive threads
+    const bool strided = ii > ig;
     a.wfast = strided ? 1 : 0;
     int tpt = choose_tpt(L, spec.radices);
-    const size_t per = tile_smem_per_transform<T>((int)L) + Swz<T>::G * sizeof(cpx<T>);
-    const size_t limit = 232448;
+    const size_t per = a.pp ? pp_per : tile_smem_per_transform<T>((int)L) + Swz<T>::G * sizeof(cpx<T>);
     int64_t W;
     if (strided) {
       W = std::min<int64_t>({(int64_t)(limit / per), 8, G});
@@ -365,6 +398,44 @@ class Builder {
       cld w = unit_root(k, n, -1);
       h[(size_t)k] = mk((T)w.real(), (T)w.imag());
     }
+    DevPtr d = upload(h.data(), h.size() * sizeof(cpx<T>));
+    prog_.owned.push_back(d);
+    return reinterpret_cast<const cpx<T> *>(d->ptr);
+  }
+
+  // Bluestein chirp exp(-+ i pi (j^2 mod 2n) / n), j < n (+ for the inverse).
+  const cpx<T> *table_chirp(int64_t n, bool inverse) {
+    std::vector<cpx<T>> h((size_t)n);
+    for (int64_t j = 0; j < n; ++j) {
+      cld c = chirp_value(j, n, inverse ? 1 : -1);
+      h[(size_t)j] = mk((T)c.real(), (T)c.imag());
+    }
+    DevPtr d = upload(h.data(), h.size() * sizeof(cpx<T>));
+    prog_.owned.push_back(d);
+    return reinterpret_cast<const cpx<T> *>(d->ptr);
+  }
+
+  // Bluestein kernel spectrum B[k] / M laid out per row k1 of an n1 x n2
+  // four-step: entry k1 * n2 + p holds B[k1 + n1 k2] for p = k2 (Stockham
+  // passes) or the n2-point DIF position of k2 (in-place passes).
+  const cpx<T> *table_bluestein_rows(const NodePtr &node, const std::vector<int> &col_radices, int64_t n1,
+                                     int64_t n2, bool inverse, bool natural) {
+    const int64_t n = node->length, M = node->conv_length;
+    const int sign = inverse ? 1 : -1;
+    std::vector<cld> b((size_t)M, cld(0));
+    for (int64_t k = 0; k < n; ++k) {
+      cld bc = chirp_value(k, n, -sign);
+      b[(size_t)k] = bc;
+      if (k) b[(size_t)(M - k)] = bc;
+    }
+    host_fft(b, -1);
+    std::vector<cpx<T>> h((size_t)M);
+    for (int64_t k1 = 0; k1 < n1; ++k1)
+      for (int64_t k2 = 0; k2 < n2; ++k2) {
+        cld v = b[(size_t)(k1 + n1 * k2)] / (long double)M;
+        const int64_t p = natural ? k2 : dif_position(k2, col_radices);
+        h[(size_t)(k1 * n2 + p)] = mk((T)v.real(), (T)v.imag());
+      }
     DevPtr d = upload(h.data(), h.size() * sizeof(cpx<T>));
     prog_.owned.push_back(d);
     return reinterpret_cast<const cpx<T> *>(d->ptr);
@@ -435,7 +506,7 @@ class Builder {
     std::vector<cpx<T>> kern((size_t)L);
     for (int64_t k = 0; k < L; ++k) {
       cld v = b[(size_t)k] / (long double)L;
-      kern[(size_t)dif_position(k, spec.radices)] = mk((T)v.real(), (T)v.imag());
+      kern[(size_t)(a.pp ? k : dif_position(k, spec.radices))] = mk((T)v.real(), (T)v.imag());
     }
     DevPtr dk = upload(kern.data(), kern.size() * sizeof(cpx<T>));
     prog_.owned.push_back(dk);
@@ -447,56 +518,133 @@ class Builder {
   std::vector<std::pair<int64_t, DevPtr>> tw_cache_;
 };
 
+// A length-n complex transform over `batch` rows (row distances idist / odist)
+// from `src` to `dst`; `ws` is a workspace of batch * (n or the Bluestein
+// convolution length) elements when the plan needs more than one pass.
+template <typename T>
+void lower_c2c(Builder<T> &bld, Program &prog, const NodePtr &root, bool inverse, int64_t n, int64_t batch,
+               long long idist, long long odist, Buf src, Buf dst) {
+  CoreSpec spec;
+  if (bld.core_for(root, spec)) {
+    bld.add_pass(spec, IoKind::C2C, inverse, 1, batch, 0, idist, 1, 0, odist, 1, src, dst, n);
+    return;
+  }
+  if (batch > 65535) throw std::runtime_error("multi-pass batch above 65535");
+  if (root->kind == NodeKind::FourStep) {
+    CoreSpec sa, sb;
+    if (bld.core_for(root->row, sa) && bld.core_for(root->col, sb)) {
+      const int64_t n1 = root->n1, n2 = root->n2;
+      prog.scratch0 = std::make_shared<DevMem>((size_t)(batch * n) * sizeof(cpx<T>));
+      // pass A: columns j2 (stride n2) of length n1, x W_n^{j2 k1}, rows Y[j2][k1]
+      auto *pa = bld.add_pass(sa, IoKind::C2C, inverse, batch, n2, idist, 1, n2, n, n1, 1, src, Buf::Scratch0, n1);
+      bld.set_post_twiddle(pa->a, n);
+      // pass B: for each k1, length n2 over Y[j2][k1] -> X[k1 + n1 k2]
+      bld.add_pass(sb, IoKind::C2C, inverse, batch, n1, n, 1, n1, odist, 1, n1, Buf::Scratch0, dst, n2);
+      return;
+    }
+  }
+  if (root->kind == NodeKind::Bluestein && root->child->kind == NodeKind::FourStep) {
+    // Convolution of length M = n1 * n2 too long for one CTA: three passes
+    // through an M-point workspace, with the chirps, the kernel product and
+    // both four-step twiddles fused (src/exec/raw_nodes.cpp:153-204 runs the
+    // same chain as 7 launches).
+    const NodePtr &fs = root->child;
+    CoreSpec sa, sb;
+    if (bld.core_for(fs->row, sa) && bld.core_for(fs->col, sb) && sa.kind == CoreKind::Dit &&
+        sb.kind == CoreKind::Dit) {
+      const int64_t M = root->conv_length, n1 = fs->n1, n2 = fs->n2;
+      prog.scratch0 = std::make_shared<DevMem>((size_t)(batch * M) * sizeof(cpx<T>));
+      const cpx<T> *chirp = bld.table_chirp(n, inverse);
+      // A: a_j = x_j c_j (j = j1 n2 + j2 < n), FFT over j1, x W_M^{j2 k1} -> Y[k1][j2]
+      auto *pa = bld.add_pass(sa, IoKind::C2C, false, batch, n2, idist, 1, n2, M, 1, n2, src, Buf::Scratch0, n);
+      pa->a.chirp_mode = 1;
+      pa->a.chirp = chirp;
+      pa->a.cj_e = n2;
+      pa->a.cj_g = 1;
+      bld.set_post_twiddle(pa->a, M);
+      pa->note = "bluestein 1/3: chirp + column FFT";
+      // B: per k1: FFT over j2, x B[k1 + n1 k2] / M, inverse FFT over k2, x W_M^{-j2 k1}
+      CoreSpec sc = sb;
+      sc.kind = CoreKind::Conv;
+      auto *pb = bld.add_pass(sc, IoKind::C2C, true, batch, n1, M, n2, 1, M, n2, 1, Buf::Scratch0, Buf::Scratch0, n2);
+      pb->a.kern = bld.table_bluestein_rows(root, sb.radices, n1, n2, inverse, pb->a.pp != 0);
+      pb->a.kern_stride = n2;
+      bld.set_post_twiddle(pb->a, M);
+      pb->note = "bluestein 2/3: row convolution";
+      // C: inverse FFT over k1 -> j1, y_j = conv_j c_j for j = j1 n2 + j2 < n
+      auto *pc = bld.add_pass(sa, IoKind::C2C, true, batch, n2, M, 1, n2, odist, 1, n2, Buf::Scratch0, dst, n);
+      pc->a.chirp_mode = 2;
+      pc->a.chirp = chirp;
+      pc->a.cj_e = n2;
+      pc->a.cj_g = 1;
+      pc->note = "bluestein 3/3: column inverse FFT + chirp";
+      return;
+    }
+  }
+  throw std::runtime_error("plan tree has no lowering on this engine: " + root->key_repr());
+}
+
 template <typename T>
 std::unique_ptr<Program> lower_t(const NodePtr &root, Planner &planner, Transform t, bool inverse, int64_t n,
                                  const Layout &lay, bool in_place_real) {
   auto prog = std::make_unique<Program>();
   Builder<T> bld(*prog, planner);
-  CoreSpec spec;
   const int64_t batch = lay.batch;
 
   if (t == Transform::C2C) {
-    if (bld.core_for(root, spec)) {
-      bld.add_pass(spec, IoKind::C2C, inverse, 1, batch, 0, lay.idist, 1, 0, lay.odist, 1, Buf::In, Buf::Out, n);
-      return prog;
-    }
-    if (root->kind == NodeKind::FourStep) {
-      CoreSpec sa, sb;
-      if (bld.core_for(root->row, sa) && bld.core_for(root->col, sb)) {
-        const int64_t n1 = root->n1, n2 = root->n2;
-        if (batch > 65535) throw std::runtime_error("four-step batch above 65535");
-        prog->scratch0 = std::make_shared<DevMem>((size_t)(batch * n) * sizeof(cpx<T>));
-        // pass A: columns j2 (stride n2) of length n1, twiddle W_n^{j2 k1}, rows Y[j2][k1]
-        auto *pa = bld.add_pass(sa, IoKind::C2C, inverse, batch, n2, lay.idist, 1, n2, n, n1, 1, Buf::In,
-                                Buf::Scratch0, n1);
-        bld.set_post_twiddle(pa->a, n);
-        // pass B: for each k1, length n2 over Y[j2][k1] -> X[k1 + n1 k2]
-        bld.add_pass(sb, IoKind::C2C, inverse, batch, n1, n, 1, n1, lay.odist, 1, n1, Buf::Scratch0, Buf::Out, n2);
-        return prog;
-      }
-    }
-    throw std::runtime_error("plan tree has no lowering yet: " + root->key_repr());
+    lower_c2c<T>(bld, *prog, root, inverse, n, batch, lay.idist, lay.odist, Buf::In, Buf::Out);
+    return prog;
   }
 
-  // Real transforms.  Even n: half-length complex core with fused pack/unpack.
+  // Real transforms.  Even n: n/2-point complex core with the pack / unpack
+  // fused into its load and store; odd n: the n-point core on real data.
   const bool even = (n % 2) == 0;
-  NodePtr core_node = root;
-  if (even) core_node = build_raw_root(planner, n / 2, nullptr, nullptr);
-  if (!bld.core_for(core_node, spec)) throw std::runtime_error("real transform length has no on-chip lowering yet");
-  if (t == Transform::R2C) {
-    const int64_t idist = in_place_real ? std::max<int64_t>(lay.idist, 2 * (n / 2 + 1)) : lay.idist;
-    auto *p = bld.add_pass(spec, even ? IoKind::R2C : IoKind::R2CFull, false, 1, batch, 0, idist, 1, 0, lay.odist, 1,
-                           Buf::In, Buf::Out, n);
-    if (even) p->a.rtw = bld.table_rtw(n);
-    p->note = even ? "n/2-point complex core" : "n-point complex core";
-  } else {
-    const int64_t odist = in_place_real ? std::max<int64_t>(lay.odist, 2 * (n / 2 + 1)) : lay.odist;
-    auto *p = bld.add_pass(spec, even ? IoKind::C2R : IoKind::C2RFull, true, 1, batch, 0, lay.idist, 1, 0, odist, 1,
-                           Buf::In, Buf::Out, n);
-    if (even) p->a.rtw = bld.table_rtw(n);
-    p->note = even ? "n/2-point complex core" : "n-point complex core";
+  const int64_t L = n / 2;
+  NodePtr core_node = even ? build_raw_root(planner, L, nullptr, nullptr) : root;
+  const int64_t idist = (t == Transform::R2C && in_place_real) ? std::max<int64_t>(lay.idist, 2 * (L + 1)) : lay.idist;
+  const int64_t odist = (t == Transform::C2R && in_place_real) ? std::max<int64_t>(lay.odist, 2 * (L + 1)) : lay.odist;
+  CoreSpec spec;
+  if (bld.core_for(core_node, spec)) {
+    if (t == Transform::R2C) {
+      auto *p = bld.add_pass(spec, even ? IoKind::R2C : IoKind::R2CFull, false, 1, batch, 0, idist, even ? 2 : 1, 0,
+                             odist, 1, Buf::In, Buf::Out, n);
+      if (even) p->a.rtw = bld.table_rtw(n);
+      p->note = even ? "n/2-point complex core" : "n-point complex core";
+    } else {
+      auto *p = bld.add_pass(spec, even ? IoKind::C2R : IoKind::C2RFull, true, 1, batch, 0, idist, 1, 0, odist,
+                             even ? 2 : 1, Buf::In, Buf::Out, n);
+      if (even) p->a.rtw = bld.table_rtw(n);
+      p->note = even ? "n/2-point complex core" : "n-point complex core";
+    }
+    return prog;
   }
-  return prog;
+  CoreSpec sa, sb;
+  if (even && core_node->kind == NodeKind::FourStep && bld.core_for(core_node->row, sa) &&
+      bld.core_for(core_node->col, sb)) {
+    if (batch > 65535) throw std::runtime_error("multi-pass batch above 65535");
+    const int64_t n1 = core_node->n1, n2 = core_node->n2;
+    const cpx<T> *rtw = bld.table_rtw(n);
+    prog->scratch0 = std::make_shared<DevMem>((size_t)(batch * L) * sizeof(cpx<T>));
+    if (t == Transform::R2C) {
+      // A: z_j = x_2j + i x_2j+1 (j = j1 n2 + j2), FFT over j1, x W_L^{j2 k1} -> Y[j2][k1]
+      auto *pa = bld.add_pass(sa, IoKind::PackC2C, false, batch, n2, idist, 2, 2 * n2, L, n1, 1, Buf::In,
+                              Buf::Scratch0, n1);
+      bld.set_post_twiddle(pa->a, L);
+      // B: FFT over j2 -> Z[k1 + n1 k2] in the output rows
+      bld.add_pass(sb, IoKind::C2C, false, batch, n1, L, 1, n1, odist, 1, n1, Buf::Scratch0, Buf::Out, n2);
+      prog->passes.push_back(std::make_unique<RealPass<T>>(true, Buf::Out, Buf::Out, batch, odist, odist, L, rtw));
+    } else {
+      prog->scratch1 = std::make_shared<DevMem>((size_t)(batch * L) * sizeof(cpx<T>));
+      prog->passes.push_back(
+          std::make_unique<RealPass<T>>(false, Buf::In, Buf::Scratch1, batch, idist, L, L, rtw));
+      auto *pa = bld.add_pass(sa, IoKind::C2C, true, batch, n2, L, 1, n2, L, n1, 1, Buf::Scratch1, Buf::Scratch0, n1);
+      bld.set_post_twiddle(pa->a, L);
+      // B: inverse FFT over j2, z_j -> x_2j, x_2j+1 (j = k1 + n1 k2)
+      bld.add_pass(sb, IoKind::C2CUnpack, true, batch, n1, L, 1, n1, odist, 2, 2 * n1, Buf::Scratch0, Buf::Out, n2);
+    }
+    return prog;
+  }
+  throw std::runtime_error("real transform length has no lowering on this engine");
 }
 
 template <typename T>
@@ -521,14 +669,14 @@ std::unique_ptr<Program> lower_2d_t(const NodePtr &root, Planner &planner, Trans
   prog->scratch0 = std::make_shared<DevMem>((size_t)(batch * n0 * h1) * sizeof(cpx<T>));
   if (t == Transform::R2C) {
     // rows into the workspace, then column tiles into the output (safe in place)
-    auto *p = bld.add_pass(rs, even ? IoKind::R2C : IoKind::R2CFull, false, 1, batch * n0, 0, n1, 1, 0, h1, 1,
-                           Buf::In, Buf::Scratch0, n1);
+    auto *p = bld.add_pass(rs, even ? IoKind::R2C : IoKind::R2CFull, false, 1, batch * n0, 0, n1, even ? 2 : 1, 0,
+                           h1, 1, Buf::In, Buf::Scratch0, n1);
     if (even) p->a.rtw = bld.table_rtw(n1);
     bld.add_pass(cs, IoKind::C2C, false, batch, h1, n0 * h1, 1, h1, n0 * h1, 1, h1, Buf::Scratch0, Buf::Out, n0);
   } else {
     bld.add_pass(cs, IoKind::C2C, true, batch, h1, n0 * h1, 1, h1, n0 * h1, 1, h1, Buf::In, Buf::Scratch0, n0);
-    auto *p = bld.add_pass(rs, even ? IoKind::C2R : IoKind::C2RFull, true, 1, batch * n0, 0, h1, 1, 0, n1, 1,
-                           Buf::Scratch0, Buf::Out, n1);
+    auto *p = bld.add_pass(rs, even ? IoKind::C2R : IoKind::C2RFull, true, 1, batch * n0, 0, h1, 1, 0, n1,
+                           even ? 2 : 1, Buf::Scratch0, Buf::Out, n1);
     if (even) p->a.rtw = bld.table_rtw(n1);
   }
   return prog;

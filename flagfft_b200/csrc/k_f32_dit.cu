@@ -1,0 +1,11 @@
+// Instantiates one group of on-chip FFT pass kernels (float); split from
+// kernels.cu so the kernel variants compile in parallel.
+#include "tile_impl.cuh"
+
+namespace ffb {
+namespace tile {
+template cudaError_t launch_group<float, 0>(const TileArgs<float> &, int, size_t, cudaStream_t);
+template cudaError_t launch_one<float, 0, 5>(const TileArgs<float> &, size_t, cudaStream_t);
+template cudaError_t launch_one<float, 0, 6>(const TileArgs<float> &, size_t, cudaStream_t);
+}  // namespace tile
+}  // namespace ffb

@@ -1,366 +1,130 @@
-// On-chip FFT passes for sm_100a.
-//
-// One kernel template covers every pass that keeps whole transforms in shared
-// memory: contiguous rows (1-D batches, 2-D rows), strided column tiles (2-D
-// columns, four-step column and row passes), the fused Bluestein and Rader
-// chains, and the fused real-to-complex / complex-to-real packing.  Each CTA
-// holds W transforms; every element crosses HBM once on the way in and once on
-// the way out.
-//
-// The body (tile_body) is written once against an execution policy: DevX runs
-// it as a CUDA thread block; HostX runs the identical code sequentially on the
-// CPU with one "thread" and no-op barriers (built only with
-// FFB_HOST_EMULATION, for host-side checks of the index arithmetic; never part
-// of libflagfft.so).  Sequential execution is exact because every phase's
-// iterations touch disjoint shared-memory positions.
-#include "kernels.cuh"
-
+// Dispatch of the on-chip FFT passes (the kernel bodies are in tile_impl.cuh,
+// instantiated per precision and core kind in k_*.cu) and the elementwise
+// real-transform pre/post kernels.
+#include <algorithm>
 #include <cstring>
-#include <vector>
+
+#include "kernels.cuh"
 
 namespace ffb {
 
+namespace tile {
+// defined in k_*.cu
+template <typename T, int K>
+cudaError_t launch_group(const TileArgs<T> &a, int io, size_t smem, cudaStream_t s);
+template <typename T, int K>
+cudaError_t launch_pp(const TileArgs<T> &a, size_t smem, cudaStream_t s);
+template <typename T, int KIND, int IO>
+cudaError_t launch_one(const TileArgs<T> &a, size_t smem, cudaStream_t s);
+}  // namespace tile
+
 namespace {
 
+// One thread per pair (k, L-k), k = 0..L/2: reads both Z values, writes both
+// X values, so z and x may alias.
 template <typename T>
-FFB_HD cpx<T> ld_cpx(const void *base, long long idx) {
-  return ldg_c(reinterpret_cast<const cpx<T> *>(base) + idx);
-}
-template <typename T>
-FFB_HD T ld_real(const void *base, long long idx) {
-  return ldg_v(reinterpret_cast<const T *>(base) + idx);
-}
-template <typename T>
-FFB_HD void st_cpx(void *base, long long idx, cpx<T> v) {
-  reinterpret_cast<cpx<T> *>(base)[idx] = v;
-}
-template <typename T>
-FFB_HD void st_real(void *base, long long idx, T v) {
-  reinterpret_cast<T *>(base)[idx] = v;
-}
-
-// CUDA thread block.
-struct DevX {
-  int tpt;
-  FFB_HD int tid() const {
-#ifdef __CUDA_ARCH__
-    return threadIdx.x;
-#else
-    return 0;
-#endif
-  }
-  FFB_HD int nthreads() const {
-#ifdef __CUDA_ARCH__
-    return blockDim.x;
-#else
-    return 1;
-#endif
-  }
-  FFB_HD void sync() const {
-#ifdef __CUDA_ARCH__
-    __syncthreads();
-#endif
-  }
-  // Runs f(slot, tid-in-slot, threads-per-slot) for this thread's transform.
-  template <class F>
-  FFB_HD void per_slot(int /*W*/, F f) const {
-    const int t = tid();
-    const int slot = t / tpt;
-    f(slot, t - slot * tpt, tpt);
-  }
-};
-
-// Sequential host execution of one block.
-struct HostX {
-  FFB_HD int tid() const { return 0; }
-  FFB_HD int nthreads() const { return 1; }
-  FFB_HD void sync() const {}
-  template <class F>
-  FFB_HD void per_slot(int W, F f) const {
-    for (int s = 0; s < W; ++s) f(s, 0, 1);
-  }
-};
-
-// Splits a flat element counter e over (transform w, element i) of a CTA tile.
-FFB_HD void split_elem(int e, int W, int Lx, int wfast, const FastDiv &wdiv, const FastDiv &ldiv, int &w, int &i) {
-  if (wfast) {
-    i = (int)fdiv((uint32_t)e, wdiv);
-    w = e - i * W;
-  } else {
-    w = (int)fdiv((uint32_t)e, ldiv);
-    i = e - w * Lx;
-  }
-}
-
-template <typename T, int KIND, int IO, class X>
-FFB_HD void tile_body(const TileArgs<T> &a, long long bx, long long by, cpx<T> *sm, const X &x) {
-  constexpr int G = Swz<T>::G;
-  const int L = a.core.L;                // core (buffer) length
-  const int Lp = Swz<T>::padded(L) + G;  // + a spare group: Rader's x0 / X0 slots
-  const int W = a.W;
-  const long long b = by;
-  const long long g0 = bx * W;
-  constexpr bool real_in = IO == 1 || IO == 3;
-  constexpr bool real_out = IO == 2 || IO == 4;
-  const void *in = reinterpret_cast<const unsigned char *>(a.in) +
-                   b * a.ib * (long long)(real_in ? sizeof(T) : sizeof(cpx<T>));
-  void *out = reinterpret_cast<unsigned char *>(a.out) + b * a.ob * (long long)(real_out ? sizeof(T) : sizeof(cpx<T>));
-  const int n = a.n;
-  const int half_n = n / 2;  // real transforms: n reals, half_n + 1 bins
-  const int t0 = x.tid(), nt = x.nthreads();
-
-  // Logical input element i of the core's transform g.
-  auto core_input = [&](long long g, int i) -> cpx<T> {
-    const long long base = g * a.ig;
-    if constexpr (IO == 0) {
-      return ld_cpx<T>(in, base + (long long)i * a.ii);
-    } else if constexpr (IO == 1) {  // z_i = x_2i + i x_2i+1
-      T re = ld_real<T>(in, base + (long long)(2 * i) * a.ii);
-      T im = ld_real<T>(in, base + (long long)(2 * i + 1) * a.ii);
-      return mk(re, im);
-    } else if constexpr (IO == 3) {  // real x_i, imaginary part 0
-      return mk(ld_real<T>(in, base + (long long)i * a.ii), (T)0);
-    } else if constexpr (IO == 2) {
-      // Z_i = (X_i + conj X_{L-i}) + i (X_i - conj X_{L-i}) W_n^{-i};  Im X_0, Im X_L dropped
-      cpx<T> xk = ld_cpx<T>(in, base + (long long)i * a.ii);
-      cpx<T> xm = ld_cpx<T>(in, base + (long long)(half_n - i) * a.ii);
-      if (i == 0) {
-        xk.y = (T)0;
-        xm.y = (T)0;
-      }
-      cpx<T> s = mk(xk.x + xm.x, xk.y - xm.y);
-      cpx<T> d = mk(xk.x - xm.x, xk.y + xm.y);
-      cpx<T> w = ldg_c(a.rtw + i);
-      cpx<T> dw = mk(d.x * w.x + d.y * w.y, d.y * w.x - d.x * w.y);  // d * conj(w)
-      return mk(s.x - dw.y, s.y + dw.x);                           // s + i dw
-    } else {  // IO == 4: Hermitian expansion of the half spectrum to n points
-      const bool mirror = i > half_n;
-      cpx<T> v = ld_cpx<T>(in, base + (long long)(mirror ? n - i : i) * a.ii);
-      if (mirror) v.y = -v.y;
-      if (i == 0 || ((n & 1) == 0 && i == half_n)) v.y = (T)0;
-      return v;
-    }
+FFB_HD void real_post_pair(const cpx<T> *z, cpx<T> *x, int L, int k, const cpx<T> *rtw) {
+  auto post = [&](cpx<T> zk, cpx<T> zm, int kk) {
+    cpx<T> ev = mk((zk.x + zm.x) * (T)0.5, (zk.y - zm.y) * (T)0.5);
+    cpx<T> od = mk((zk.y + zm.y) * (T)0.5, (zm.x - zk.x) * (T)0.5);
+    return ev + cmul(ldg_c(rtw + kk), od);
   };
-
-  // ---------------------------------------------------------------- load
-  {
-    const int total = W * L;
-    const int nl = (IO == 1 || IO == 2) ? half_n : n;  // Bluestein logical length
-    for (int e = t0; e < total; e += nt) {
-      int w, i;
-      split_elem(e, W, L, a.wfast, a.wdiv, a.ldiv, w, i);
-      const long long g = g0 + w;
-      cpx<T> v = mk((T)0, (T)0);
-      if constexpr (KIND == 0) {
-        if (g < a.G) v = core_input(g, i);
-        sm[w * Lp + Swz<T>::phys(dit_position(i, a.core))] = v;
-      } else if constexpr (KIND == 1) {
-        if (g < a.G && i < nl) v = cmul(core_input(g, i), ldg_c(a.chirp + i));
-        sm[w * Lp + Swz<T>::phys(i)] = v;
-      } else {  // Rader: a[q] = x[g^-q], q < L = p - 1
-        if (g < a.G) v = core_input(g, ldg_v(a.perm_in + i));
-        sm[w * Lp + Swz<T>::phys(i)] = v;
-      }
-    }
-    if constexpr (KIND == 2) {
-      for (int w = t0; w < W; w += nt) {
-        const long long g = g0 + w;
-        sm[w * Lp + Lp - G] = (g < a.G) ? core_input(g, 0) : mk((T)0, (T)0);  // x0
-      }
-    }
-  }
-  x.sync();
-
-  // ---------------------------------------------------------------- core
-  auto sync = [&]() { x.sync(); };
-  x.per_slot(W, [&](int slot, int tid, int tpt) {
-    cpx<T> *buf = sm + slot * Lp;
-    if constexpr (KIND == 0) {
-      run_dit<T>(buf, a.core, tid, tpt, a.tw, a.inv != 0, sync);
-    } else {
-      run_dif<T>(buf, a.core, tid, tpt, a.tw, false, sync);
-      for (int p = tid; p < L; p += tpt) {
-        cpx<T> v = buf[Swz<T>::phys(p)];
-        if constexpr (KIND == 2) {
-          if (p == 0) buf[Lp - G + 1] = v + buf[Lp - G];  // X0 = x0 + sum_q a[q]
-        }
-        buf[Swz<T>::phys(p)] = cmul(v, ldg_c(a.kern + p));
-      }
-      sync();
-      run_dit<T>(buf, a.core2, tid, tpt, a.tw, true, sync);
-    }
-  });
-
-  // Four-step column passes multiply output k of transform g by W_N^{g k}
-  // (forward sign; conjugated for the inverse), g*k < N < 2^31.
-  auto post_twiddle = [&](cpx<T> v, long long g, int k) -> cpx<T> {
-    if (!a.post_twiddle) return v;
-    const uint32_t m = (uint32_t)(g * (long long)k);
-    const uint32_t hi = fdiv(m, a.ptw_div);
-    const uint32_t lo = m - hi * a.ptw_div.d;
-    cpx<T> t = cmul(ldg_c(a.ptw_hi + hi), ldg_c(a.ptw_lo + lo));
-    if (a.inv) t.y = -t.y;
-    return cmul(v, t);
-  };
-
-  // Natural-order output element k of the core's transform in slot w.
-  auto out_elem = [&](int w, int k) -> cpx<T> {
-    const cpx<T> *bw = sm + w * Lp;
-    if constexpr (KIND == 0) {
-      return bw[Swz<T>::phys(k)];
-    } else if constexpr (KIND == 1) {
-      return cmul(bw[Swz<T>::phys(k)], ldg_c(a.chirp + k));
-    } else {
-      if (k == 0) return bw[Lp - G + 1];
-      const int q = ldg_v(a.perm_in + L + k);  // log_g(k)
-      return bw[Lp - G] + bw[Swz<T>::phys(q)];
-    }
-  };
-
-  // ---------------------------------------------------------------- store
-  if constexpr (IO == 0) {
-    if constexpr (KIND == 2) {
-      // X[g^q] = x0 + conv[q] (scatter by q keeps the reads conflict-free);  X[0] = x0 + sum
-      const int total = W * L;
-      for (int e = t0; e < total; e += nt) {
-        int w, q;
-        split_elem(e, W, L, a.wfast, a.wdiv, a.ldiv, w, q);
-        const long long g = g0 + w;
-        if (g < a.G) {
-          const cpx<T> *bw = sm + w * Lp;
-          const int k = ldg_v(a.perm_out + q);
-          st_cpx<T>(out, g * a.og + (long long)k * a.ok, post_twiddle(bw[Lp - G] + bw[Swz<T>::phys(q)], g, k));
-        }
-      }
-      for (int w = t0; w < W; w += nt) {
-        const long long g = g0 + w;
-        if (g < a.G) st_cpx<T>(out, g * a.og, sm[w * Lp + Lp - G + 1]);
-      }
-    } else {
-      const int nout = KIND == 1 ? n : L;
-      const int total = W * nout;
-      for (int e = t0; e < total; e += nt) {
-        int w, k;
-        split_elem(e, W, nout, a.wfast, a.wdiv, KIND == 1 ? a.ndiv : a.ldiv, w, k);
-        const long long g = g0 + w;
-        if (g < a.G) st_cpx<T>(out, g * a.og + (long long)k * a.ok, post_twiddle(out_elem(w, k), g, k));
-      }
-    }
-  } else if constexpr (IO == 1) {
-    // X_k = E_k + W_n^k O_k,  E = (Z_k + conj Z_{L-k})/2,  O = -i (Z_k - conj Z_{L-k})/2
-    const int nbins = half_n + 1;
-    const int total = W * nbins;
-    for (int e = t0; e < total; e += nt) {
-      int w, k;
-      if (a.wfast) {
-        k = e / W;
-        w = e - k * W;
-      } else {
-        w = e / nbins;
-        k = e - w * nbins;
-      }
-      const long long g = g0 + w;
-      if (g >= a.G) continue;
-      cpx<T> zk = out_elem(w, k == half_n ? 0 : k);
-      cpx<T> zm = out_elem(w, k == 0 ? 0 : half_n - k);
-      cpx<T> ev = mk((zk.x + zm.x) * (T)0.5, (zk.y - zm.y) * (T)0.5);
-      cpx<T> od = mk((zk.y + zm.y) * (T)0.5, (zm.x - zk.x) * (T)0.5);
-      st_cpx<T>(out, g * a.og + (long long)k * a.ok, ev + cmul(ldg_c(a.rtw + k), od));
-    }
-  } else if constexpr (IO == 2) {
-    // x_2j = Re z_j, x_2j+1 = Im z_j
-    const int total = W * half_n;
-    for (int e = t0; e < total; e += nt) {
-      int w, j;
-      split_elem(e, W, half_n, a.wfast, a.wdiv, a.hdiv, w, j);
-      const long long g = g0 + w;
-      if (g >= a.G) continue;
-      cpx<T> z = out_elem(w, j);
-      st_real<T>(out, g * a.og + (long long)(2 * j) * a.ok, z.x);
-      st_real<T>(out, g * a.og + (long long)(2 * j + 1) * a.ok, z.y);
-    }
-  } else if constexpr (IO == 3) {
-    const int nbins = half_n + 1;
-    const int total = W * nbins;
-    for (int e = t0; e < total; e += nt) {
-      int w, k;
-      if (a.wfast) {
-        k = e / W;
-        w = e - k * W;
-      } else {
-        w = e / nbins;
-        k = e - w * nbins;
-      }
-      const long long g = g0 + w;
-      if (g < a.G) st_cpx<T>(out, g * a.og + (long long)k * a.ok, out_elem(w, k));
-    }
-  } else {  // IO == 4
-    const int total = W * n;
-    for (int e = t0; e < total; e += nt) {
-      int w, k;
-      split_elem(e, W, n, a.wfast, a.wdiv, a.ndiv, w, k);
-      const long long g = g0 + w;
-      if (g < a.G) st_real<T>(out, g * a.og + (long long)k * a.ok, out_elem(w, k).x);
-    }
-  }
+  const int m = L - k;
+  cpx<T> zk = z[k == 0 ? 0 : k];
+  cpx<T> zm = z[k == 0 ? 0 : m];
+  cpx<T> xk = post(zk, zm, k);
+  cpx<T> xm = post(zm, zk, m);  // k = 0: X_L from Z_0
+  x[k] = xk;
+  if (m != k) x[m] = xm;
 }
 
 template <typename T>
-struct TileBounds {
-  // float kernels run up to 512 threads (128 registers); double up to 256 (255)
-  static constexpr int kMaxThreads = sizeof(T) == 4 ? 512 : 256;
-};
-
-template <typename T, int KIND, int IO>
-__global__ void __launch_bounds__(TileBounds<T>::kMaxThreads) k_tile(const TileArgs<T> a) {
-  extern __shared__ __align__(16) unsigned char smraw[];
-  DevX x{a.tpt};
-  tile_body<T, KIND, IO>(a, (long long)blockIdx.x, (long long)blockIdx.y, reinterpret_cast<cpx<T> *>(smraw), x);
-}
-
-#ifndef FFB_HOST_EMULATION
-template <typename T, int KIND, int IO>
-cudaError_t launch_one(const TileArgs<T> &a, size_t smem, cudaStream_t s) {
-  static bool configured = false;
-  if (!configured) {
-    cudaError_t e = cudaFuncSetAttribute(k_tile<T, KIND, IO>, cudaFuncAttributeMaxDynamicSharedMemorySize, 232448);
-    if (e != cudaSuccess) return e;
-    configured = true;
+FFB_HD void real_pre_one(const cpx<T> *x, cpx<T> *z, int L, int k, const cpx<T> *rtw) {
+  cpx<T> xk = x[k], xm = x[L - k];
+  if (k == 0) {
+    xk.y = (T)0;
+    xm.y = (T)0;
   }
-  dim3 grid((unsigned)((a.G + a.W - 1) / a.W), (unsigned)a.nbatch, 1);
-  dim3 block((unsigned)(a.W * a.tpt), 1, 1);
-  k_tile<T, KIND, IO><<<grid, block, smem, s>>>(a);
-  return cudaGetLastError();
+  cpx<T> s = mk(xk.x + xm.x, xk.y - xm.y);
+  cpx<T> d = mk(xk.x - xm.x, xk.y + xm.y);
+  cpx<T> w = ldg_c(rtw + k);
+  cpx<T> dw = mk(d.x * w.x + d.y * w.y, d.y * w.x - d.x * w.y);
+  z[k] = mk(s.x - dw.y, s.y + dw.x);
 }
-#else
-template <typename T, int KIND, int IO>
-cudaError_t launch_one(const TileArgs<T> &a, size_t smem, cudaStream_t) {
-  std::vector<unsigned char> buf(smem + 64);
-  cpx<T> *sm = reinterpret_cast<cpx<T> *>(buf.data());
-  const long long tiles = (a.G + a.W - 1) / a.W;
-  HostX x;
-  for (long long by = 0; by < a.nbatch; ++by)
-    for (long long bx = 0; bx < tiles; ++bx) {
-      std::memset(buf.data(), 0xff, buf.size());  // poison: unwritten positions show up as NaN
-      tile_body<T, KIND, IO>(a, bx, by, sm, x);
-    }
-  return cudaSuccess;
+
+template <typename T>
+__global__ void k_real_post(const cpx<T> *z, cpx<T> *x, long long zdist, long long xdist, int L,
+                            const cpx<T> *rtw) {
+  const long long b = blockIdx.y;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k <= L / 2; k += gridDim.x * blockDim.x)
+    real_post_pair<T>(z + b * zdist, x + b * xdist, L, k, rtw);
 }
-#endif
+
+template <typename T>
+__global__ void k_real_pre(const cpx<T> *x, cpx<T> *z, long long xdist, long long zdist, int L, const cpx<T> *rtw) {
+  const long long b = blockIdx.y;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < L; k += gridDim.x * blockDim.x)
+    real_pre_one<T>(x + b * xdist, z + b * zdist, L, k, rtw);
+}
 
 }  // namespace
 
 template <typename T>
+cudaError_t launch_real_post(const cpx<T> *z, cpx<T> *x, long long batch, long long zdist, long long xdist, int L,
+                             const cpx<T> *rtw, cudaStream_t s) {
+#ifndef FFB_HOST_EMULATION
+  const int threads = 256;
+  const int blocks = (int)std::min<long long>((L / 2 + threads) / threads, 1024);
+  k_real_post<T><<<dim3(blocks, (unsigned)batch), threads, 0, s>>>(z, x, zdist, xdist, L, rtw);
+  return cudaGetLastError();
+#else
+  for (long long b = 0; b < batch; ++b)
+    for (int k = 0; k <= L / 2; ++k) real_post_pair<T>(z + b * zdist, x + b * xdist, L, k, rtw);
+  return cudaSuccess;
+#endif
+}
+
+template <typename T>
+cudaError_t launch_real_pre(const cpx<T> *x, cpx<T> *z, long long batch, long long xdist, long long zdist, int L,
+                            const cpx<T> *rtw, cudaStream_t s) {
+#ifndef FFB_HOST_EMULATION
+  const int threads = 256;
+  const int blocks = (int)std::min<long long>((L + threads - 1) / threads, 2048);
+  k_real_pre<T><<<dim3(blocks, (unsigned)batch), threads, 0, s>>>(x, z, xdist, zdist, L, rtw);
+  return cudaGetLastError();
+#else
+  for (long long b = 0; b < batch; ++b)
+    for (int k = 0; k < L; ++k) real_pre_one<T>(x + b * xdist, z + b * zdist, L, k, rtw);
+  return cudaSuccess;
+#endif
+}
+
+template cudaError_t launch_real_post<float>(const cpx<float> *, cpx<float> *, long long, long long, long long, int,
+                                             const cpx<float> *, cudaStream_t);
+template cudaError_t launch_real_post<double>(const cpx<double> *, cpx<double> *, long long, long long, long long,
+                                              int, const cpx<double> *, cudaStream_t);
+template cudaError_t launch_real_pre<float>(const cpx<float> *, cpx<float> *, long long, long long, long long, int,
+                                            const cpx<float> *, cudaStream_t);
+template cudaError_t launch_real_pre<double>(const cpx<double> *, cpx<double> *, long long, long long, long long,
+                                             int, const cpx<double> *, cudaStream_t);
+
+template <typename T>
 cudaError_t launch_tile(const TileArgs<T> &a, CoreKind kind, IoKind io, size_t smem, cudaStream_t s) {
   const int k = (int)kind, o = (int)io;
-#define FFB_L(K, O) \
-  if (k == K && o == O) return launch_one<T, K, O>(a, smem, s);
-  FFB_L(0, 0) FFB_L(1, 0) FFB_L(2, 0)
-  FFB_L(0, 1) FFB_L(1, 1) FFB_L(2, 1)
-  FFB_L(0, 2) FFB_L(1, 2) FFB_L(2, 2)
-  FFB_L(0, 3) FFB_L(1, 3) FFB_L(2, 3)
-  FFB_L(0, 4) FFB_L(1, 4) FFB_L(2, 4)
-#undef FFB_L
+  if (a.pp && o == 0) {
+    switch (k) {
+      case 0: return tile::launch_pp<T, 0>(a, smem, s);
+      case 1: return tile::launch_pp<T, 1>(a, smem, s);
+      case 2: return tile::launch_pp<T, 2>(a, smem, s);
+      case 3: return tile::launch_pp<T, 3>(a, smem, s);
+      default: return cudaErrorInvalidValue;
+    }
+  }
+  if (k == 3 && o == 0) return tile::launch_one<T, 3, 0>(a, smem, s);
+  if (k == 0 && (o == 5 || o == 6)) return o == 5 ? tile::launch_one<T, 0, 5>(a, smem, s) : tile::launch_one<T, 0, 6>(a, smem, s);
+  if (k == 0) return tile::launch_group<T, 0>(a, o, smem, s);
+  if (k == 1) return tile::launch_group<T, 1>(a, o, smem, s);
+  if (k == 2) return tile::launch_group<T, 2>(a, o, smem, s);
   return cudaErrorInvalidValue;
 }
 

@@ -14,6 +14,7 @@ enum class CoreKind : int {
   Dit = 0,        // plain C2C: digit-reversed load, DIT stages, natural store
   Bluestein = 1,  // chirp * x zero-padded -> DIF fwd -> x kernel -> DIT inv -> x chirp
   Rader = 2,      // permuted load -> DIF fwd -> x kernel -> DIT inv -> permuted store + x0
+  Conv = 3,       // DIF fwd -> x kernel (per transform: kern + g * kern_stride) -> DIT inv
 };
 
 // How the pass reads its input and writes its output.
@@ -23,6 +24,8 @@ enum class IoKind : int {
   C2R = 2,  // half spectrum in (L+1 bins), real out (2L reals)
   R2CFull = 3,  // real in, complex core of length n (imag 0), first n/2+1 bins out
   C2RFull = 4,  // half spectrum in, Hermitian-expanded core of length n, real part out
+  PackC2C = 5,    // real pairs in (z_i = in[i*ii] + i in[i*ii + 1]), complex out
+  C2CUnpack = 6,  // complex in, real pairs out (out[k*ok] = Re z_k, out[k*ok + 1] = Im z_k)
 };
 
 // One pass = nbatch x G independent transforms, W of them per CTA.
@@ -60,7 +63,30 @@ struct TileArgs {
   FastDiv wdiv;  // / W
   FastDiv ndiv;  // / n
   FastDiv hdiv;  // / (n / 2)
+  // Bluestein chirp on a Dit core's load (chirp_mode 1) or store (2): element
+  // e of transform g is logical index j = e*cj_e + g*cj_g, live while j < n.
+  int chirp_mode;
+  long long cj_e, cj_g;
+  // Conv cores: transform g multiplies by kern + g * kern_stride.
+  long long kern_stride;
+  // 1: Stockham ping-pong path (C2C passes whose two buffers fit): the first
+  // stage reads global memory and the last writes it directly; convolution
+  // kernels are then in natural order.  0: in-place DIT/DIF path.
+  int pp;
 };
+
+// Real-transform pre/post processing between the passes of a multi-pass
+// R2C / C2R (L = n/2 complex points per transform, rtw[k] = W_n^k, k <= L):
+//   post: X_k = (Z_k + conj Z_{L-k})/2 - i W_n^k (Z_k - conj Z_{L-k})/2, k = 0..L
+//         (in place allowed: z and x may alias with zdist == xdist)
+//   pre:  Z_k = (X_k + conj X_{L-k}) + i W_n^-k (X_k - conj X_{L-k}), k < L,
+//         Im X_0 and Im X_L ignored
+template <typename T>
+cudaError_t launch_real_post(const cpx<T> *z, cpx<T> *x, long long batch, long long zdist, long long xdist, int L,
+                             const cpx<T> *rtw, cudaStream_t stream);
+template <typename T>
+cudaError_t launch_real_pre(const cpx<T> *x, cpx<T> *z, long long batch, long long xdist, long long zdist, int L,
+                            const cpx<T> *rtw, cudaStream_t stream);
 
 template <typename T>
 cudaError_t launch_tile(const TileArgs<T> &a, CoreKind kind, IoKind io, size_t smem_bytes, cudaStream_t stream);

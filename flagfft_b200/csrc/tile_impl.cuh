@@ -1,0 +1,528 @@
+// On-chip FFT passes for sm_100a.
+//
+// One kernel template covers every pass that keeps whole transforms in shared
+// memory: contiguous rows (1-D batches, 2-D rows), strided column tiles (2-D
+// columns, four-step column and row passes), the fused Bluestein and Rader
+// chains, and the fused real-to-complex / complex-to-real packing.  Each CTA
+// holds W transforms; every element crosses HBM once on the way in and once on
+// the way out.
+//
+// The body (tile_body) is written once against an execution policy: DevX runs
+// it as a CUDA thread block; HostX runs the identical code sequentially on the
+// CPU with one "thread" and no-op barriers (built only with
+// FFB_HOST_EMULATION, for host-side checks of the index arithmetic; never part
+// of libflagfft.so).  Sequential execution is exact because every phase's
+// iterations touch disjoint shared-memory positions.
+#pragma once
+
+#include "kernels.cuh"
+
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+namespace ffb {
+namespace tile {
+
+template <typename T>
+FFB_HD cpx<T> ld_cpx(const void *base, long long idx) {
+  return ldg_c(reinterpret_cast<const cpx<T> *>(base) + idx);
+}
+template <typename T>
+FFB_HD T ld_real(const void *base, long long idx) {
+  return ldg_v(reinterpret_cast<const T *>(base) + idx);
+}
+template <typename T>
+FFB_HD void st_cpx(void *base, long long idx, cpx<T> v) {
+  reinterpret_cast<cpx<T> *>(base)[idx] = v;
+}
+template <typename T>
+FFB_HD void st_real(void *base, long long idx, T v) {
+  reinterpret_cast<T *>(base)[idx] = v;
+}
+
+// CUDA thread block.
+struct DevX {
+  int tpt;
+  FFB_HD int tid() const {
+#ifdef __CUDA_ARCH__
+    return threadIdx.x;
+#else
+    return 0;
+#endif
+  }
+  FFB_HD int nthreads() const {
+#ifdef __CUDA_ARCH__
+    return blockDim.x;
+#else
+    return 1;
+#endif
+  }
+  FFB_HD void sync() const {
+#ifdef __CUDA_ARCH__
+    __syncthreads();
+#endif
+  }
+  int wfast;
+  // Runs f(slot, tid-in-slot, threads-per-slot) for this thread's transform.
+  // Column tiles put consecutive transforms on consecutive threads.
+  template <class F>
+  FFB_HD void per_slot(int W, F f) const {
+    const int t = tid();
+    if (wfast) {
+      const int slot = t % W;
+      f(slot, t / W, tpt);
+    } else {
+      const int slot = t / tpt;
+      f(slot, t - slot * tpt, tpt);
+    }
+  }
+};
+
+// Sequential host execution of one block.
+struct HostX {
+  FFB_HD int tid() const { return 0; }
+  FFB_HD int nthreads() const { return 1; }
+  FFB_HD void sync() const {}
+  template <class F>
+  FFB_HD void per_slot(int W, F f) const {
+    for (int s = 0; s < W; ++s) f(s, 0, 1);
+  }
+};
+
+// Splits a flat element counter e over (transform w, element i) of a CTA tile.
+FFB_HD void split_elem(int e, int W, int Lx, int wfast, const FastDiv &wdiv, const FastDiv &ldiv, int &w, int &i) {
+  if (wfast) {
+    i = (int)fdiv((uint32_t)e, wdiv);
+    w = e - i * W;
+  } else {
+    w = (int)fdiv((uint32_t)e, ldiv);
+    i = e - w * Lx;
+  }
+}
+
+template <typename T, int KIND, int IO, class X>
+FFB_HD void tile_body(const TileArgs<T> &a, long long bx, long long by, cpx<T> *sm, const X &x) {
+  constexpr int G = Swz<T>::G;
+  const int L = a.core.L;                // core (buffer) length
+  const int Lp = Swz<T>::padded(L) + G;  // + a spare group: Rader's x0 / X0 slots
+  const int W = a.W;
+  const long long b = by;
+  const long long g0 = bx * W;
+  constexpr bool real_in = IO == 1 || IO == 3 || IO == 5;
+  constexpr bool real_out = IO == 2 || IO == 4 || IO == 6;
+  const void *in = reinterpret_cast<const unsigned char *>(a.in) +
+                   b * a.ib * (long long)(real_in ? sizeof(T) : sizeof(cpx<T>));
+  void *out = reinterpret_cast<unsigned char *>(a.out) + b * a.ob * (long long)(real_out ? sizeof(T) : sizeof(cpx<T>));
+  const int n = a.n;
+  const int half_n = n / 2;  // real transforms: n reals, half_n + 1 bins
+  const int t0 = x.tid(), nt = x.nthreads();
+
+  // Logical input element i of the core's transform g.
+  auto core_input = [&](long long g, int i) -> cpx<T> {
+    const long long base = g * a.ig;
+    if constexpr (IO == 0 || IO == 6) {
+      return ld_cpx<T>(in, base + (long long)i * a.ii);
+    } else if constexpr (IO == 1 || IO == 5) {  // z_i = x_2i + i x_2i+1: adjacent reals at i*ii
+      T re = ld_real<T>(in, base + (long long)i * a.ii);
+      T im = ld_real<T>(in, base + (long long)i * a.ii + 1);
+      return mk(re, im);
+    } else if constexpr (IO == 3) {  // real x_i, imaginary part 0
+      return mk(ld_real<T>(in, base + (long long)i * a.ii), (T)0);
+    } else if constexpr (IO == 2) {
+      // Z_i = (X_i + conj X_{L-i}) + i (X_i - conj X_{L-i}) W_n^{-i};  Im X_0, Im X_L dropped
+      cpx<T> xk = ld_cpx<T>(in, base + (long long)i * a.ii);
+      cpx<T> xm = ld_cpx<T>(in, base + (long long)(half_n - i) * a.ii);
+      if (i == 0) {
+        xk.y = (T)0;
+        xm.y = (T)0;
+      }
+      cpx<T> s = mk(xk.x + xm.x, xk.y - xm.y);
+      cpx<T> d = mk(xk.x - xm.x, xk.y + xm.y);
+      cpx<T> w = ldg_c(a.rtw + i);
+      cpx<T> dw = mk(d.x * w.x + d.y * w.y, d.y * w.x - d.x * w.y);  // d * conj(w)
+      return mk(s.x - dw.y, s.y + dw.x);                           // s + i dw
+    } else {  // IO == 4: Hermitian expansion of the half spectrum to n points
+      const bool mirror = i > half_n;
+      cpx<T> v = ld_cpx<T>(in, base + (long long)(mirror ? n - i : i) * a.ii);
+      if (mirror) v.y = -v.y;
+      if (i == 0 || ((n & 1) == 0 && i == half_n)) v.y = (T)0;
+      return v;
+    }
+  };
+
+  // ---------------------------------------------------------------- load
+  {
+    const int total = W * L;
+    const int nl = (IO == 1 || IO == 2) ? half_n : n;  // Bluestein logical length
+    for (int e = t0; e < total; e += nt) {
+      int w, i;
+      split_elem(e, W, L, a.wfast, a.wdiv, a.ldiv, w, i);
+      const long long g = g0 + w;
+      cpx<T> v = mk((T)0, (T)0);
+      if constexpr (KIND == 0) {
+        if (a.chirp_mode == 1) {
+          const long long j = (long long)i * a.cj_e + g * a.cj_g;
+          if (g < a.G && j < n) v = cmul(core_input(g, i), ldg_c(a.chirp + j));
+        } else if (g < a.G) {
+          v = core_input(g, i);
+        }
+        sm[w * Lp + Swz<T>::phys(dit_position(i, a.core))] = v;
+      } else if constexpr (KIND == 3) {
+        if (g < a.G) v = core_input(g, i);
+        sm[w * Lp + Swz<T>::phys(i)] = v;
+      } else if constexpr (KIND == 1) {
+        if (g < a.G && i < nl) v = cmul(core_input(g, i), ldg_c(a.chirp + i));
+        sm[w * Lp + Swz<T>::phys(i)] = v;
+      } else {  // Rader: a[q] = x[g^-q], q < L = p - 1
+        if (g < a.G) v = core_input(g, ldg_v(a.perm_in + i));
+        sm[w * Lp + Swz<T>::phys(i)] = v;
+      }
+    }
+    if constexpr (KIND == 2) {
+      for (int w = t0; w < W; w += nt) {
+        const long long g = g0 + w;
+        sm[w * Lp + Lp - G] = (g < a.G) ? core_input(g, 0) : mk((T)0, (T)0);  // x0
+      }
+    }
+  }
+  x.sync();
+
+  // ---------------------------------------------------------------- core
+  auto sync = [&]() { x.sync(); };
+  x.per_slot(W, [&](int slot, int tid, int tpt) {
+    cpx<T> *buf = sm + slot * Lp;
+    if constexpr (KIND == 0) {
+      run_dit<T>(buf, a.core, tid, tpt, a.tw, a.inv != 0, sync);
+    } else {
+      run_dif<T>(buf, a.core, tid, tpt, a.tw, false, sync);
+      const cpx<T> *kern = a.kern;
+      if constexpr (KIND == 3) kern += (g0 + slot < a.G ? g0 + slot : 0) * a.kern_stride;
+      for (int p = tid; p < L; p += tpt) {
+        cpx<T> v = buf[Swz<T>::phys(p)];
+        if constexpr (KIND == 2) {
+          if (p == 0) buf[Lp - G + 1] = v + buf[Lp - G];  // X0 = x0 + sum_q a[q]
+        }
+        buf[Swz<T>::phys(p)] = cmul(v, ldg_c(kern + p));
+      }
+      sync();
+      run_dit<T>(buf, a.core2, tid, tpt, a.tw, true, sync);
+    }
+  });
+
+  // Four-step column passes multiply output k of transform g by W_N^{g k}
+  // (forward sign; conjugated for the inverse), g*k < N < 2^31.
+  auto post_twiddle = [&](cpx<T> v, long long g, int k) -> cpx<T> {
+    if (!a.post_twiddle) return v;
+    const uint32_t m = (uint32_t)(g * (long long)k);
+    const uint32_t hi = fdiv(m, a.ptw_div);
+    const uint32_t lo = m - hi * a.ptw_div.d;
+    cpx<T> t = cmul(ldg_c(a.ptw_hi + hi), ldg_c(a.ptw_lo + lo));
+    if (a.inv) t.y = -t.y;
+    return cmul(v, t);
+  };
+
+  // Natural-order output element k of the core's transform in slot w.
+  auto out_elem = [&](int w, int k) -> cpx<T> {
+    const cpx<T> *bw = sm + w * Lp;
+    if constexpr (KIND == 0 || KIND == 3) {
+      return bw[Swz<T>::phys(k)];
+    } else if constexpr (KIND == 1) {
+      return cmul(bw[Swz<T>::phys(k)], ldg_c(a.chirp + k));
+    } else {
+      if (k == 0) return bw[Lp - G + 1];
+      const int q = ldg_v(a.perm_in + L + k);  // log_g(k)
+      return bw[Lp - G] + bw[Swz<T>::phys(q)];
+    }
+  };
+
+  // ---------------------------------------------------------------- store
+  if constexpr (IO == 0) {
+    if constexpr (KIND == 2) {
+      // X[g^q] = x0 + conv[q] (scatter by q keeps the reads conflict-free);  X[0] = x0 + sum
+      const int total = W * L;
+      for (int e = t0; e < total; e += nt) {
+        int w, q;
+        split_elem(e, W, L, a.wfast, a.wdiv, a.ldiv, w, q);
+        const long long g = g0 + w;
+        if (g < a.G) {
+          const cpx<T> *bw = sm + w * Lp;
+          const int k = ldg_v(a.perm_out + q);
+          st_cpx<T>(out, g * a.og + (long long)k * a.ok, post_twiddle(bw[Lp - G] + bw[Swz<T>::phys(q)], g, k));
+        }
+      }
+      for (int w = t0; w < W; w += nt) {
+        const long long g = g0 + w;
+        if (g < a.G) st_cpx<T>(out, g * a.og, sm[w * Lp + Lp - G + 1]);
+      }
+    } else {
+      const int nout = KIND == 1 ? n : L;
+      const int total = W * nout;
+      for (int e = t0; e < total; e += nt) {
+        int w, k;
+        split_elem(e, W, nout, a.wfast, a.wdiv, KIND == 1 ? a.ndiv : a.ldiv, w, k);
+        const long long g = g0 + w;
+        if (g >= a.G) continue;
+        cpx<T> v = out_elem(w, k);
+        if constexpr (KIND == 0) {
+          if (a.chirp_mode == 2) {  // Bluestein output: y_j = conv_j * chirp_j, j < n
+            const long long j = (long long)k * a.cj_e + g * a.cj_g;
+            if (j >= n) continue;
+            v = cmul(v, ldg_c(a.chirp + j));
+          }
+        }
+        st_cpx<T>(out, g * a.og + (long long)k * a.ok, post_twiddle(v, g, k));
+      }
+    }
+  } else if constexpr (IO == 1) {
+    // X_k = E_k + W_n^k O_k,  E = (Z_k + conj Z_{L-k})/2,  O = -i (Z_k - conj Z_{L-k})/2
+    const int nbins = half_n + 1;
+    const int total = W * nbins;
+    for (int e = t0; e < total; e += nt) {
+      int w, k;
+      if (a.wfast) {
+        k = e / W;
+        w = e - k * W;
+      } else {
+        w = e / nbins;
+        k = e - w * nbins;
+      }
+      const long long g = g0 + w;
+      if (g >= a.G) continue;
+      cpx<T> zk = out_elem(w, k == half_n ? 0 : k);
+      cpx<T> zm = out_elem(w, k == 0 ? 0 : half_n - k);
+      cpx<T> ev = mk((zk.x + zm.x) * (T)0.5, (zk.y - zm.y) * (T)0.5);
+      cpx<T> od = mk((zk.y + zm.y) * (T)0.5, (zm.x - zk.x) * (T)0.5);
+      st_cpx<T>(out, g * a.og + (long long)k * a.ok, ev + cmul(ldg_c(a.rtw + k), od));
+    }
+  } else if constexpr (IO == 2 || IO == 6) {
+    // x_2j = Re z_j, x_2j+1 = Im z_j: adjacent reals at j*ok
+    const int cnt = IO == 2 ? half_n : L;
+    const int total = W * cnt;
+    for (int e = t0; e < total; e += nt) {
+      int w, j;
+      split_elem(e, W, cnt, a.wfast, a.wdiv, IO == 2 ? a.hdiv : a.ldiv, w, j);
+      const long long g = g0 + w;
+      if (g >= a.G) continue;
+      cpx<T> z = out_elem(w, j);
+      st_real<T>(out, g * a.og + (long long)j * a.ok, z.x);
+      st_real<T>(out, g * a.og + (long long)j * a.ok + 1, z.y);
+    }
+  } else if constexpr (IO == 5) {
+    const int total = W * L;
+    for (int e = t0; e < total; e += nt) {
+      int w, k;
+      split_elem(e, W, L, a.wfast, a.wdiv, a.ldiv, w, k);
+      const long long g = g0 + w;
+      if (g < a.G) st_cpx<T>(out, g * a.og + (long long)k * a.ok, post_twiddle(out_elem(w, k), g, k));
+    }
+  } else if constexpr (IO == 3) {
+    const int nbins = half_n + 1;
+    const int total = W * nbins;
+    for (int e = t0; e < total; e += nt) {
+      int w, k;
+      if (a.wfast) {
+        k = e / W;
+        w = e - k * W;
+      } else {
+        w = e / nbins;
+        k = e - w * nbins;
+      }
+      const long long g = g0 + w;
+      if (g < a.G) st_cpx<T>(out, g * a.og + (long long)k * a.ok, out_elem(w, k));
+    }
+  } else {  // IO == 4
+    const int total = W * n;
+    for (int e = t0; e < total; e += nt) {
+      int w, k;
+      split_elem(e, W, n, a.wfast, a.wdiv, a.ndiv, w, k);
+      const long long g = g0 + w;
+      if (g < a.G) st_real<T>(out, g * a.og + (long long)k * a.ok, out_elem(w, k).x);
+    }
+  }
+}
+
+// Stockham ping-pong pass for C2C tiles (first stage reads global memory,
+// last stage writes it).  Dead slots (g >= G) run on a clamped transform so
+// every thread passes the same barriers, and store nothing.
+template <typename T, int KIND, class X>
+FFB_HD void tile_body_pp(const TileArgs<T> &a, long long bx, long long by, cpx<T> *sm, const X &x) {
+  const int L = a.core.L;
+  const int Lq = pp_size(L);
+  const int W = a.W;
+  const long long g0 = bx * W;
+  const cpx<T> *in = reinterpret_cast<const cpx<T> *>(a.in) + by * a.ib;
+  cpx<T> *out = reinterpret_cast<cpx<T> *>(a.out) + by * a.ob;
+  const int n = a.n;
+  auto sync = [&]() { x.sync(); };
+  x.per_slot(W, [&](int slot, int tid, int tpt) {
+    const long long g = g0 + slot;
+    const bool live = g < a.G;
+    const long long gc = live ? g : a.G - 1;
+    cpx<T> *const b0 = sm + slot * 2 * Lq, *const b1 = b0 + Lq;
+    const cpx<T> *xin = in + gc * a.ig;
+    cpx<T> *yout = out + gc * a.og;
+    auto post_twiddle = [&](cpx<T> v, int k) -> cpx<T> {
+      if (!a.post_twiddle) return v;
+      const uint32_t m = (uint32_t)(gc * (long long)k);
+      const uint32_t hi = fdiv(m, a.ptw_div);
+      const uint32_t lo = m - hi * a.ptw_div.d;
+      cpx<T> t = cmul(ldg_c(a.ptw_hi + hi), ldg_c(a.ptw_lo + lo));
+      if (a.inv) t.y = -t.y;
+      return cmul(v, t);
+    };
+    if constexpr (KIND == 0) {
+      // chirp_mode 1 / 2: Bluestein chirp on the load / store of a multi-pass chain
+      auto src = [&](int p) -> cpx<T> {
+        if (a.chirp_mode == 1) {
+          const long long j = (long long)p * a.cj_e + gc * a.cj_g;
+          return j < n ? cmul(ldg_c(xin + (long long)p * a.ii), ldg_c(a.chirp + j)) : mk((T)0, (T)0);
+        }
+        return ldg_c(xin + (long long)p * a.ii);
+      };
+      auto dst = [&](int p, cpx<T> v) {
+        if (!live) return;
+        if (a.chirp_mode == 2) {
+          const long long j = (long long)p * a.cj_e + gc * a.cj_g;
+          if (j < n) yout[(long long)p * a.ok] = cmul(v, ldg_c(a.chirp + j));
+          return;
+        }
+        yout[(long long)p * a.ok] = post_twiddle(v, p);
+      };
+      run_stockham<T>(a.core, b0, b1, tid, tpt, a.tw, a.inv != 0, src, dst, sync);
+    } else {
+      // forward FFT of the convolution input, kernel product into F, inverse FFT
+      const int S = a.core.nst;
+      cpx<T> *const F = ((S - 1) & 1) ? b1 : b0;
+      cpx<T> *const G0 = ((S - 1) & 1) ? b0 : b1;
+      const cpx<T> *kern = a.kern;
+      if constexpr (KIND == 3) kern += gc * a.kern_stride;
+      cpx<T> x0 = mk((T)0, (T)0);
+      if constexpr (KIND == 2) x0 = ldg_c(xin);
+      auto src = [&](int p) -> cpx<T> {
+        if constexpr (KIND == 1) {
+          return p < n ? cmul(ldg_c(xin + (long long)p * a.ii), ldg_c(a.chirp + p)) : mk((T)0, (T)0);
+        } else if constexpr (KIND == 2) {
+          return ldg_c(xin + (long long)ldg_v(a.perm_in + p) * a.ii);
+        } else {
+          return ldg_c(xin + (long long)p * a.ii);
+        }
+      };
+      auto mid = [&](int p, cpx<T> v) {
+        if constexpr (KIND == 2) {
+          if (p == 0 && live) yout[0] = x0 + v;  // X0 = x0 + sum_q a[q]
+        }
+        F[pp_pos(p)] = cmul(v, ldg_c(kern + p));
+      };
+      run_stockham<T>(a.core, b0, b1, tid, tpt, a.tw, false, src, mid, sync);
+      sync();
+      PPRead<T> rd{F};
+      auto dst = [&](int p, cpx<T> v) {
+        if (!live) return;
+        if constexpr (KIND == 1) {
+          if (p < n) yout[(long long)p * a.ok] = cmul(v, ldg_c(a.chirp + p));
+        } else if constexpr (KIND == 2) {
+          yout[(long long)ldg_v(a.perm_out + p) * a.ok] = x0 + v;
+        } else {
+          yout[(long long)p * a.ok] = post_twiddle(v, p);
+        }
+      };
+      run_stockham<T>(a.core2, G0, F, tid, tpt, a.tw, true, rd, dst, sync);
+    }
+  });
+}
+
+template <typename T>
+struct TileBounds {
+  // float kernels run up to 512 threads (128 registers); double up to 256 (255)
+  static constexpr int kMaxThreads = sizeof(T) == 4 ? 512 : 256;
+};
+
+template <typename T, int KIND, int IO>
+__global__ void __launch_bounds__(TileBounds<T>::kMaxThreads) k_tile(const __grid_constant__ TileArgs<T> a) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  DevX x{a.tpt, a.wfast};
+  tile_body<T, KIND, IO>(a, (long long)blockIdx.x, (long long)blockIdx.y, reinterpret_cast<cpx<T> *>(smraw), x);
+}
+
+template <typename T, int KIND>
+__global__ void __launch_bounds__(TileBounds<T>::kMaxThreads) k_tile_pp(const __grid_constant__ TileArgs<T> a) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  DevX x{a.tpt, a.wfast};
+  tile_body_pp<T, KIND>(a, (long long)blockIdx.x, (long long)blockIdx.y, reinterpret_cast<cpx<T> *>(smraw), x);
+}
+
+#ifndef FFB_HOST_EMULATION
+template <typename T, int KIND, int IO>
+cudaError_t launch_one(const TileArgs<T> &a, size_t smem, cudaStream_t s) {
+  static bool configured = false;
+  if (!configured) {
+    cudaError_t e = cudaFuncSetAttribute(k_tile<T, KIND, IO>, cudaFuncAttributeMaxDynamicSharedMemorySize, 232448);
+    if (e != cudaSuccess) return e;
+    configured = true;
+  }
+  dim3 grid((unsigned)((a.G + a.W - 1) / a.W), (unsigned)a.nbatch, 1);
+  dim3 block((unsigned)(a.W * a.tpt), 1, 1);
+  k_tile<T, KIND, IO><<<grid, block, smem, s>>>(a);
+  return cudaGetLastError();
+}
+template <typename T, int KIND>
+cudaError_t launch_pp(const TileArgs<T> &a, size_t smem, cudaStream_t s) {
+  static bool configured = false;
+  if (!configured) {
+    cudaError_t e = cudaFuncSetAttribute(k_tile_pp<T, KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize, 232448);
+    if (e != cudaSuccess) return e;
+    configured = true;
+  }
+  dim3 grid((unsigned)((a.G + a.W - 1) / a.W), (unsigned)a.nbatch, 1);
+  dim3 block((unsigned)(a.W * a.tpt), 1, 1);
+  k_tile_pp<T, KIND><<<grid, block, smem, s>>>(a);
+  return cudaGetLastError();
+}
+#else
+template <typename T, int KIND>
+cudaError_t launch_pp(const TileArgs<T> &a, size_t smem, cudaStream_t) {
+  std::vector<unsigned char> buf(smem + 64);
+  cpx<T> *sm = reinterpret_cast<cpx<T> *>(buf.data());
+  const long long tiles = (a.G + a.W - 1) / a.W;
+  HostX x;
+  for (long long by = 0; by < a.nbatch; ++by)
+    for (long long bx = 0; bx < tiles; ++bx) {
+      std::memset(buf.data(), 0xff, buf.size());
+      tile_body_pp<T, KIND>(a, bx, by, sm, x);
+    }
+  return cudaSuccess;
+}
+
+template <typename T, int KIND, int IO>
+cudaError_t launch_one(const TileArgs<T> &a, size_t smem, cudaStream_t) {
+  std::vector<unsigned char> buf(smem + 64);
+  cpx<T> *sm = reinterpret_cast<cpx<T> *>(buf.data());
+  const long long tiles = (a.G + a.W - 1) / a.W;
+  HostX x;
+  for (long long by = 0; by < a.nbatch; ++by)
+    for (long long bx = 0; bx < tiles; ++bx) {
+      std::memset(buf.data(), 0xff, buf.size());  // poison: unwritten positions show up as NaN
+      tile_body<T, KIND, IO>(a, bx, by, sm, x);
+    }
+  return cudaSuccess;
+}
+#endif
+
+// Launches every IO variant of core kind K (one translation unit per
+// (precision, kind) keeps the compile parallel).
+template <typename T, int K>
+cudaError_t launch_group(const TileArgs<T> &a, int io, size_t smem, cudaStream_t s) {
+  switch (io) {
+    case 0: return launch_one<T, K, 0>(a, smem, s);
+    case 1: return launch_one<T, K, 1>(a, smem, s);
+    case 2: return launch_one<T, K, 2>(a, smem, s);
+    case 3: return launch_one<T, K, 3>(a, smem, s);
+    case 4: return launch_one<T, K, 4>(a, smem, s);
+    default: break;
+  }
+  return cudaErrorInvalidValue;
+}
+
+}  // namespace tile
+}  // namespace ffb
