@@ -512,4 +512,20 @@ FFB_HD void run_stockham(const Core &c, cpx<T> *b0, cpx<T> *b1, int tid, int nth
   }
 }
 
+// All stages of `c` shared -> shared: stage s reads buffer (s even ? src : oth)
+// and writes the other; every stage ends with a barrier.  The result is in
+// `src` when nst is even, in `oth` when odd.
+template <typename T, class Sync>
+FFB_HD void run_stockham_smem(const Core &c, cpx<T> *src, cpx<T> *oth, int tid, int nthr,
+                              const cpx<T> *__restrict__ tw, bool inv, Sync sync) {
+  for (int s = 0; s < c.nst; ++s) {
+    PPRead<T> rd{(s & 1) ? oth : src};
+    PPWrite<T> w{(s & 1) ? src : oth};
+#define FFB_SS(R) stockham_stage_r<R, T>(c, s, tid, nthr, tw, inv, rd, w)
+    FFB_RADIX_SWITCH(c.radix[s], FFB_SS)
+#undef FFB_SS
+    sync();
+  }
+}
+
 }  // namespace ffb

@@ -268,6 +268,12 @@ class Builder {
   Builder(Program &prog, Planner &planner) : prog_(prog), planner_(planner) {}
 
   static constexpr int kMaxThreads = sizeof(T) == 4 ? 512 : 256;
+  static constexpr int64_t kSMs = 148;
+
+  // Two ping-pong buffers of a length-L transform fit one CTA.
+  static bool pp_fits(int64_t L) {
+    return (2 * (size_t)pp_size((int)L) + 2) * sizeof(cpx<T>) <= 232448;
+  }
 
   // On-chip core for a complex transform node, if one exists.
   bool core_for(const NodePtr &node, CoreSpec &spec) const {
@@ -333,7 +339,7 @@ class Builder {
     const size_t limit = 232448;
     // Stockham ping-pong when two buffers of the transform fit (C2C passes);
     // the in-place DIT / DIF path otherwise.
-    const size_t pp_per = 2 * (size_t)pp_size((int)L) * sizeof(cpx<T>);
+    const size_t pp_per = (2 * (size_t)pp_size((int)L) + 2) * sizeof(cpx<T>);
     a.pp = (io == IoKind::C2C && L > 1 && pp_per <= limit) ? 1 : 0;
     if (spec.kind == CoreKind::Dit) {
       a.core = make_dit_core(L, spec.radices);
@@ -350,14 +356,16 @@ class Builder {
     a.wfast = strided ? 1 : 0;
     int tpt = choose_tpt(L, spec.radices);
     const size_t per = a.pp ? pp_per : tile_smem_per_transform<T>((int)L) + Swz<T>::G * sizeof(cpx<T>);
-    int64_t W;
-    if (strided) {
-      W = std::min<int64_t>({(int64_t)(limit / per), 8, G});
-    } else {
-      W = std::max<int64_t>(1, 256 / tpt);
-      W = std::min<int64_t>({W, (int64_t)(limit / per), G});
-      // keep at least ~2 CTAs per SM worth of work spread when the batch is small
-    }
+    // Transforms per CTA: about 256 threads' worth, within a shared-memory
+    // budget that leaves room for a second CTA per SM, and no more than keeps
+    // ~2 CTAs per SM busy; column tiles take at least 8 transforms so each
+    // row segment they read is 64-128 bytes.
+    const size_t budget = std::max<size_t>(per, 110 * 1024);
+    const int64_t w_thr = std::max<int64_t>(1, 256 / tpt);
+    const int64_t w_smem = std::max<int64_t>(1, (int64_t)(std::min(budget, limit) / per));
+    const int64_t w_par = std::max<int64_t>(1, (nbatch * G) / (2 * kSMs));
+    int64_t W = std::min<int64_t>({w_thr, w_smem, w_par, G});
+    if (strided) W = std::max<int64_t>(W, std::min<int64_t>({8, G, (int64_t)(limit / per)}));
     W = std::max<int64_t>(W, 1);
     if (W * tpt > kMaxThreads) tpt = std::max<int>(1, (int)(kMaxThreads / W));
     a.W = (int)W;
@@ -521,11 +529,33 @@ class Builder {
 // A length-n complex transform over `batch` rows (row distances idist / odist)
 // from `src` to `dst`; `ws` is a workspace of batch * (n or the Bluestein
 // convolution length) elements when the plan needs more than one pass.
+// On-chip policy ($FLAGFFT_ONCHIP_POLICY): "auto" keeps a transform in one
+// pass when its two Stockham buffers fit a CTA and otherwise prefers a
+// multi-pass lowering of the plan tree over the in-place single-pass one;
+// "inplace" keeps every transform that fits in place on chip; "multipass"
+// splits every tree that has a multi-pass lowering.
+static int onchip_policy() {
+  const char *v = std::getenv("FLAGFFT_ONCHIP_POLICY");
+  if (!v) return 0;
+  std::string s(v);
+  return s == "inplace" ? 1 : s == "multipass" ? 2 : 0;
+}
+
 template <typename T>
 void lower_c2c(Builder<T> &bld, Program &prog, const NodePtr &root, bool inverse, int64_t n, int64_t batch,
                long long idist, long long odist, Buf src, Buf dst) {
   CoreSpec spec;
-  if (bld.core_for(root, spec)) {
+  const bool onchip = bld.core_for(root, spec);
+  CoreSpec ca, cb;
+  const bool mp_four = root->kind == NodeKind::FourStep && bld.core_for(root->row, ca) && bld.core_for(root->col, cb);
+  const bool mp_blue = root->kind == NodeKind::Bluestein && root->child->kind == NodeKind::FourStep &&
+                       bld.core_for(root->child->row, ca) && bld.core_for(root->child->col, cb) &&
+                       ca.kind == CoreKind::Dit && cb.kind == CoreKind::Dit;
+  const int policy = onchip_policy();
+  const bool use_onchip =
+      onchip && (policy == 1 || (policy == 0 && (Builder<T>::pp_fits(spec.L) || !(mp_four || mp_blue))) ||
+                 (policy == 2 && !(mp_four || mp_blue)));
+  if (use_onchip) {
     bld.add_pass(spec, IoKind::C2C, inverse, 1, batch, 0, idist, 1, 0, odist, 1, src, dst, n);
     return;
   }

@@ -342,94 +342,128 @@ FFB_HD void tile_body(const TileArgs<T> &a, long long bx, long long by, cpx<T> *
   }
 }
 
-// Stockham ping-pong pass for C2C tiles (first stage reads global memory,
-// last stage writes it).  Dead slots (g >= G) run on a clamped transform so
-// every thread passes the same barriers, and store nothing.
+// Stockham ping-pong pass for C2C tiles.  A coalesced load phase fills
+// buffer 0 of every slot (natural order, chirp / permutation / zero padding
+// applied), all stages run shared -> shared (one code path per radix, warm in
+// the instruction cache after the first stage), and a coalesced store phase
+// writes the result (unchirp / scatter / four-step twiddle applied).  Slot
+// layout: two buffers of pp_size(L) plus two spare elements (Rader x0, X0).
 template <typename T, int KIND, class X>
 FFB_HD void tile_body_pp(const TileArgs<T> &a, long long bx, long long by, cpx<T> *sm, const X &x) {
   const int L = a.core.L;
   const int Lq = pp_size(L);
+  const int slot_len = 2 * Lq + 2;
   const int W = a.W;
   const long long g0 = bx * W;
   const cpx<T> *in = reinterpret_cast<const cpx<T> *>(a.in) + by * a.ib;
   cpx<T> *out = reinterpret_cast<cpx<T> *>(a.out) + by * a.ob;
   const int n = a.n;
+  const int t0 = x.tid(), nt = x.nthreads();
+
+  // ---- load
+  {
+    const int total = W * L;
+    for (int e = t0; e < total; e += nt) {
+      int w, i;
+      split_elem(e, W, L, a.wfast, a.wdiv, a.ldiv, w, i);
+      const long long g = g0 + w;
+      const long long gc = g < a.G ? g : a.G - 1;
+      const cpx<T> *xin = in + gc * a.ig;
+      cpx<T> v;
+      if constexpr (KIND == 0) {
+        if (a.chirp_mode == 1) {
+          const long long j = (long long)i * a.cj_e + gc * a.cj_g;
+          v = j < n ? cmul(ldg_c(xin + (long long)i * a.ii), ldg_c(a.chirp + j)) : mk((T)0, (T)0);
+        } else {
+          v = ldg_c(xin + (long long)i * a.ii);
+        }
+      } else if constexpr (KIND == 1) {
+        v = i < n ? cmul(ldg_c(xin + (long long)i * a.ii), ldg_c(a.chirp + i)) : mk((T)0, (T)0);
+      } else if constexpr (KIND == 2) {
+        v = ldg_c(xin + (long long)ldg_v(a.perm_in + i) * a.ii);
+      } else {
+        v = ldg_c(xin + (long long)i * a.ii);
+      }
+      sm[w * slot_len + pp_pos(i)] = v;
+    }
+    if constexpr (KIND == 2) {
+      for (int w = t0; w < W; w += nt) {
+        const long long g = g0 + w;
+        const long long gc = g < a.G ? g : a.G - 1;
+        sm[w * slot_len + 2 * Lq] = ldg_c(in + gc * a.ig);  // x0
+      }
+    }
+  }
+  x.sync();
+
+  // ---- stages
   auto sync = [&]() { x.sync(); };
   x.per_slot(W, [&](int slot, int tid, int tpt) {
-    const long long g = g0 + slot;
-    const bool live = g < a.G;
-    const long long gc = live ? g : a.G - 1;
-    cpx<T> *const b0 = sm + slot * 2 * Lq, *const b1 = b0 + Lq;
-    const cpx<T> *xin = in + gc * a.ig;
-    cpx<T> *yout = out + gc * a.og;
-    auto post_twiddle = [&](cpx<T> v, int k) -> cpx<T> {
-      if (!a.post_twiddle) return v;
-      const uint32_t m = (uint32_t)(gc * (long long)k);
-      const uint32_t hi = fdiv(m, a.ptw_div);
-      const uint32_t lo = m - hi * a.ptw_div.d;
-      cpx<T> t = cmul(ldg_c(a.ptw_hi + hi), ldg_c(a.ptw_lo + lo));
-      if (a.inv) t.y = -t.y;
-      return cmul(v, t);
-    };
-    if constexpr (KIND == 0) {
-      // chirp_mode 1 / 2: Bluestein chirp on the load / store of a multi-pass chain
-      auto src = [&](int p) -> cpx<T> {
-        if (a.chirp_mode == 1) {
-          const long long j = (long long)p * a.cj_e + gc * a.cj_g;
-          return j < n ? cmul(ldg_c(xin + (long long)p * a.ii), ldg_c(a.chirp + j)) : mk((T)0, (T)0);
-        }
-        return ldg_c(xin + (long long)p * a.ii);
-      };
-      auto dst = [&](int p, cpx<T> v) {
-        if (!live) return;
-        if (a.chirp_mode == 2) {
-          const long long j = (long long)p * a.cj_e + gc * a.cj_g;
-          if (j < n) yout[(long long)p * a.ok] = cmul(v, ldg_c(a.chirp + j));
-          return;
-        }
-        yout[(long long)p * a.ok] = post_twiddle(v, p);
-      };
-      run_stockham<T>(a.core, b0, b1, tid, tpt, a.tw, a.inv != 0, src, dst, sync);
-    } else {
-      // forward FFT of the convolution input, kernel product into F, inverse FFT
-      const int S = a.core.nst;
-      cpx<T> *const F = ((S - 1) & 1) ? b1 : b0;
-      cpx<T> *const G0 = ((S - 1) & 1) ? b0 : b1;
+    cpx<T> *const b0 = sm + slot * slot_len, *const b1 = b0 + Lq;
+    const int S = a.core.nst;
+    run_stockham_smem<T>(a.core, b0, b1, tid, tpt, a.tw, KIND == 0 ? a.inv != 0 : false, sync);
+    if constexpr (KIND != 0) {
+      // kernel product on the forward result (natural order), then the inverse
+      const long long g = g0 + slot;
+      const long long gc = g < a.G ? g : a.G - 1;
       const cpx<T> *kern = a.kern;
       if constexpr (KIND == 3) kern += gc * a.kern_stride;
-      cpx<T> x0 = mk((T)0, (T)0);
-      if constexpr (KIND == 2) x0 = ldg_c(xin);
-      auto src = [&](int p) -> cpx<T> {
-        if constexpr (KIND == 1) {
-          return p < n ? cmul(ldg_c(xin + (long long)p * a.ii), ldg_c(a.chirp + p)) : mk((T)0, (T)0);
-        } else if constexpr (KIND == 2) {
-          return ldg_c(xin + (long long)ldg_v(a.perm_in + p) * a.ii);
-        } else {
-          return ldg_c(xin + (long long)p * a.ii);
-        }
-      };
-      auto mid = [&](int p, cpx<T> v) {
+      cpx<T> *const r = (S & 1) ? b1 : b0;
+      for (int p = tid; p < L; p += tpt) {
+        cpx<T> v = r[pp_pos(p)];
         if constexpr (KIND == 2) {
-          if (p == 0 && live) yout[0] = x0 + v;  // X0 = x0 + sum_q a[q]
+          if (p == 0) b0[2 * Lq + 1] = v + b0[2 * Lq];  // X0 = x0 + sum_q a[q]
         }
-        F[pp_pos(p)] = cmul(v, ldg_c(kern + p));
-      };
-      run_stockham<T>(a.core, b0, b1, tid, tpt, a.tw, false, src, mid, sync);
+        r[pp_pos(p)] = cmul(v, ldg_c(kern + p));
+      }
       sync();
-      PPRead<T> rd{F};
-      auto dst = [&](int p, cpx<T> v) {
-        if (!live) return;
-        if constexpr (KIND == 1) {
-          if (p < n) yout[(long long)p * a.ok] = cmul(v, ldg_c(a.chirp + p));
-        } else if constexpr (KIND == 2) {
-          yout[(long long)ldg_v(a.perm_out + p) * a.ok] = x0 + v;
-        } else {
-          yout[(long long)p * a.ok] = post_twiddle(v, p);
-        }
-      };
-      run_stockham<T>(a.core2, G0, F, tid, tpt, a.tw, true, rd, dst, sync);
+      run_stockham_smem<T>(a.core2, r, (S & 1) ? b0 : b1, tid, tpt, a.tw, true, sync);
     }
   });
+
+  // ---- store
+  const int S_total = a.core.nst + (KIND == 0 ? 0 : a.core2.nst);
+  const int res_off = (S_total & 1) ? Lq : 0;
+  auto post_twiddle = [&](cpx<T> v, long long g, int k) -> cpx<T> {
+    if (!a.post_twiddle) return v;
+    const uint32_t m = (uint32_t)(g * (long long)k);
+    const uint32_t hi = fdiv(m, a.ptw_div);
+    const uint32_t lo = m - hi * a.ptw_div.d;
+    cpx<T> t = cmul(ldg_c(a.ptw_hi + hi), ldg_c(a.ptw_lo + lo));
+    if (a.inv) t.y = -t.y;
+    return cmul(v, t);
+  };
+  const int nout = KIND == 1 ? n : L;
+  const int total = W * nout;
+  for (int e = t0; e < total; e += nt) {
+    int w, k;
+    split_elem(e, W, nout, a.wfast, a.wdiv, KIND == 1 ? a.ndiv : a.ldiv, w, k);
+    const long long g = g0 + w;
+    if (g >= a.G) continue;
+    const cpx<T> *bw = sm + w * slot_len;
+    cpx<T> v = bw[res_off + pp_pos(k)];
+    cpx<T> *yout = out + g * a.og;
+    if constexpr (KIND == 0) {
+      if (a.chirp_mode == 2) {
+        const long long j = (long long)k * a.cj_e + g * a.cj_g;
+        if (j < n) yout[(long long)k * a.ok] = cmul(v, ldg_c(a.chirp + j));
+      } else {
+        yout[(long long)k * a.ok] = post_twiddle(v, g, k);
+      }
+    } else if constexpr (KIND == 1) {
+      yout[(long long)k * a.ok] = cmul(v, ldg_c(a.chirp + k));
+    } else if constexpr (KIND == 2) {
+      yout[(long long)ldg_v(a.perm_out + k) * a.ok] = bw[2 * Lq] + v;
+    } else {
+      yout[(long long)k * a.ok] = post_twiddle(v, g, k);
+    }
+  }
+  if constexpr (KIND == 2) {
+    for (int w = t0; w < W; w += nt) {
+      const long long g = g0 + w;
+      if (g < a.G) out[g * a.og] = sm[w * slot_len + 2 * Lq + 1];
+    }
+  }
 }
 
 template <typename T>
