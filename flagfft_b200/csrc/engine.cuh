@@ -512,6 +512,26 @@ FFB_HD void run_stockham(const Core &c, cpx<T> *b0, cpx<T> *b1, int tid, int nth
   }
 }
 
+// Flat loop over e = t0, t0 + nt, ... < total, U iterations at a time: the U
+// values are all produced (their global loads issued back to back) before
+// any is consumed, so a thread keeps U loads in flight instead of one.
+template <int U, class V, class Produce, class Consume>
+FFB_HD void chunked_loop(int t0, int nt, int total, Produce &&produce, Consume &&consume) {
+  for (int base = t0; base < total; base += U * nt) {
+    V v[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int e = base + u * nt;
+      if (e < total) v[u] = produce(e);
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int e = base + u * nt;
+      if (e < total) consume(e, v[u]);
+    }
+  }
+}
+
 // All stages of `c` shared -> shared: stage s reads buffer (s even ? src : oth)
 // and writes the other; every stage ends with a barrier.  The result is in
 // `src` when nst is even, in `oth` when odd.

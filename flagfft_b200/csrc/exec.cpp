@@ -529,11 +529,10 @@ class Builder {
 // A length-n complex transform over `batch` rows (row distances idist / odist)
 // from `src` to `dst`; `ws` is a workspace of batch * (n or the Bluestein
 // convolution length) elements when the plan needs more than one pass.
-// On-chip policy ($FLAGFFT_ONCHIP_POLICY): "auto" keeps a transform in one
-// pass when its two Stockham buffers fit a CTA and otherwise prefers a
-// multi-pass lowering of the plan tree over the in-place single-pass one;
-// "inplace" keeps every transform that fits in place on chip; "multipass"
-// splits every tree that has a multi-pass lowering.
+// On-chip policy ($FLAGFFT_ONCHIP_POLICY): by default a transform that fits
+// one CTA (two Stockham buffers, or in place) runs as one pass; "multipass"
+// splits every tree that has a multi-pass lowering instead (one HBM round
+// trip more, but smaller, more numerous CTAs).
 static int onchip_policy() {
   const char *v = std::getenv("FLAGFFT_ONCHIP_POLICY");
   if (!v) return 0;
@@ -552,9 +551,7 @@ void lower_c2c(Builder<T> &bld, Program &prog, const NodePtr &root, bool inverse
                        bld.core_for(root->child->row, ca) && bld.core_for(root->child->col, cb) &&
                        ca.kind == CoreKind::Dit && cb.kind == CoreKind::Dit;
   const int policy = onchip_policy();
-  const bool use_onchip =
-      onchip && (policy == 1 || (policy == 0 && (Builder<T>::pp_fits(spec.L) || !(mp_four || mp_blue))) ||
-                 (policy == 2 && !(mp_four || mp_blue)));
+  const bool use_onchip = onchip && (policy != 2 || !(mp_four || mp_blue));
   if (use_onchip) {
     bld.add_pass(spec, IoKind::C2C, inverse, 1, batch, 0, idist, 1, 0, odist, 1, src, dst, n);
     return;

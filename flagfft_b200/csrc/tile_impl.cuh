@@ -155,7 +155,7 @@ FFB_HD void tile_body(const TileArgs<T> &a, long long bx, long long by, cpx<T> *
   {
     const int total = W * L;
     const int nl = (IO == 1 || IO == 2) ? half_n : n;  // Bluestein logical length
-    for (int e = t0; e < total; e += nt) {
+    auto produce = [&](int e) -> cpx<T> {
       int w, i;
       split_elem(e, W, L, a.wfast, a.wdiv, a.ldiv, w, i);
       const long long g = g0 + w;
@@ -167,18 +167,25 @@ FFB_HD void tile_body(const TileArgs<T> &a, long long bx, long long by, cpx<T> *
         } else if (g < a.G) {
           v = core_input(g, i);
         }
-        sm[w * Lp + Swz<T>::phys(dit_position(i, a.core))] = v;
       } else if constexpr (KIND == 3) {
         if (g < a.G) v = core_input(g, i);
-        sm[w * Lp + Swz<T>::phys(i)] = v;
       } else if constexpr (KIND == 1) {
         if (g < a.G && i < nl) v = cmul(core_input(g, i), ldg_c(a.chirp + i));
-        sm[w * Lp + Swz<T>::phys(i)] = v;
       } else {  // Rader: a[q] = x[g^-q], q < L = p - 1
         if (g < a.G) v = core_input(g, ldg_v(a.perm_in + i));
+      }
+      return v;
+    };
+    auto consume = [&](int e, cpx<T> v) {
+      int w, i;
+      split_elem(e, W, L, a.wfast, a.wdiv, a.ldiv, w, i);
+      if constexpr (KIND == 0) {
+        sm[w * Lp + Swz<T>::phys(dit_position(i, a.core))] = v;
+      } else {
         sm[w * Lp + Swz<T>::phys(i)] = v;
       }
-    }
+    };
+    chunked_loop<8, cpx<T>>(t0, nt, total, produce, consume);
     if constexpr (KIND == 2) {
       for (int w = t0; w < W; w += nt) {
         const long long g = g0 + w;
@@ -258,21 +265,31 @@ FFB_HD void tile_body(const TileArgs<T> &a, long long bx, long long by, cpx<T> *
     } else {
       const int nout = KIND == 1 ? n : L;
       const int total = W * nout;
-      for (int e = t0; e < total; e += nt) {
+      auto produce = [&](int e) -> cpx<T> {
         int w, k;
         split_elem(e, W, nout, a.wfast, a.wdiv, KIND == 1 ? a.ndiv : a.ldiv, w, k);
         const long long g = g0 + w;
-        if (g >= a.G) continue;
+        const long long gc = g < a.G ? g : a.G - 1;
         cpx<T> v = out_elem(w, k);
         if constexpr (KIND == 0) {
           if (a.chirp_mode == 2) {  // Bluestein output: y_j = conv_j * chirp_j, j < n
-            const long long j = (long long)k * a.cj_e + g * a.cj_g;
-            if (j >= n) continue;
-            v = cmul(v, ldg_c(a.chirp + j));
+            const long long j = (long long)k * a.cj_e + gc * a.cj_g;
+            return j < n ? cmul(v, ldg_c(a.chirp + j)) : v;
           }
         }
-        st_cpx<T>(out, g * a.og + (long long)k * a.ok, post_twiddle(v, g, k));
-      }
+        return post_twiddle(v, gc, k);
+      };
+      auto consume = [&](int e, cpx<T> v) {
+        int w, k;
+        split_elem(e, W, nout, a.wfast, a.wdiv, KIND == 1 ? a.ndiv : a.ldiv, w, k);
+        const long long g = g0 + w;
+        if (g >= a.G) return;
+        if constexpr (KIND == 0) {
+          if (a.chirp_mode == 2 && (long long)k * a.cj_e + g * a.cj_g >= n) return;
+        }
+        st_cpx<T>(out, g * a.og + (long long)k * a.ok, v);
+      };
+      chunked_loop<8, cpx<T>>(t0, nt, total, produce, consume);
     }
   } else if constexpr (IO == 1) {
     // X_k = E_k + W_n^k O_k,  E = (Z_k + conj Z_{L-k})/2,  O = -i (Z_k - conj Z_{L-k})/2
@@ -363,29 +380,32 @@ FFB_HD void tile_body_pp(const TileArgs<T> &a, long long bx, long long by, cpx<T
   // ---- load
   {
     const int total = W * L;
-    for (int e = t0; e < total; e += nt) {
+    auto produce = [&](int e) -> cpx<T> {
       int w, i;
       split_elem(e, W, L, a.wfast, a.wdiv, a.ldiv, w, i);
       const long long g = g0 + w;
       const long long gc = g < a.G ? g : a.G - 1;
       const cpx<T> *xin = in + gc * a.ig;
-      cpx<T> v;
       if constexpr (KIND == 0) {
         if (a.chirp_mode == 1) {
           const long long j = (long long)i * a.cj_e + gc * a.cj_g;
-          v = j < n ? cmul(ldg_c(xin + (long long)i * a.ii), ldg_c(a.chirp + j)) : mk((T)0, (T)0);
-        } else {
-          v = ldg_c(xin + (long long)i * a.ii);
+          return j < n ? cmul(ldg_c(xin + (long long)i * a.ii), ldg_c(a.chirp + j)) : mk((T)0, (T)0);
         }
+        return ldg_c(xin + (long long)i * a.ii);
       } else if constexpr (KIND == 1) {
-        v = i < n ? cmul(ldg_c(xin + (long long)i * a.ii), ldg_c(a.chirp + i)) : mk((T)0, (T)0);
+        return i < n ? cmul(ldg_c(xin + (long long)i * a.ii), ldg_c(a.chirp + i)) : mk((T)0, (T)0);
       } else if constexpr (KIND == 2) {
-        v = ldg_c(xin + (long long)ldg_v(a.perm_in + i) * a.ii);
+        return ldg_c(xin + (long long)ldg_v(a.perm_in + i) * a.ii);
       } else {
-        v = ldg_c(xin + (long long)i * a.ii);
+        return ldg_c(xin + (long long)i * a.ii);
       }
+    };
+    auto consume = [&](int e, cpx<T> v) {
+      int w, i;
+      split_elem(e, W, L, a.wfast, a.wdiv, a.ldiv, w, i);
       sm[w * slot_len + pp_pos(i)] = v;
-    }
+    };
+    chunked_loop<8, cpx<T>>(t0, nt, total, produce, consume);
     if constexpr (KIND == 2) {
       for (int w = t0; w < W; w += nt) {
         const long long g = g0 + w;
@@ -435,29 +455,44 @@ FFB_HD void tile_body_pp(const TileArgs<T> &a, long long bx, long long by, cpx<T
   };
   const int nout = KIND == 1 ? n : L;
   const int total = W * nout;
-  for (int e = t0; e < total; e += nt) {
+  // produce: the value to store (smem read, twiddle / chirp loads issued together)
+  auto produce = [&](int e) -> cpx<T> {
     int w, k;
     split_elem(e, W, nout, a.wfast, a.wdiv, KIND == 1 ? a.ndiv : a.ldiv, w, k);
     const long long g = g0 + w;
-    if (g >= a.G) continue;
+    const long long gc = g < a.G ? g : a.G - 1;
     const cpx<T> *bw = sm + w * slot_len;
     cpx<T> v = bw[res_off + pp_pos(k)];
-    cpx<T> *yout = out + g * a.og;
     if constexpr (KIND == 0) {
       if (a.chirp_mode == 2) {
-        const long long j = (long long)k * a.cj_e + g * a.cj_g;
-        if (j < n) yout[(long long)k * a.ok] = cmul(v, ldg_c(a.chirp + j));
-      } else {
-        yout[(long long)k * a.ok] = post_twiddle(v, g, k);
+        const long long j = (long long)k * a.cj_e + gc * a.cj_g;
+        return j < n ? cmul(v, ldg_c(a.chirp + j)) : v;
       }
+      return post_twiddle(v, gc, k);
     } else if constexpr (KIND == 1) {
-      yout[(long long)k * a.ok] = cmul(v, ldg_c(a.chirp + k));
+      return cmul(v, ldg_c(a.chirp + k));
     } else if constexpr (KIND == 2) {
-      yout[(long long)ldg_v(a.perm_out + k) * a.ok] = bw[2 * Lq] + v;
+      return bw[2 * Lq] + v;
     } else {
-      yout[(long long)k * a.ok] = post_twiddle(v, g, k);
+      return post_twiddle(v, gc, k);
     }
-  }
+  };
+  auto consume = [&](int e, cpx<T> v) {
+    int w, k;
+    split_elem(e, W, nout, a.wfast, a.wdiv, KIND == 1 ? a.ndiv : a.ldiv, w, k);
+    const long long g = g0 + w;
+    if (g >= a.G) return;
+    cpx<T> *yout = out + g * a.og;
+    if constexpr (KIND == 0) {
+      if (a.chirp_mode == 2 && (long long)k * a.cj_e + g * a.cj_g >= n) return;
+      yout[(long long)k * a.ok] = v;
+    } else if constexpr (KIND == 2) {
+      yout[(long long)ldg_v(a.perm_out + k) * a.ok] = v;
+    } else {
+      yout[(long long)k * a.ok] = v;
+    }
+  };
+  chunked_loop<8, cpx<T>>(t0, nt, total, produce, consume);
   if constexpr (KIND == 2) {
     for (int w = t0; w < W; w += nt) {
       const long long g = g0 + w;
