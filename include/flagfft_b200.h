@@ -40,6 +40,33 @@ FLAGFFT_API const char *flagfftB200PlanJson(flagfftHandle plan);
  * counterpart. */
 FLAGFFT_API int flagfftB200LaunchCount(flagfftHandle plan, int direction);
 
+/* Batched complex64 FFT of power-of-two length n (8192 <= n <= 2^24) that
+ * allocates no memory.  No counterpart in the reference.
+ *
+ * For callers that cannot call cudaMalloc when they transform: code running
+ * under a memory pool or allocator that must not grow, inside a region that
+ * forbids device allocation, or with no spare memory left to carve a plan
+ * workspace from.  Transforms of this size need an intermediate buffer of
+ * batch * n elements; here it is a fixed 32 MiB array built into the library
+ * (every GPU that loads the library holds it until the process exits), so
+ * batch * n may not exceed 2^22 elements.  Larger requests return
+ * FLAGFFT_INVALID_SIZE with a message on stderr; the entry point never calls
+ * cudaMalloc, cudaFree or an allocating library routine.
+ *
+ * idata / odata are device pointers to batch contiguous rows of n
+ * flagfftComplex (odata may equal idata); direction is FLAGFFT_FORWARD or
+ * FLAGFFT_INVERSE (unnormalized); work is queued on `stream`.
+ *
+ * The first call on a device looks up the fixed arrays' device addresses and
+ * fills a twiddle table with the device current, then waits for that fill:
+ * make the first call on each device before any stream capture.  Every call
+ * shares the one workspace and rewrites its twiddle tables, so calls whose
+ * work overlaps on the GPU race with each other: serialise them (one stream,
+ * or events).  Nothing in the arrays has to start at zero: each call writes
+ * every workspace and table element it reads before reading it. */
+FLAGFFT_API flagfftResult flagfftB200ExecC2CNoAlloc(const flagfftComplex *idata, flagfftComplex *odata, int n,
+                                                    int batch, int direction, flagfftStream_t stream);
+
 #ifdef __cplusplus
 }
 #endif
