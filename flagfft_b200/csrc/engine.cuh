@@ -442,20 +442,37 @@ FFB_HD void run_dif(cpx<T> *buf, const Core &c, int tid, int nthr,
 FFB_HD int pp_pos(int p) { return p + (p >> 4); }
 FFB_HD int pp_size(int L) { return ((L + (L >> 4) + 1) + 1) & ~1; }
 
-template <int R, typename T, class Src, class Dst>
-FFB_HD void stockham_stage_r(const Core &c, int s, int tid, int nthr, const cpx<T> *__restrict__ tw, bool inv,
-                             Src &src, Dst &dst) {
+// Twiddle table readers: global (read-only cache) or shared memory.
+template <typename T>
+struct TwGlobal {
+  const cpx<T> *p;
+  FFB_HD cpx<T> operator()(int m) const { return ldg_c(p + m); }
+};
+template <typename T>
+struct TwShared {
+  const cpx<T> *p;
+  FFB_HD cpx<T> operator()(int m) const { return p[m]; }
+};
+
+template <int R, typename T, class Src, class Dst, class Tw>
+FFB_HD void stockham_stage_r(const Core &c, int s, int tid, int nthr, const Tw &tw, bool inv, Src &src, Dst &dst) {
   const int Ns = c.span[s];
   const int tws = c.tws[s];
   const int nb = c.L / R;
+  const T sgn = inv ? (T)-1 : (T)1;
   for (int j = tid; j < nb; j += nthr) {
     const int k = j - (int)fdiv((uint32_t)j, c.sdiv[s]) * Ns;
     cpx<T> v[R];
 #pragma unroll
     for (int r = 0; r < R; ++r) v[r] = src(j + r * nb);
     if (k != 0) {
+      const int step = k * tws;
 #pragma unroll
-      for (int r = 1; r < R; ++r) v[r] = cmul(v[r], twiddle(tw, r * k * tws, inv));
+      for (int r = 1; r < R; ++r) {
+        cpx<T> w = tw(r * step);
+        w.y *= sgn;
+        v[r] = cmul(v[r], w);
+      }
     }
     dft_dir<R, T>(v, inv);
     const int base = (j - k) * R + k;
@@ -484,27 +501,28 @@ struct PPWrite {
 template <typename T, class Src, class Dst, class Sync>
 FFB_HD void run_stockham(const Core &c, cpx<T> *b0, cpx<T> *b1, int tid, int nthr, const cpx<T> *__restrict__ tw,
                          bool inv, Src &src, Dst &dst, Sync sync) {
+  const TwGlobal<T> twl{tw};
   const int S = c.nst;
   for (int s = 0; s < S; ++s) {
     const bool first = s == 0, last = s == S - 1;
     if (first && last) {
-#define FFB_SS(R) stockham_stage_r<R, T>(c, s, tid, nthr, tw, inv, src, dst)
+#define FFB_SS(R) stockham_stage_r<R, T>(c, s, tid, nthr, twl, inv, src, dst)
       FFB_RADIX_SWITCH(c.radix[s], FFB_SS)
 #undef FFB_SS
     } else if (first) {
       PPWrite<T> w{b0};
-#define FFB_SS(R) stockham_stage_r<R, T>(c, s, tid, nthr, tw, inv, src, w)
+#define FFB_SS(R) stockham_stage_r<R, T>(c, s, tid, nthr, twl, inv, src, w)
       FFB_RADIX_SWITCH(c.radix[s], FFB_SS)
 #undef FFB_SS
     } else if (last) {
       PPRead<T> rd{((s - 1) & 1) ? b1 : b0};
-#define FFB_SS(R) stockham_stage_r<R, T>(c, s, tid, nthr, tw, inv, rd, dst)
+#define FFB_SS(R) stockham_stage_r<R, T>(c, s, tid, nthr, twl, inv, rd, dst)
       FFB_RADIX_SWITCH(c.radix[s], FFB_SS)
 #undef FFB_SS
     } else {
       PPRead<T> rd{((s - 1) & 1) ? b1 : b0};
       PPWrite<T> w{(s & 1) ? b1 : b0};
-#define FFB_SS(R) stockham_stage_r<R, T>(c, s, tid, nthr, tw, inv, rd, w)
+#define FFB_SS(R) stockham_stage_r<R, T>(c, s, tid, nthr, twl, inv, rd, w)
       FFB_RADIX_SWITCH(c.radix[s], FFB_SS)
 #undef FFB_SS
     }
@@ -535,9 +553,9 @@ FFB_HD void chunked_loop(int t0, int nt, int total, Produce &&produce, Consume &
 // All stages of `c` shared -> shared: stage s reads buffer (s even ? src : oth)
 // and writes the other; every stage ends with a barrier.  The result is in
 // `src` when nst is even, in `oth` when odd.
-template <typename T, class Sync>
-FFB_HD void run_stockham_smem(const Core &c, cpx<T> *src, cpx<T> *oth, int tid, int nthr,
-                              const cpx<T> *__restrict__ tw, bool inv, Sync sync) {
+template <typename T, class Tw, class Sync>
+FFB_HD void run_stockham_smem(const Core &c, cpx<T> *src, cpx<T> *oth, int tid, int nthr, const Tw &tw, bool inv,
+                              Sync sync) {
   for (int s = 0; s < c.nst; ++s) {
     PPRead<T> rd{(s & 1) ? oth : src};
     PPWrite<T> w{(s & 1) ? src : oth};

@@ -272,7 +272,7 @@ class Builder {
 
   // Two ping-pong buffers of a length-L transform fit one CTA.
   static bool pp_fits(int64_t L) {
-    return (2 * (size_t)pp_size((int)L) + 2) * sizeof(cpx<T>) <= 232448;
+    return (2 * (size_t)pp_size((int)L) + 3) * sizeof(cpx<T>) <= 232448;
   }
 
   // On-chip core for a complex transform node, if one exists.
@@ -339,7 +339,7 @@ class Builder {
     const size_t limit = 232448;
     // Stockham ping-pong when two buffers of the transform fit (C2C passes);
     // the in-place DIT / DIF path otherwise.
-    const size_t pp_per = (2 * (size_t)pp_size((int)L) + 2) * sizeof(cpx<T>);
+    const size_t pp_per = (2 * (size_t)pp_size((int)L) + 3) * sizeof(cpx<T>);
     a.pp = (io == IoKind::C2C && L > 1 && pp_per <= limit) ? 1 : 0;
     if (spec.kind == CoreKind::Dit) {
       a.core = make_dit_core(L, spec.radices);
@@ -370,13 +370,29 @@ class Builder {
     if (W * tpt > kMaxThreads) tpt = std::max<int>(1, (int)(kMaxThreads / W));
     a.W = (int)W;
     a.tpt = tpt;
+    // offsets inside one CTA's tile are 32-bit in the kernels
+    if (W * std::llabs(ig) + L * std::llabs(ii) >= (1ll << 31) || W * std::llabs(og) + L * std::llabs(ok) >= (1ll << 31))
+      throw std::runtime_error("tile extent above 2^31 elements");
+    // ping-pong passes stage the twiddle table in shared memory when it fits
+    // without costing a CTA of occupancy
+    size_t smem = per * (size_t)W;
+    if (a.pp) {
+      const size_t tw_bytes = (size_t)L * sizeof(cpx<T>);
+      const size_t with = smem + tw_bytes;
+      const int ctas_without = (int)std::min<size_t>(8, 232448 / smem);
+      const int ctas_with = (int)std::min<size_t>(8, 232448 / with);
+      if (with <= limit && ctas_with >= std::min(ctas_without, 2)) {
+        a.tw_smem = 1;
+        smem = with;
+      }
+    }
     a.ldiv = make_fastdiv((uint32_t)L);
     a.wdiv = make_fastdiv((uint32_t)W);
     a.ndiv = make_fastdiv((uint32_t)std::max<int64_t>(1, logical_n));
     a.hdiv = make_fastdiv((uint32_t)std::max<int64_t>(1, logical_n / 2));
     p->kind = spec.kind;
     p->io = io;
-    p->smem = per * (size_t)W;
+    p->smem = smem;
     p->src = src;
     p->dst = dst;
     TilePass<T> *raw = p.get();

@@ -69,10 +69,11 @@ struct TileArgs {
   long long cj_e, cj_g;
   // Conv cores: transform g multiplies by kern + g * kern_stride.
   long long kern_stride;
-  // 1: Stockham ping-pong path (C2C passes whose two buffers fit): the first
-  // stage reads global memory and the last writes it directly; convolution
-  // kernels are then in natural order.  0: in-place DIT/DIF path.
+  // 1: Stockham ping-pong path (C2C passes whose two buffers fit; convolution
+  // kernels then in natural order).  0: in-place DIT/DIF path.
   int pp;
+  // ping-pong path: 1 = the twiddle table is staged in shared memory after the slots
+  int tw_smem;
 };
 
 // Real-transform pre/post processing between the passes of a multi-pass

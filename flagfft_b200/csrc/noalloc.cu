@@ -112,7 +112,7 @@ TileArgs<float> pass_args(int L, int G, long long nbatch, long long ib, long lon
   const int rmax = L >= 16 ? 16 : L;
   int tpt = (L + rmax - 1) / rmax;
   tpt = tpt <= 32 ? tpt : (tpt + 31) / 32 * 32;
-  const size_t per = (2 * (size_t)pp_size(L) + 2) * sizeof(cpx<float>);
+  const size_t per = (2 * (size_t)pp_size(L) + 3) * sizeof(cpx<float>);
   int W = a.wfast ? 8 : (256 / tpt > 1 ? 256 / tpt : 1);
   if (W > G) W = G;
   while (W > 1 && per * W > 110 * 1024) --W;

@@ -361,21 +361,34 @@ FFB_HD void tile_body(const TileArgs<T> &a, long long bx, long long by, cpx<T> *
 
 // Stockham ping-pong pass for C2C tiles.  A coalesced load phase fills
 // buffer 0 of every slot (natural order, chirp / permutation / zero padding
-// applied), all stages run shared -> shared (one code path per radix, warm in
-// the instruction cache after the first stage), and a coalesced store phase
-// writes the result (unchirp / scatter / four-step twiddle applied).  Slot
-// layout: two buffers of pp_size(L) plus two spare elements (Rader x0, X0).
+// applied) and, when a.tw_smem, copies the twiddle table next to the slots;
+// all stages run shared -> shared (one code path per radix, warm in the
+// instruction cache after the first stage); a coalesced store phase writes
+// the result (unchirp / scatter / four-step twiddle applied).
+// Slot layout: two buffers of pp_size(L) and three spare elements (Rader x0,
+// X0, and one so the slot stride is odd: consecutive slots then fall in
+// different banks).  Offsets inside a CTA's tile are 32-bit.
+template <typename T>
+FFB_HD int pp_slot_len(int L) {
+  return 2 * pp_size(L) + 3;
+}
+
 template <typename T, int KIND, class X>
 FFB_HD void tile_body_pp(const TileArgs<T> &a, long long bx, long long by, cpx<T> *sm, const X &x) {
   const int L = a.core.L;
   const int Lq = pp_size(L);
-  const int slot_len = 2 * Lq + 2;
+  const int slot_len = pp_slot_len<T>(L);
   const int W = a.W;
   const long long g0 = bx * W;
-  const cpx<T> *in = reinterpret_cast<const cpx<T> *>(a.in) + by * a.ib;
-  cpx<T> *out = reinterpret_cast<cpx<T> *>(a.out) + by * a.ob;
+  // CTA base pointers; transform w of the tile is at w * ig, element i at i * ii
+  const cpx<T> *in = reinterpret_cast<const cpx<T> *>(a.in) + by * a.ib + g0 * a.ig;
+  cpx<T> *out = reinterpret_cast<cpx<T> *>(a.out) + by * a.ob + g0 * a.og;
+  const int ig = (int)a.ig, ii = (int)a.ii, og = (int)a.og, ok = (int)a.ok;
+  const int wlive = (int)((a.G - g0) < W ? (a.G - g0) : W);  // live transforms in this tile
   const int n = a.n;
   const int t0 = x.tid(), nt = x.nthreads();
+  cpx<T> *const tws = sm + W * slot_len;
+  constexpr int U = sizeof(T) == 4 ? 16 : 8;
 
   // ---- load
   {
@@ -383,21 +396,20 @@ FFB_HD void tile_body_pp(const TileArgs<T> &a, long long bx, long long by, cpx<T
     auto produce = [&](int e) -> cpx<T> {
       int w, i;
       split_elem(e, W, L, a.wfast, a.wdiv, a.ldiv, w, i);
-      const long long g = g0 + w;
-      const long long gc = g < a.G ? g : a.G - 1;
-      const cpx<T> *xin = in + gc * a.ig;
+      const int wc = w < wlive ? w : wlive - 1;
+      const cpx<T> *xin = in + wc * ig;
       if constexpr (KIND == 0) {
         if (a.chirp_mode == 1) {
-          const long long j = (long long)i * a.cj_e + gc * a.cj_g;
-          return j < n ? cmul(ldg_c(xin + (long long)i * a.ii), ldg_c(a.chirp + j)) : mk((T)0, (T)0);
+          const long long j = (long long)i * a.cj_e + (g0 + wc) * a.cj_g;
+          return j < n ? cmul(ldg_c(xin + i * ii), ldg_c(a.chirp + j)) : mk((T)0, (T)0);
         }
-        return ldg_c(xin + (long long)i * a.ii);
+        return ldg_c(xin + i * ii);
       } else if constexpr (KIND == 1) {
-        return i < n ? cmul(ldg_c(xin + (long long)i * a.ii), ldg_c(a.chirp + i)) : mk((T)0, (T)0);
+        return i < n ? cmul(ldg_c(xin + i * ii), ldg_c(a.chirp + i)) : mk((T)0, (T)0);
       } else if constexpr (KIND == 2) {
-        return ldg_c(xin + (long long)ldg_v(a.perm_in + i) * a.ii);
+        return ldg_c(xin + ldg_v(a.perm_in + i) * ii);
       } else {
-        return ldg_c(xin + (long long)i * a.ii);
+        return ldg_c(xin + i * ii);
       }
     };
     auto consume = [&](int e, cpx<T> v) {
@@ -405,12 +417,14 @@ FFB_HD void tile_body_pp(const TileArgs<T> &a, long long bx, long long by, cpx<T
       split_elem(e, W, L, a.wfast, a.wdiv, a.ldiv, w, i);
       sm[w * slot_len + pp_pos(i)] = v;
     };
-    chunked_loop<8, cpx<T>>(t0, nt, total, produce, consume);
+    chunked_loop<U, cpx<T>>(t0, nt, total, produce, consume);
+    if (a.tw_smem) {
+      for (int m = t0; m < L; m += nt) tws[m] = ldg_c(a.tw + m);
+    }
     if constexpr (KIND == 2) {
       for (int w = t0; w < W; w += nt) {
-        const long long g = g0 + w;
-        const long long gc = g < a.G ? g : a.G - 1;
-        sm[w * slot_len + 2 * Lq] = ldg_c(in + gc * a.ig);  // x0
+        const int wc = w < wlive ? w : wlive - 1;
+        sm[w * slot_len + 2 * Lq] = ldg_c(in + wc * ig);  // x0
       }
     }
   }
@@ -418,28 +432,34 @@ FFB_HD void tile_body_pp(const TileArgs<T> &a, long long bx, long long by, cpx<T
 
   // ---- stages
   auto sync = [&]() { x.sync(); };
-  x.per_slot(W, [&](int slot, int tid, int tpt) {
-    cpx<T> *const b0 = sm + slot * slot_len, *const b1 = b0 + Lq;
-    const int S = a.core.nst;
-    run_stockham_smem<T>(a.core, b0, b1, tid, tpt, a.tw, KIND == 0 ? a.inv != 0 : false, sync);
-    if constexpr (KIND != 0) {
-      // kernel product on the forward result (natural order), then the inverse
-      const long long g = g0 + slot;
-      const long long gc = g < a.G ? g : a.G - 1;
-      const cpx<T> *kern = a.kern;
-      if constexpr (KIND == 3) kern += gc * a.kern_stride;
-      cpx<T> *const r = (S & 1) ? b1 : b0;
-      for (int p = tid; p < L; p += tpt) {
-        cpx<T> v = r[pp_pos(p)];
-        if constexpr (KIND == 2) {
-          if (p == 0) b0[2 * Lq + 1] = v + b0[2 * Lq];  // X0 = x0 + sum_q a[q]
+  auto stages = [&](const auto &tw) {
+    x.per_slot(W, [&](int slot, int tid, int tpt) {
+      cpx<T> *const b0 = sm + slot * slot_len, *const b1 = b0 + Lq;
+      const int S = a.core.nst;
+      run_stockham_smem<T>(a.core, b0, b1, tid, tpt, tw, KIND == 0 ? a.inv != 0 : false, sync);
+      if constexpr (KIND != 0) {
+        // kernel product on the forward result (natural order), then the inverse
+        const int wc = slot < wlive ? slot : wlive - 1;
+        const cpx<T> *kern = a.kern;
+        if constexpr (KIND == 3) kern += (g0 + wc) * a.kern_stride;
+        cpx<T> *const r = (S & 1) ? b1 : b0;
+        for (int p = tid; p < L; p += tpt) {
+          cpx<T> v = r[pp_pos(p)];
+          if constexpr (KIND == 2) {
+            if (p == 0) b0[2 * Lq + 1] = v + b0[2 * Lq];  // X0 = x0 + sum_q a[q]
+          }
+          r[pp_pos(p)] = cmul(v, ldg_c(kern + p));
         }
-        r[pp_pos(p)] = cmul(v, ldg_c(kern + p));
+        sync();
+        run_stockham_smem<T>(a.core2, r, (S & 1) ? b0 : b1, tid, tpt, tw, true, sync);
       }
-      sync();
-      run_stockham_smem<T>(a.core2, r, (S & 1) ? b0 : b1, tid, tpt, a.tw, true, sync);
-    }
-  });
+    });
+  };
+  if (a.tw_smem) {
+    stages(TwShared<T>{tws});
+  } else {
+    stages(TwGlobal<T>{a.tw});
+  }
 
   // ---- store
   const int S_total = a.core.nst + (KIND == 0 ? 0 : a.core2.nst);
@@ -455,49 +475,43 @@ FFB_HD void tile_body_pp(const TileArgs<T> &a, long long bx, long long by, cpx<T
   };
   const int nout = KIND == 1 ? n : L;
   const int total = W * nout;
-  // produce: the value to store (smem read, twiddle / chirp loads issued together)
   auto produce = [&](int e) -> cpx<T> {
     int w, k;
     split_elem(e, W, nout, a.wfast, a.wdiv, KIND == 1 ? a.ndiv : a.ldiv, w, k);
-    const long long g = g0 + w;
-    const long long gc = g < a.G ? g : a.G - 1;
+    const int wc = w < wlive ? w : wlive - 1;
     const cpx<T> *bw = sm + w * slot_len;
     cpx<T> v = bw[res_off + pp_pos(k)];
     if constexpr (KIND == 0) {
       if (a.chirp_mode == 2) {
-        const long long j = (long long)k * a.cj_e + gc * a.cj_g;
+        const long long j = (long long)k * a.cj_e + (g0 + wc) * a.cj_g;
         return j < n ? cmul(v, ldg_c(a.chirp + j)) : v;
       }
-      return post_twiddle(v, gc, k);
+      return post_twiddle(v, g0 + wc, k);
     } else if constexpr (KIND == 1) {
       return cmul(v, ldg_c(a.chirp + k));
     } else if constexpr (KIND == 2) {
       return bw[2 * Lq] + v;
     } else {
-      return post_twiddle(v, gc, k);
+      return post_twiddle(v, g0 + wc, k);
     }
   };
   auto consume = [&](int e, cpx<T> v) {
     int w, k;
     split_elem(e, W, nout, a.wfast, a.wdiv, KIND == 1 ? a.ndiv : a.ldiv, w, k);
-    const long long g = g0 + w;
-    if (g >= a.G) return;
-    cpx<T> *yout = out + g * a.og;
+    if (w >= wlive) return;
+    cpx<T> *yout = out + w * og;
     if constexpr (KIND == 0) {
-      if (a.chirp_mode == 2 && (long long)k * a.cj_e + g * a.cj_g >= n) return;
-      yout[(long long)k * a.ok] = v;
+      if (a.chirp_mode == 2 && (long long)k * a.cj_e + (g0 + w) * a.cj_g >= n) return;
+      yout[k * ok] = v;
     } else if constexpr (KIND == 2) {
-      yout[(long long)ldg_v(a.perm_out + k) * a.ok] = v;
+      yout[ldg_v(a.perm_out + k) * ok] = v;
     } else {
-      yout[(long long)k * a.ok] = v;
+      yout[k * ok] = v;
     }
   };
-  chunked_loop<8, cpx<T>>(t0, nt, total, produce, consume);
+  chunked_loop<U, cpx<T>>(t0, nt, total, produce, consume);
   if constexpr (KIND == 2) {
-    for (int w = t0; w < W; w += nt) {
-      const long long g = g0 + w;
-      if (g < a.G) out[g * a.og] = sm[w * slot_len + 2 * Lq + 1];
-    }
+    for (int w = t0; w < wlive; w += nt) out[w * og] = sm[w * slot_len + 2 * Lq + 1];
   }
 }
 
