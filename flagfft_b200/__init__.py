@@ -5,8 +5,9 @@ The binding mirrors the C API one to one (``plan1d`` / ``plan2d`` / ``plan3d`` /
 ``plan_many`` -> ``flagfftPlan*``, ``Plan.exec_*`` -> ``flagfftExec*``,
 ``Plan.set_stream`` / ``Plan.destroy`` / ``Plan.description``), takes device
 pointers as integers or CUDA torch tensors, and raises ``FlagFFTError`` with the
-C status code on any non-success result.  There is no fallback: if the shared
-library is missing the import fails.
+C status code on any non-success result.  There is no fallback: the shared
+library is loaded on first use (so that ``python -m flagfft_b200.build`` works
+on a fresh tree) and, if it is missing, that first use raises ImportError.
 """
 from __future__ import annotations
 
@@ -78,7 +79,20 @@ def _load():
     return lib
 
 
-LIB = _load()
+_LIB = None
+
+
+def _lib():
+    global _LIB
+    if _LIB is None:
+        _LIB = _load()
+    return _LIB
+
+
+def __getattr__(name):
+    if name == "LIB":
+        return _lib()
+    raise AttributeError(f"module {__name__!r} has no attribute {name!r}")
 
 
 def _check(code: int, what: str) -> None:
@@ -121,7 +135,7 @@ class Plan:
         return self._h.value or 0
 
     def _exec(self, fn: str, idata, odata, *extra) -> None:
-        _check(getattr(LIB, fn)(self._h, ctypes.c_void_p(_ptr(idata)), ctypes.c_void_p(_ptr(odata)), *extra), fn)
+        _check(getattr(_lib(), fn)(self._h, ctypes.c_void_p(_ptr(idata)), ctypes.c_void_p(_ptr(odata)), *extra), fn)
 
     def exec_c2c(self, idata, odata, direction: int) -> None:
         self._exec("flagfftExecC2C", idata, odata, direction)
@@ -158,32 +172,32 @@ class Plan:
             self.exec_z2d(idata, odata)
 
     def set_stream(self, stream) -> None:
-        _check(LIB.flagfftSetStream(self._h, ctypes.c_void_p(_stream_handle(stream))), "flagfftSetStream")
+        _check(_lib().flagfftSetStream(self._h, ctypes.c_void_p(_stream_handle(stream))), "flagfftSetStream")
 
     def description(self) -> str:
-        s = LIB.flagfftGetPlanDescription(self._h)
+        s = _lib().flagfftGetPlanDescription(self._h)
         if s is None:
             raise FlagFFTError(1, "flagfftGetPlanDescription")
         return s.decode()
 
     def tree(self) -> dict:
-        s = LIB.flagfftB200PlanJson(self._h)
+        s = _lib().flagfftB200PlanJson(self._h)
         if s is None:
             raise FlagFFTError(1, "flagfftB200PlanJson")
         return json.loads(s.decode())
 
     def launch_count(self, direction: int = FORWARD) -> int:
-        return int(LIB.flagfftB200LaunchCount(self._h, direction))
+        return int(_lib().flagfftB200LaunchCount(self._h, direction))
 
     def destroy(self) -> None:
         if self._h.value:
-            _check(LIB.flagfftDestroy(self._h), "flagfftDestroy")
+            _check(_lib().flagfftDestroy(self._h), "flagfftDestroy")
             self._h = ctypes.c_void_p(0)
 
     def __del__(self):
         try:
             if self._h.value:
-                LIB.flagfftDestroy(self._h)
+                _lib().flagfftDestroy(self._h)
         except Exception:
             pass
 
@@ -196,19 +210,19 @@ class Plan:
 
 def plan1d(nx: int, ftype: int, batch: int = 1) -> Plan:
     h = ctypes.c_void_p(0)
-    _check(LIB.flagfftPlan1d(ctypes.byref(h), nx, ftype, batch), "flagfftPlan1d")
+    _check(_lib().flagfftPlan1d(ctypes.byref(h), nx, ftype, batch), "flagfftPlan1d")
     return Plan(h.value, ftype, (nx,), batch)
 
 
 def plan2d(nx: int, ny: int, ftype: int) -> Plan:
     h = ctypes.c_void_p(0)
-    _check(LIB.flagfftPlan2d(ctypes.byref(h), nx, ny, ftype), "flagfftPlan2d")
+    _check(_lib().flagfftPlan2d(ctypes.byref(h), nx, ny, ftype), "flagfftPlan2d")
     return Plan(h.value, ftype, (nx, ny), 1)
 
 
 def plan3d(nx: int, ny: int, nz: int, ftype: int) -> Plan:
     h = ctypes.c_void_p(0)
-    _check(LIB.flagfftPlan3d(ctypes.byref(h), nx, ny, nz, ftype), "flagfftPlan3d")
+    _check(_lib().flagfftPlan3d(ctypes.byref(h), nx, ny, nz, ftype), "flagfftPlan3d")
     return Plan(h.value, ftype, (nx, ny, nz), 1)
 
 
@@ -217,20 +231,20 @@ def plan_many(n, inembed, istride: int, idist: int, onembed, ostride: int, odist
     rank = len(n)
     arr = lambda v: None if v is None else (ctypes.c_int * rank)(*v)  # noqa: E731
     h = ctypes.c_void_p(0)
-    _check(LIB.flagfftPlanMany(ctypes.byref(h), rank, arr(n), arr(inembed), istride, idist, arr(onembed), ostride,
+    _check(_lib().flagfftPlanMany(ctypes.byref(h), rank, arr(n), arr(inembed), istride, idist, arr(onembed), ostride,
                                odist, ftype, batch), "flagfftPlanMany")
     return Plan(h.value, ftype, tuple(n), batch)
 
 
 def planner_tree(n: int, is_double: bool = False, smem_bytes: int = 0) -> dict:
     """Plan tree for a 1-D complex length, host only (no GPU)."""
-    need = LIB.flagfftB200PlannerTree(n, int(is_double), smem_bytes, None, 0)
+    need = _lib().flagfftB200PlannerTree(n, int(is_double), smem_bytes, None, 0)
     if need < 0:
         raise FlagFFTError(4, f"planner rejected length {n}")
     buf = ctypes.create_string_buffer(need + 1)
-    LIB.flagfftB200PlannerTree(n, int(is_double), smem_bytes, buf, need + 1)
+    _lib().flagfftB200PlannerTree(n, int(is_double), smem_bytes, buf, need + 1)
     return json.loads(buf.value.decode())
 
 
 def version() -> str:
-    return LIB.flagfftB200Version().decode()
+    return _lib().flagfftB200Version().decode()
