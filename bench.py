@@ -59,7 +59,17 @@ def parse_args():
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="arbitrary_1d")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="budget of the CPU baseline sample")
     ap.add_argument("--no-cufft", action="store_true")
-    return ap.parse_args()
+    ap.add_argument("--problem", default=None, metavar="TYPE:N:BATCH",
+                    help="run one problem instead of a named workload (profiling captures), e.g. C2C:10007:1024")
+    args = ap.parse_args()
+    if args.problem:
+        t, n, b = args.problem.split(":")
+        if t not in ("C2C", "Z2Z", "R2C", "D2Z", "C2R", "Z2D"):
+            ap.error(f"unknown transform type {t}")
+        WORKLOADS["problem"] = [(t, int(n), int(b))]
+        WORKLOAD_DESC["problem"] = f"{t} N={n} x{b}, forward, out-of-place"
+        args.workload = "problem"
+    return args
 
 
 # ---------------------------------------------------------------------------

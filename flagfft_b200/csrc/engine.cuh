@@ -266,9 +266,12 @@ constexpr int kMaxStages = 16;
 
 // One on-chip transform of length L as a sequence of radix stages.
 //   DIT stage s:  span[s] = R0*...*R(s-1)       (sub-transform length before it)
-//                 tws[s]  = L / (span[s]*R(s))  (twiddle index stride)
 //   DIF stage s:  span[s] = L / (R0*...*R(s-1)) (sub-length it splits)
-//                 tws[s]  = L / span[s]
+//   twoff[s] is the offset of stage s's twiddle block in the core's table:
+//   R(s)-1 rows of `inner` entries, row r-1 entry j = W_{inner R(s)}^{r j} with
+//   inner = span[s] (DIT / Stockham) or span[s]/R(s) (DIF), so one butterfly
+//   reads its R-1 twiddles from R-1 rows at the same column j and neighbouring
+//   butterflies read neighbouring entries.
 //   sdiv[s] divides the butterfly index by the inner block length
 //   (DIT: span[s]; DIF: span[s]/R(s)).
 //   rdiv[s] divides by R(s) (digit reversal).
@@ -277,7 +280,7 @@ struct Core {
   int nst;
   int radix[kMaxStages];
   int span[kMaxStages];
-  int tws[kMaxStages];
+  int twoff[kMaxStages];
   FastDiv sdiv[kMaxStages];
   FastDiv rdiv[kMaxStages];
 };
@@ -321,7 +324,7 @@ FFB_HD V ldg_v(const V *p) {
 #endif
 }
 
-// Twiddle W_L^{m} (forward) or its conjugate (inverse) from the length-L table.
+// Twiddle tw[m] (forward sign) or its conjugate (inverse).
 template <typename T>
 FFB_HD cpx<T> twiddle(const cpx<T> *__restrict__ tw, int m, bool inv) {
   cpx<T> w = ldg_c(tw + m);
@@ -334,7 +337,7 @@ template <int R, typename T>
 FFB_HD void dit_stage_r(cpx<T> *buf, const Core &c, int s, int tid, int nthr,
                                             const cpx<T> *__restrict__ tw, bool inv) {
   const int Ls = c.span[s];
-  const int tws = c.tws[s];
+  const int toff = c.twoff[s] - Ls;  // row r starts at toff + r * Ls
   const int nb = c.L / R;
   for (int u = tid; u < nb; u += nthr) {
     const int b = (int)fdiv((uint32_t)u, c.sdiv[s]);
@@ -345,7 +348,7 @@ FFB_HD void dit_stage_r(cpx<T> *buf, const Core &c, int s, int tid, int nthr,
     for (int r = 0; r < R; ++r) v[r] = buf[Swz<T>::phys(base + r * Ls)];
     if (j != 0) {
 #pragma unroll
-      for (int r = 1; r < R; ++r) v[r] = cmul(v[r], twiddle(tw, r * j * tws, inv));
+      for (int r = 1; r < R; ++r) v[r] = cmul(v[r], twiddle(tw, toff + r * Ls + j, inv));
     }
     dft_dir<R, T>(v, inv);
 #pragma unroll
@@ -360,7 +363,7 @@ FFB_HD void dif_stage_r(cpx<T> *buf, const Core &c, int s, int tid, int nthr,
                                             const cpx<T> *__restrict__ tw, bool inv) {
   const int Ms = c.span[s];
   const int stride = Ms / R;
-  const int tws = c.tws[s];
+  const int toff = c.twoff[s] - stride;  // row q starts at toff + q * stride
   const int nb = c.L / R;
   for (int u = tid; u < nb; u += nthr) {
     const int b = (int)fdiv((uint32_t)u, c.sdiv[s]);
@@ -372,7 +375,7 @@ FFB_HD void dif_stage_r(cpx<T> *buf, const Core &c, int s, int tid, int nthr,
     dft_dir<R, T>(v, inv);
     if (j != 0) {
 #pragma unroll
-      for (int q = 1; q < R; ++q) v[q] = cmul(v[q], twiddle(tw, q * j * tws, inv));
+      for (int q = 1; q < R; ++q) v[q] = cmul(v[q], twiddle(tw, toff + q * stride + j, inv));
     }
 #pragma unroll
     for (int q = 0; q < R; ++q) buf[Swz<T>::phys(base + q * stride)] = v[q];
@@ -434,7 +437,7 @@ FFB_HD void run_dif(cpx<T> *buf, const Core &c, int tid, int nthr,
 // caller's source and the last writes the caller's sink directly, so global
 // memory is read and written in the coalesced j + r*L/R pattern and the
 // stages in between ping-pong between two shared-memory buffers.  Uses the
-// DIT core's fields (span = Ns, tws = L/(Ns R), sdiv = / Ns).
+// DIT core's fields (span = Ns, twiddle block at twoff, sdiv = / Ns).
 // ---------------------------------------------------------------------------
 
 // Shared-memory position of element p in a ping-pong buffer: one pad element
@@ -442,22 +445,17 @@ FFB_HD void run_dif(cpx<T> *buf, const Core &c, int tid, int nthr,
 FFB_HD int pp_pos(int p) { return p + (p >> 4); }
 FFB_HD int pp_size(int L) { return ((L + (L >> 4) + 1) + 1) & ~1; }
 
-// Twiddle table readers: global (read-only cache) or shared memory.
+// Twiddle table reader (read-only data cache).
 template <typename T>
 struct TwGlobal {
   const cpx<T> *p;
   FFB_HD cpx<T> operator()(int m) const { return ldg_c(p + m); }
 };
-template <typename T>
-struct TwShared {
-  const cpx<T> *p;
-  FFB_HD cpx<T> operator()(int m) const { return p[m]; }
-};
 
 template <int R, typename T, class Src, class Dst, class Tw>
 FFB_HD void stockham_stage_r(const Core &c, int s, int tid, int nthr, const Tw &tw, bool inv, Src &src, Dst &dst) {
   const int Ns = c.span[s];
-  const int tws = c.tws[s];
+  const int toff = c.twoff[s] - Ns;  // row r starts at toff + r * Ns
   const int nb = c.L / R;
   const T sgn = inv ? (T)-1 : (T)1;
   for (int j = tid; j < nb; j += nthr) {
@@ -466,10 +464,9 @@ FFB_HD void stockham_stage_r(const Core &c, int s, int tid, int nthr, const Tw &
 #pragma unroll
     for (int r = 0; r < R; ++r) v[r] = src(j + r * nb);
     if (k != 0) {
-      const int step = k * tws;
 #pragma unroll
       for (int r = 1; r < R; ++r) {
-        cpx<T> w = tw(r * step);
+        cpx<T> w = tw(toff + r * Ns + k);
         w.y *= sgn;
         v[r] = cmul(v[r], w);
       }

@@ -231,11 +231,12 @@ static Core make_dit_core(int64_t L, const std::vector<int> &r) {
   Core c{};
   c.L = (int)L;
   c.nst = (int)r.size();
-  int64_t span = 1;
+  int64_t span = 1, off = 0;
   for (size_t s = 0; s < r.size(); ++s) {
     c.radix[s] = r[s];
     c.span[s] = (int)span;
-    c.tws[s] = (int)(L / (span * r[s]));
+    c.twoff[s] = (int)off;
+    off += (r[s] - 1) * span;
     c.sdiv[s] = make_fastdiv((uint32_t)span);
     c.rdiv[s] = make_fastdiv((uint32_t)r[s]);
     span *= r[s];
@@ -249,11 +250,12 @@ static Core make_dif_core(int64_t L, const std::vector<int> &r) {
   Core c{};
   c.L = (int)L;
   c.nst = (int)r.size();
-  int64_t span = L;
+  int64_t span = L, off = 0;
   for (size_t s = 0; s < r.size(); ++s) {
     c.radix[s] = r[s];
     c.span[s] = (int)span;
-    c.tws[s] = (int)(L / span);
+    c.twoff[s] = (int)off;
+    off += (r[s] - 1) * (span / r[s]);
     c.sdiv[s] = make_fastdiv((uint32_t)(span / r[s]));
     c.rdiv[s] = make_fastdiv((uint32_t)r[s]);
     span /= r[s];
@@ -349,7 +351,8 @@ class Builder {
       a.core2 = make_dit_core(L, rev);
       if (spec.kind != CoreKind::Conv) fill_convolution(a, spec, inverse);  // Conv: caller supplies the kernel
     }
-    a.tw = table_tw(L);
+    a.tw = table_stage_twiddles(a.core, a.pp == 0 && spec.kind != CoreKind::Dit);
+    if (spec.kind != CoreKind::Dit) a.tw2 = table_stage_twiddles(a.core2, false);
     // thread and tile shape: column tiles (transform index fastest in memory)
     // take consecutive transforms on consecutive threads
     const bool strided = ii > ig;
@@ -373,19 +376,7 @@ class Builder {
     // offsets inside one CTA's tile are 32-bit in the kernels
     if (W * std::llabs(ig) + L * std::llabs(ii) >= (1ll << 31) || W * std::llabs(og) + L * std::llabs(ok) >= (1ll << 31))
       throw std::runtime_error("tile extent above 2^31 elements");
-    // ping-pong passes stage the twiddle table in shared memory when it fits
-    // without costing a CTA of occupancy
-    size_t smem = per * (size_t)W;
-    if (a.pp) {
-      const size_t tw_bytes = (size_t)L * sizeof(cpx<T>);
-      const size_t with = smem + tw_bytes;
-      const int ctas_without = (int)std::min<size_t>(8, 232448 / smem);
-      const int ctas_with = (int)std::min<size_t>(8, 232448 / with);
-      if (with <= limit && ctas_with >= std::min(ctas_without, 2)) {
-        a.tw_smem = 1;
-        smem = with;
-      }
-    }
+    const size_t smem = per * (size_t)W;
     a.ldiv = make_fastdiv((uint32_t)L);
     a.wdiv = make_fastdiv((uint32_t)W);
     a.ndiv = make_fastdiv((uint32_t)std::max<int64_t>(1, logical_n));
@@ -400,18 +391,31 @@ class Builder {
     return raw;
   }
 
-  // W_L^m, m < L (forward sign).
-  const cpx<T> *table_tw(int64_t L) {
+  // Per-stage twiddle blocks of a core (forward sign): stage s's block at
+  // core.twoff[s], entry [r - 1][j] = W_{span R}^{r j} (DIT / Stockham, j <
+  // span) or W_{span}^{r j} (DIF, j < span / R).  A length-L core's blocks
+  // hold L - 1 entries in all.  Cached per radix sequence.
+  const cpx<T> *table_stage_twiddles(const Core &c, bool dif) {
+    std::vector<int64_t> key = {c.L, dif ? 1 : 0};
+    for (int s = 0; s < c.nst; ++s) key.push_back(c.radix[s]);
     for (auto &e : tw_cache_)
-      if (e.first == L) return reinterpret_cast<const cpx<T> *>(e.second->ptr);
-    std::vector<cpx<T>> h((size_t)L);
-    for (int64_t m = 0; m < L; ++m) {
-      cld w = unit_root(m, L, -1);
-      h[(size_t)m] = mk((T)w.real(), (T)w.imag());
+      if (e.first == key) return reinterpret_cast<const cpx<T> *>(e.second->ptr);
+    int64_t total = 0;
+    for (int s = 0; s < c.nst; ++s) total += (int64_t)(c.radix[s] - 1) * (dif ? c.span[s] / c.radix[s] : c.span[s]);
+    std::vector<cpx<T>> h((size_t)std::max<int64_t>(total, 1), mk((T)1, (T)0));
+    for (int s = 0; s < c.nst; ++s) {
+      const int64_t R = c.radix[s];
+      const int64_t inner = dif ? c.span[s] / R : c.span[s];
+      const int64_t den = dif ? c.span[s] : c.span[s] * R;
+      for (int64_t r = 1; r < R; ++r)
+        for (int64_t j = 0; j < inner; ++j) {
+          cld w = unit_root(r * j, den, -1);
+          h[(size_t)(c.twoff[s] + (r - 1) * inner + j)] = mk((T)w.real(), (T)w.imag());
+        }
     }
     DevPtr d = upload(h.data(), h.size() * sizeof(cpx<T>));
     prog_.owned.push_back(d);
-    tw_cache_.push_back({L, d});
+    tw_cache_.push_back({key, d});
     return reinterpret_cast<const cpx<T> *>(d->ptr);
   }
 
@@ -539,7 +543,7 @@ class Builder {
 
   Program &prog_;
   Planner &planner_;
-  std::vector<std::pair<int64_t, DevPtr>> tw_cache_;
+  std::vector<std::pair<std::vector<int64_t>, DevPtr>> tw_cache_;
 };
 
 // A length-n complex transform over `batch` rows (row distances idist / odist)

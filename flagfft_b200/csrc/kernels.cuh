@@ -47,7 +47,8 @@ struct TileArgs {
   int n;      // logical length: Bluestein n, Rader p, real-transform n; else core.L
   Core core;   // Dit stages, or the forward DIF stages of a convolution
   Core core2;  // inverse DIT stages of a convolution (radices reversed)
-  const cpx<T> *tw;     // W_L^m, m < core.L
+  const cpx<T> *tw;     // per-stage twiddle blocks of core (Core::twoff)
+  const cpx<T> *tw2;    // per-stage twiddle blocks of core2
   const cpx<T> *chirp;  // Bluestein chirp, n entries (direction folded in)
   const cpx<T> *kern;   // convolution kernel spectrum / L, in DIF position order
   const int *perm_in;   // Rader: q -> g^-q mod p
@@ -72,8 +73,6 @@ struct TileArgs {
   // 1: Stockham ping-pong path (C2C passes whose two buffers fit; convolution
   // kernels then in natural order).  0: in-place DIT/DIF path.
   int pp;
-  // ping-pong path: 1 = the twiddle table is staged in shared memory after the slots
-  int tw_smem;
 };
 
 // Real-transform pre/post processing between the passes of a multi-pass

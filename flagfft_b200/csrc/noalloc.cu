@@ -20,14 +20,16 @@ namespace {
 
 // Workspace: up to 2^22 complex64 elements (32 MiB) of batch * n.
 constexpr long long kNoAllocMaxElems = 1ll << 22;
-// Stage twiddles W_4096^m; a length-L pass (L | 4096) reads them with stride 4096 / L.
+// Per-stage twiddle blocks of the radix-16 cores of every power of two 2..4096
+// (the block set of length 2^l at offset 2^l - l - 1; 8178 entries in all).
 constexpr int kRootLen = 4096;
+constexpr int kStageTableLen = 8192;
 // Four-step twiddle W_n^m = hi[m >> 12] * lo[m & 4095] for n <= 2^24.
 constexpr int kSplitBits = 12;
 constexpr int kSplit = 1 << kSplitBits;
 
 static __device__ __align__(256) cpx<float> g_scratch[kNoAllocMaxElems];
-static __device__ __align__(256) cpx<float> g_roots[kRootLen];
+static __device__ __align__(256) cpx<float> g_roots[kStageTableLen];
 static __device__ __align__(256) cpx<float> g_ptw_lo[kSplit];
 static __device__ __align__(256) cpx<float> g_ptw_hi[kSplit];
 
@@ -49,6 +51,36 @@ __global__ void k_fill_roots(cpx<float> *dst, int count, long long n, long long 
   }
 }
 
+// Offset of the length-2^l core's stage blocks in g_roots.
+__host__ __device__ inline int stage_table_offset(int l) { return (1 << l) - l - 1; }
+
+// Fills the per-stage twiddle blocks of pow2_core(2^l), l = 1..12: entry
+// [r - 1][k] of stage s is W_{span R}^{r k} (span = 16^s, R = 16 or the
+// smaller last radix), k < span.
+__global__ void k_fill_stage_tables(cpx<float> *dst) {
+  for (int l = 1; l <= 12; ++l) {
+    const int L = 1 << l;
+    cpx<float> *t = dst + stage_table_offset(l);
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < L - 1; e += gridDim.x * blockDim.x) {
+      int span = 1, rem = L, off = 0;
+      while (rem > 1) {
+        const int R = rem >= 16 ? 16 : rem;
+        const int size = (R - 1) * span;
+        if (e < off + size) {
+          const int r = 1 + (e - off) / span, k = (e - off) % span;
+          double sn, cs;
+          sincospi(-2.0 * (double)(r * k) / (double)(span * R), &sn, &cs);
+          t[e] = mk((float)cs, (float)sn);
+          break;
+        }
+        off += size;
+        span *= R;
+        rem /= R;
+      }
+    }
+  }
+}
+
 // Device addresses of the static arrays for the current device; filled once
 // per device (the first call on a device does this set-up).
 cudaError_t device_state(DeviceState **out) {
@@ -63,7 +95,7 @@ cudaError_t device_state(DeviceState **out) {
     if ((e = cudaGetSymbolAddress(reinterpret_cast<void **>(&st.roots), g_roots)) != cudaSuccess) return e;
     if ((e = cudaGetSymbolAddress(reinterpret_cast<void **>(&st.lo), g_ptw_lo)) != cudaSuccess) return e;
     if ((e = cudaGetSymbolAddress(reinterpret_cast<void **>(&st.hi), g_ptw_hi)) != cudaSuccess) return e;
-    k_fill_roots<<<16, 256>>>(st.roots, kRootLen, kRootLen, 1);
+    k_fill_stage_tables<<<16, 256>>>(st.roots);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if ((e = cudaDeviceSynchronize()) != cudaSuccess) return e;
     st.ready = true;
@@ -76,12 +108,13 @@ Core pow2_core(int L) {
   // radix-16 stages, one smaller power-of-two stage for the remainder
   Core c{};
   c.L = L;
-  int rem = L, span = 1, s = 0;
+  int rem = L, span = 1, s = 0, off = 0;
   while (rem > 1) {
     const int r = rem >= 16 ? 16 : rem;
     c.radix[s] = r;
     c.span[s] = span;
-    c.tws[s] = (L / (span * r)) * (kRootLen / L);  // index into the W_4096 table
+    c.twoff[s] = off;
+    off += (r - 1) * span;
     c.sdiv[s] = make_fastdiv((uint32_t)span);
     c.rdiv[s] = make_fastdiv((uint32_t)r);
     span *= r;
@@ -106,7 +139,9 @@ TileArgs<float> pass_args(int L, int G, long long nbatch, long long ib, long lon
   a.inv = inverse ? 1 : 0;
   a.n = L;
   a.core = pow2_core(L);
-  a.tw = roots;
+  int l = 0;
+  while ((1 << l) < L) ++l;
+  a.tw = roots + stage_table_offset(l);
   a.pp = 1;
   a.wfast = ii > ig ? 1 : 0;
   const int rmax = L >= 16 ? 16 : L;

@@ -213,7 +213,7 @@ FFB_HD void tile_body(const TileArgs<T> &a, long long bx, long long by, cpx<T> *
         buf[Swz<T>::phys(p)] = cmul(v, ldg_c(kern + p));
       }
       sync();
-      run_dit<T>(buf, a.core2, tid, tpt, a.tw, true, sync);
+      run_dit<T>(buf, a.core2, tid, tpt, a.tw2, true, sync);
     }
   });
 
@@ -361,8 +361,7 @@ FFB_HD void tile_body(const TileArgs<T> &a, long long bx, long long by, cpx<T> *
 
 // Stockham ping-pong pass for C2C tiles.  A coalesced load phase fills
 // buffer 0 of every slot (natural order, chirp / permutation / zero padding
-// applied) and, when a.tw_smem, copies the twiddle table next to the slots;
-// all stages run shared -> shared (one code path per radix, warm in the
+// applied); all stages run shared -> shared (one code path per radix, warm in the
 // instruction cache after the first stage); a coalesced store phase writes
 // the result (unchirp / scatter / four-step twiddle applied).
 // Slot layout: two buffers of pp_size(L) and three spare elements (Rader x0,
@@ -387,7 +386,6 @@ FFB_HD void tile_body_pp(const TileArgs<T> &a, long long bx, long long by, cpx<T
   const int wlive = (int)((a.G - g0) < W ? (a.G - g0) : W);  // live transforms in this tile
   const int n = a.n;
   const int t0 = x.tid(), nt = x.nthreads();
-  cpx<T> *const tws = sm + W * slot_len;
   constexpr int U = sizeof(T) == 4 ? 16 : 8;
 
   // ---- load
@@ -418,9 +416,6 @@ FFB_HD void tile_body_pp(const TileArgs<T> &a, long long bx, long long by, cpx<T
       sm[w * slot_len + pp_pos(i)] = v;
     };
     chunked_loop<U, cpx<T>>(t0, nt, total, produce, consume);
-    if (a.tw_smem) {
-      for (int m = t0; m < L; m += nt) tws[m] = ldg_c(a.tw + m);
-    }
     if constexpr (KIND == 2) {
       for (int w = t0; w < W; w += nt) {
         const int wc = w < wlive ? w : wlive - 1;
@@ -432,7 +427,8 @@ FFB_HD void tile_body_pp(const TileArgs<T> &a, long long bx, long long by, cpx<T
 
   // ---- stages
   auto sync = [&]() { x.sync(); };
-  auto stages = [&](const auto &tw) {
+  {
+    const TwGlobal<T> tw{a.tw}, tw2{a.tw2};
     x.per_slot(W, [&](int slot, int tid, int tpt) {
       cpx<T> *const b0 = sm + slot * slot_len, *const b1 = b0 + Lq;
       const int S = a.core.nst;
@@ -451,14 +447,9 @@ FFB_HD void tile_body_pp(const TileArgs<T> &a, long long bx, long long by, cpx<T
           r[pp_pos(p)] = cmul(v, ldg_c(kern + p));
         }
         sync();
-        run_stockham_smem<T>(a.core2, r, (S & 1) ? b0 : b1, tid, tpt, tw, true, sync);
+        run_stockham_smem<T>(a.core2, r, (S & 1) ? b0 : b1, tid, tpt, tw2, true, sync);
       }
     });
-  };
-  if (a.tw_smem) {
-    stages(TwShared<T>{tws});
-  } else {
-    stages(TwGlobal<T>{a.tw});
   }
 
   // ---- store
