@@ -5,9 +5,9 @@
 //  * One transform of length L lives in one CTA's shared memory (up to 227 KB:
 //    29056 complex64 / 14528 complex128 points).  Stages run in place; each
 //    butterfly reads and writes the same R positions, so a stage needs no
-//    second buffer and a thread holds only one butterfly (R <= 19 values) in
-//    registers at a time -- any L that fits in shared memory runs at any
-//    thread count.
+//    second buffer and a thread holds one butterfly of a large radix, or a
+//    group of up to 16 values of a small one, in registers at a time -- any L
+//    that fits in shared memory runs at any thread count.
 //  * DIT stages consume a digit-reversed buffer and leave natural order; DIF
 //    stages consume natural order and leave it digit-reversed.  A DIF pass with
 //    radices (R0..Rk) followed by a DIT pass with the radices reversed needs no
@@ -16,9 +16,10 @@
 //  * Shared-memory positions are XOR-swizzled inside aligned 16-element
 //    (complex64) / 8-element (complex128) groups so the stride-R accesses of
 //    the early stages and the digit-reversed loads spread over the banks.
-//  * Twiddles W_L^m come from a per-length table built on the host in FP64 and
-//    rounded once (the reference also builds its stage twiddles in double and
-//    casts, src/codegen/tables.cpp:39-69); the inverse direction conjugates.
+//  * Twiddles come from per-stage tables built on the host in extended
+//    precision and rounded once (the reference also builds its stage twiddles
+//    in double and casts, src/codegen/tables.cpp:39-69); the inverse direction
+//    conjugates.
 //  * Codelets are the forward DFT; the inverse is conj(DFT(conj x)), the same
 //    convention the reference's codelets use (python/flagfft_codegen/kernels.py:493-512).
 #pragma once
@@ -332,54 +333,113 @@ FFB_HD cpx<T> twiddle(const cpx<T> *__restrict__ tw, int m, bool inv) {
   return w;
 }
 
-// In-place DIT stage s: combine R sub-transforms of length Ls.
+// Butterflies a thread runs together in one stage: their loads are all issued
+// before any is consumed, so K * R shared-memory (and K * (R - 1) twiddle)
+// loads are in flight at once.  Full groups of K run first, the remaining
+// butterflies one at a time.
+template <int R>
+struct Group {
+  static constexpr int K = R <= 2 ? 2 : 1;
+};
+
+// Runs body.load(u, kk) for K butterflies u = u0 + kk * nthr, then
+// body.finish(kk) for each, over all u < nb: K at a time while whole groups
+// remain, then one at a time.
+template <int K, class Body>
+FFB_HD void grouped_butterflies(int tid, int nthr, int nb, Body &body) {
+  int u0 = tid;
+  if constexpr (K > 1) {
+#pragma unroll 1
+    for (; u0 + (K - 1) * nthr < nb; u0 += K * nthr) {
+#pragma unroll
+      for (int kk = 0; kk < K; ++kk) body.load(u0 + kk * nthr, kk);
+#pragma unroll
+      for (int kk = 0; kk < K; ++kk) body.finish(kk);
+    }
+  }
+#pragma unroll 1
+  for (; u0 < nb; u0 += nthr) {
+    body.load(u0, 0);
+    body.finish(0);
+  }
+}
+
+// In-place DIT stage s: combine R sub-transforms of length Ls.  Each of the
+// L/R butterflies reads and writes the same R positions, so a thread may hold
+// several butterflies between their loads and stores.
+template <int R, int K, typename T>
+struct DitBody {
+  cpx<T> *buf;
+  const cpx<T> *__restrict__ tw;
+  int Ls, toff;
+  FastDiv sdiv;
+  bool inv;
+  cpx<T> v[K][R];
+  int base[K];
+  FFB_HD void load(int u, int kk) {
+    const int b = (int)fdiv((uint32_t)u, sdiv);
+    const int j = u - b * Ls;
+    base[kk] = b * Ls * R + j;
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[kk][r] = buf[Swz<T>::phys(base[kk] + r * Ls)];
+    if (j != 0) {
+#pragma unroll
+      for (int r = 1; r < R; ++r) v[kk][r] = cmul(v[kk][r], twiddle(tw, toff + r * Ls + j, inv));
+    }
+  }
+  FFB_HD void finish(int kk) {
+    dft_dir<R, T>(v[kk], inv);
+#pragma unroll
+    for (int q = 0; q < R; ++q) buf[Swz<T>::phys(base[kk] + q * Ls)] = v[kk][q];
+  }
+};
+
 template <int R, typename T>
 FFB_HD void dit_stage_r(cpx<T> *buf, const Core &c, int s, int tid, int nthr,
                                             const cpx<T> *__restrict__ tw, bool inv) {
-  const int Ls = c.span[s];
-  const int toff = c.twoff[s] - Ls;  // row r starts at toff + r * Ls
-  const int nb = c.L / R;
-  for (int u = tid; u < nb; u += nthr) {
-    const int b = (int)fdiv((uint32_t)u, c.sdiv[s]);
-    const int j = u - b * Ls;
-    const int base = b * Ls * R + j;
-    cpx<T> v[R];
-#pragma unroll
-    for (int r = 0; r < R; ++r) v[r] = buf[Swz<T>::phys(base + r * Ls)];
-    if (j != 0) {
-#pragma unroll
-      for (int r = 1; r < R; ++r) v[r] = cmul(v[r], twiddle(tw, toff + r * Ls + j, inv));
-    }
-    dft_dir<R, T>(v, inv);
-#pragma unroll
-    for (int q = 0; q < R; ++q) buf[Swz<T>::phys(base + q * Ls)] = v[q];
-  }
+  constexpr int K = Group<R>::K;
+  // row r of the stage's twiddle block starts at twoff - Ls + r * Ls
+  DitBody<R, K, T> body{buf, tw, c.span[s], c.twoff[s] - c.span[s], c.sdiv[s], inv};
+  grouped_butterflies<K>(tid, nthr, c.L / R, body);
 }
 
 // In-place DIF stage s: split sub-transforms of length Ms into R interleaved
 // parts; outputs are multiplied by W_Ms^{q j} after the butterfly.
+template <int R, int K, typename T>
+struct DifBody {
+  cpx<T> *buf;
+  const cpx<T> *__restrict__ tw;
+  int Ms, stride, toff;
+  FastDiv sdiv;
+  bool inv;
+  cpx<T> v[K][R];
+  int base[K], jj[K];
+  FFB_HD void load(int u, int kk) {
+    const int b = (int)fdiv((uint32_t)u, sdiv);
+    jj[kk] = u - b * stride;
+    base[kk] = b * Ms + jj[kk];
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[kk][r] = buf[Swz<T>::phys(base[kk] + r * stride)];
+  }
+  FFB_HD void finish(int kk) {
+    dft_dir<R, T>(v[kk], inv);
+    if (jj[kk] != 0) {
+#pragma unroll
+      for (int q = 1; q < R; ++q) v[kk][q] = cmul(v[kk][q], twiddle(tw, toff + q * stride + jj[kk], inv));
+    }
+#pragma unroll
+    for (int q = 0; q < R; ++q) buf[Swz<T>::phys(base[kk] + q * stride)] = v[kk][q];
+  }
+};
+
 template <int R, typename T>
 FFB_HD void dif_stage_r(cpx<T> *buf, const Core &c, int s, int tid, int nthr,
                                             const cpx<T> *__restrict__ tw, bool inv) {
-  const int Ms = c.span[s];
-  const int stride = Ms / R;
-  const int toff = c.twoff[s] - stride;  // row q starts at toff + q * stride
-  const int nb = c.L / R;
-  for (int u = tid; u < nb; u += nthr) {
-    const int b = (int)fdiv((uint32_t)u, c.sdiv[s]);
-    const int j = u - b * stride;
-    const int base = b * Ms + j;
-    cpx<T> v[R];
-#pragma unroll
-    for (int r = 0; r < R; ++r) v[r] = buf[Swz<T>::phys(base + r * stride)];
-    dft_dir<R, T>(v, inv);
-    if (j != 0) {
-#pragma unroll
-      for (int q = 1; q < R; ++q) v[q] = cmul(v[q], twiddle(tw, toff + q * stride + j, inv));
-    }
-#pragma unroll
-    for (int q = 0; q < R; ++q) buf[Swz<T>::phys(base + q * stride)] = v[q];
-  }
+  constexpr int K = Group<R>::K;
+  const int Ms = c.span[s], stride = Ms / R;
+  // row q of the stage's twiddle block starts at twoff - stride + q * stride
+  DifBody<R, K, T> body{buf, tw, Ms, stride, c.twoff[s] - stride, c.sdiv[s], inv};
+  grouped_butterflies<K>(tid, nthr, c.L / R, body);
 }
 
 #define FFB_RADIX_SWITCH(R_, CALL)                                     \
@@ -452,30 +512,47 @@ struct TwGlobal {
   FFB_HD cpx<T> operator()(int m) const { return ldg_c(p + m); }
 };
 
-template <int R, typename T, class Src, class Dst, class Tw>
-FFB_HD void stockham_stage_r(const Core &c, int s, int tid, int nthr, const Tw &tw, bool inv, Src &src, Dst &dst) {
-  const int Ns = c.span[s];
-  const int toff = c.twoff[s] - Ns;  // row r starts at toff + r * Ns
-  const int nb = c.L / R;
-  const T sgn = inv ? (T)-1 : (T)1;
-  for (int j = tid; j < nb; j += nthr) {
-    const int k = j - (int)fdiv((uint32_t)j, c.sdiv[s]) * Ns;
-    cpx<T> v[R];
+template <int R, int K, typename T, class Src, class Dst, class Tw>
+struct StockhamBody {
+  const Tw &tw;
+  Src &src;
+  Dst &dst;
+  int Ns, toff, nb;
+  FastDiv sdiv;
+  T sgn;
+  bool inv;
+  cpx<T> v[K][R];
+  int jq[K], kq[K];
+  FFB_HD void load(int j, int kk) {
+    jq[kk] = j;
+    kq[kk] = j - (int)fdiv((uint32_t)j, sdiv) * Ns;
 #pragma unroll
-    for (int r = 0; r < R; ++r) v[r] = src(j + r * nb);
-    if (k != 0) {
+    for (int r = 0; r < R; ++r) v[kk][r] = src(j + r * nb);
+    if (kq[kk] != 0) {
 #pragma unroll
       for (int r = 1; r < R; ++r) {
-        cpx<T> w = tw(toff + r * Ns + k);
+        cpx<T> w = tw(toff + r * Ns + kq[kk]);
         w.y *= sgn;
-        v[r] = cmul(v[r], w);
+        v[kk][r] = cmul(v[kk][r], w);
       }
     }
-    dft_dir<R, T>(v, inv);
-    const int base = (j - k) * R + k;
-#pragma unroll
-    for (int q = 0; q < R; ++q) dst(base + q * Ns, v[q]);
   }
+  FFB_HD void finish(int kk) {
+    dft_dir<R, T>(v[kk], inv);
+    const int base = (jq[kk] - kq[kk]) * R + kq[kk];
+#pragma unroll
+    for (int q = 0; q < R; ++q) dst(base + q * Ns, v[kk][q]);
+  }
+};
+
+template <int R, typename T, class Src, class Dst, class Tw>
+FFB_HD void stockham_stage_r(const Core &c, int s, int tid, int nthr, const Tw &tw, bool inv, Src &src, Dst &dst) {
+  constexpr int K = Group<R>::K;
+  const int Ns = c.span[s], nb = c.L / R;
+  // row r of the stage's twiddle block starts at twoff - Ns + r * Ns
+  StockhamBody<R, K, T, Src, Dst, Tw> body{tw, src, dst, Ns, c.twoff[s] - Ns, nb, c.sdiv[s],
+                                           inv ? (T)-1 : (T)1, inv};
+  grouped_butterflies<K>(tid, nthr, nb, body);
 }
 
 // Shared-memory reader / writer of a ping-pong buffer.

@@ -163,7 +163,8 @@ struct TilePass final : PassBase {
 
   std::string describe() const override {
     std::ostringstream o;
-    o << kind_name(kind) << "/" << io_name(io) << " " << (sizeof(T) == 4 ? "f32" : "f64") << " L=" << a.core.L
+    o << (a.regcol ? "register-columns" : kind_name(kind)) << "/" << io_name(io) << " "
+      << (sizeof(T) == 4 ? "f32" : "f64") << " L=" << a.core.L
       << " radices=[";
     for (int s = 0; s < a.core.nst; ++s) o << (s ? "," : "") << a.core.radix[s];
     o << "] n=" << a.n << " transforms=" << a.nbatch << "x" << a.G << " per_cta=" << a.W
@@ -350,6 +351,23 @@ class Builder {
       std::vector<int> rev(spec.radices.rbegin(), spec.radices.rend());
       a.core2 = make_dit_core(L, rev);
       if (spec.kind != CoreKind::Conv) fill_convolution(a, spec, inverse);  // Conv: caller supplies the kernel
+    }
+    // one-codelet transforms lying side by side in memory on both sides run
+    // one per thread in registers
+    if (spec.kind == CoreKind::Dit && io == IoKind::C2C && spec.radices.size() == 1 && spec.radices[0] == L &&
+        regcol_supports((int)L) && ig == 1 && og == 1) {
+      a.pp = 0;
+      a.regcol = 1;
+      a.W = 1;
+      a.tpt = 1;
+      p->kind = spec.kind;
+      p->io = io;
+      p->smem = 0;
+      p->src = src;
+      p->dst = dst;
+      TilePass<T> *raw = p.get();
+      prog_.passes.push_back(std::move(p));
+      return raw;
     }
     a.tw = table_stage_twiddles(a.core, a.pp == 0 && spec.kind != CoreKind::Dit);
     if (spec.kind != CoreKind::Dit) a.tw2 = table_stage_twiddles(a.core2, false);

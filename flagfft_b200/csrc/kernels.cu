@@ -111,6 +111,7 @@ template cudaError_t launch_real_pre<double>(const cpx<double> *, cpx<double> *,
 template <typename T>
 cudaError_t launch_tile(const TileArgs<T> &a, CoreKind kind, IoKind io, size_t smem, cudaStream_t s) {
   const int k = (int)kind, o = (int)io;
+  if (a.regcol) return launch_regcol<T>(a, s);
   if (a.pp && o == 0) {
     switch (k) {
       case 0: return tile::launch_pp<T, 0>(a, smem, s);

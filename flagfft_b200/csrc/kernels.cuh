@@ -73,6 +73,10 @@ struct TileArgs {
   // 1: Stockham ping-pong path (C2C passes whose two buffers fit; convolution
   // kernels then in natural order).  0: in-place DIT/DIF path.
   int pp;
+  // 1: register column pass -- one thread per transform, the whole transform
+  // one codelet in registers, no shared memory (Dit core with one stage,
+  // C2C, transforms contiguous in memory on both sides: ig == og == 1).
+  int regcol;
 };
 
 // Real-transform pre/post processing between the passes of a multi-pass
@@ -90,6 +94,20 @@ cudaError_t launch_real_pre(const cpx<T> *x, cpx<T> *z, long long batch, long lo
 
 template <typename T>
 cudaError_t launch_tile(const TileArgs<T> &a, CoreKind kind, IoKind io, size_t smem_bytes, cudaStream_t stream);
+
+// Register column pass (TileArgs::regcol); defined in regcol.cu.
+template <typename T>
+cudaError_t launch_regcol(const TileArgs<T> &a, cudaStream_t stream);
+// Codelet lengths the register column pass has kernels for.
+inline bool regcol_supports(int L) {
+  switch (L) {
+    case 2: case 3: case 4: case 5: case 6: case 7: case 8: case 9: case 10:
+    case 11: case 12: case 13: case 15: case 16: case 17: case 19:
+      return true;
+    default:
+      return false;
+  }
+}
 
 // Shared memory one transform of the pass occupies (bytes).
 template <typename T>

@@ -1,0 +1,90 @@
+// Register column pass: one thread per transform for single-codelet lengths
+// (L <= 19) whose transforms sit side by side in memory (input and output
+// transform distance 1, elements strided) -- the column passes of the
+// three-pass Bluestein chain.  A warp's load or store of element i touches 32
+// consecutive transforms, so every access is a full coalesced line; the
+// transform itself is one codelet in registers, so the pass needs no shared
+// memory and no barrier, and as many threads as the register file allows stay
+// resident to keep loads in flight.  Chirp-on-load (chirp_mode 1),
+// chirp-on-store (chirp_mode 2) and the four-step post-twiddle follow the tile
+// passes' definitions (kernels.cuh).
+#include "kernels.cuh"
+
+namespace ffb {
+namespace {
+
+template <typename T, int R>
+FFB_HD void regcol_transform(const TileArgs<T> &a, long long by, long long g) {
+  const cpx<T> *in = reinterpret_cast<const cpx<T> *>(a.in) + by * a.ib + g * a.ig;
+  cpx<T> *out = reinterpret_cast<cpx<T> *>(a.out) + by * a.ob + g * a.og;
+  cpx<T> v[R];
+  if (a.chirp_mode == 1) {
+#pragma unroll
+    for (int i = 0; i < R; ++i) {
+      const long long j = (long long)i * a.cj_e + g * a.cj_g;
+      v[i] = j < a.n ? cmul(ldg_c(in + i * a.ii), ldg_c(a.chirp + j)) : mk((T)0, (T)0);
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < R; ++i) v[i] = ldg_c(in + i * a.ii);
+  }
+  dft_dir<R, T>(v, a.inv != 0);
+  if (a.chirp_mode == 2) {
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+      const long long j = (long long)k * a.cj_e + g * a.cj_g;
+      if (j < a.n) out[k * a.ok] = cmul(v[k], ldg_c(a.chirp + j));
+    }
+  } else if (a.post_twiddle) {
+    // output k of transform g times W_N^{g k} = hi[m / split] * lo[m % split]
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+      const uint32_t m = (uint32_t)(g * k);
+      const uint32_t hi = fdiv(m, a.ptw_div);
+      cpx<T> t = cmul(ldg_c(a.ptw_hi + hi), ldg_c(a.ptw_lo + (m - hi * a.ptw_div.d)));
+      if (a.inv) t.y = -t.y;
+      out[k * a.ok] = cmul(v[k], t);
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < R; ++k) out[k * a.ok] = v[k];
+  }
+}
+
+constexpr int kRegcolThreads = 128;
+
+template <typename T, int R>
+__global__ void __launch_bounds__(kRegcolThreads) k_regcol(const __grid_constant__ TileArgs<T> a) {
+  const long long g = (long long)blockIdx.x * kRegcolThreads + threadIdx.x;
+  if (g < a.G) regcol_transform<T, R>(a, (long long)blockIdx.y, g);
+}
+
+template <typename T, int R>
+cudaError_t launch_r(const TileArgs<T> &a, cudaStream_t s) {
+#ifndef FFB_HOST_EMULATION
+  dim3 grid((unsigned)((a.G + kRegcolThreads - 1) / kRegcolThreads), (unsigned)a.nbatch, 1);
+  k_regcol<T, R><<<grid, kRegcolThreads, 0, s>>>(a);
+  return cudaGetLastError();
+#else
+  (void)s;
+  for (long long by = 0; by < a.nbatch; ++by)
+    for (long long g = 0; g < a.G; ++g) regcol_transform<T, R>(a, by, g);
+  return cudaSuccess;
+#endif
+}
+
+}  // namespace
+
+template <typename T>
+cudaError_t launch_regcol(const TileArgs<T> &a, cudaStream_t s) {
+  if (a.core.nst != 1 || a.core.radix[0] != a.core.L) return cudaErrorInvalidValue;
+#define FFB_REGCOL(R) return launch_r<T, R>(a, s)
+  FFB_RADIX_SWITCH(a.core.L, FFB_REGCOL)
+#undef FFB_REGCOL
+  return cudaErrorInvalidValue;
+}
+
+template cudaError_t launch_regcol<float>(const TileArgs<float> &, cudaStream_t);
+template cudaError_t launch_regcol<double>(const TileArgs<double> &, cudaStream_t);
+
+}  // namespace ffb
