@@ -339,7 +339,7 @@ FFB_HD cpx<T> twiddle(const cpx<T> *__restrict__ tw, int m, bool inv) {
 // butterflies one at a time.
 template <int R>
 struct Group {
-  static constexpr int K = R <= 2 ? 2 : 1;
+  static constexpr int K = 1;
 };
 
 // Runs body.load(u, kk) for K butterflies u = u0 + kk * nthr, then
@@ -382,10 +382,9 @@ struct DitBody {
     base[kk] = b * Ls * R + j;
 #pragma unroll
     for (int r = 0; r < R; ++r) v[kk][r] = buf[Swz<T>::phys(base[kk] + r * Ls)];
-    if (j != 0) {
+    // j == 0 reads W^0 = 1 from the table: no branch
 #pragma unroll
-      for (int r = 1; r < R; ++r) v[kk][r] = cmul(v[kk][r], twiddle(tw, toff + r * Ls + j, inv));
-    }
+    for (int r = 1; r < R; ++r) v[kk][r] = cmul(v[kk][r], twiddle(tw, toff + r * Ls + j, inv));
   }
   FFB_HD void finish(int kk) {
     dft_dir<R, T>(v[kk], inv);
@@ -423,10 +422,8 @@ struct DifBody {
   }
   FFB_HD void finish(int kk) {
     dft_dir<R, T>(v[kk], inv);
-    if (jj[kk] != 0) {
 #pragma unroll
-      for (int q = 1; q < R; ++q) v[kk][q] = cmul(v[kk][q], twiddle(tw, toff + q * stride + jj[kk], inv));
-    }
+    for (int q = 1; q < R; ++q) v[kk][q] = cmul(v[kk][q], twiddle(tw, toff + q * stride + jj[kk], inv));
 #pragma unroll
     for (int q = 0; q < R; ++q) buf[Swz<T>::phys(base[kk] + q * stride)] = v[kk][q];
   }
@@ -528,13 +525,12 @@ struct StockhamBody {
     kq[kk] = j - (int)fdiv((uint32_t)j, sdiv) * Ns;
 #pragma unroll
     for (int r = 0; r < R; ++r) v[kk][r] = src(j + r * nb);
-    if (kq[kk] != 0) {
+    // k == 0 reads W^0 = 1 from the table: no branch
 #pragma unroll
-      for (int r = 1; r < R; ++r) {
-        cpx<T> w = tw(toff + r * Ns + kq[kk]);
-        w.y *= sgn;
-        v[kk][r] = cmul(v[kk][r], w);
-      }
+    for (int r = 1; r < R; ++r) {
+      cpx<T> w = tw(toff + r * Ns + kq[kk]);
+      w.y *= sgn;
+      v[kk][r] = cmul(v[kk][r], w);
     }
   }
   FFB_HD void finish(int kk) {
@@ -609,19 +605,19 @@ FFB_HD void run_stockham(const Core &c, cpx<T> *b0, cpx<T> *b1, int tid, int nth
 // any is consumed, so a thread keeps U loads in flight instead of one.
 template <int U, class V, class Produce, class Consume>
 FFB_HD void chunked_loop(int t0, int nt, int total, Produce &&produce, Consume &&consume) {
-  for (int base = t0; base < total; base += U * nt) {
+  int base = t0;
+  // whole chunks: no per-element bounds test
+#pragma unroll 1
+  for (; base + (U - 1) * nt < total; base += U * nt) {
     V v[U];
 #pragma unroll
-    for (int u = 0; u < U; ++u) {
-      const int e = base + u * nt;
-      if (e < total) v[u] = produce(e);
-    }
+    for (int u = 0; u < U; ++u) v[u] = produce(base + u * nt);
 #pragma unroll
-    for (int u = 0; u < U; ++u) {
-      const int e = base + u * nt;
-      if (e < total) consume(e, v[u]);
-    }
+    for (int u = 0; u < U; ++u) consume(base + u * nt, v[u]);
   }
+  // the rest, one element at a time
+#pragma unroll 1
+  for (; base < total; base += nt) consume(base, produce(base));
 }
 
 // All stages of `c` shared -> shared: stage s reads buffer (s even ? src : oth)

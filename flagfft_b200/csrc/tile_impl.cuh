@@ -90,6 +90,13 @@ struct HostX {
   }
 };
 
+// A value with the offset it goes to.
+template <typename T>
+struct ElemAt {
+  cpx<T> v;
+  int at;
+};
+
 // Splits a flat element counter e over (transform w, element i) of a CTA tile.
 FFB_HD void split_elem(int e, int W, int Lx, int wfast, const FastDiv &wdiv, const FastDiv &ldiv, int &w, int &i) {
   if (wfast) {
@@ -391,31 +398,29 @@ FFB_HD void tile_body_pp(const TileArgs<T> &a, long long bx, long long by, cpx<T
   // ---- load
   {
     const int total = W * L;
-    auto produce = [&](int e) -> cpx<T> {
+    // produce: the element's value and its shared-memory position
+    auto produce = [&](int e) -> ElemAt<T> {
       int w, i;
       split_elem(e, W, L, a.wfast, a.wdiv, a.ldiv, w, i);
       const int wc = w < wlive ? w : wlive - 1;
       const cpx<T> *xin = in + wc * ig;
+      const int at = w * slot_len + pp_pos(i);
       if constexpr (KIND == 0) {
         if (a.chirp_mode == 1) {
           const long long j = (long long)i * a.cj_e + (g0 + wc) * a.cj_g;
-          return j < n ? cmul(ldg_c(xin + i * ii), ldg_c(a.chirp + j)) : mk((T)0, (T)0);
+          return {j < n ? cmul(ldg_c(xin + i * ii), ldg_c(a.chirp + j)) : mk((T)0, (T)0), at};
         }
-        return ldg_c(xin + i * ii);
+        return {ldg_c(xin + i * ii), at};
       } else if constexpr (KIND == 1) {
-        return i < n ? cmul(ldg_c(xin + i * ii), ldg_c(a.chirp + i)) : mk((T)0, (T)0);
+        return {i < n ? cmul(ldg_c(xin + i * ii), ldg_c(a.chirp + i)) : mk((T)0, (T)0), at};
       } else if constexpr (KIND == 2) {
-        return ldg_c(xin + ldg_v(a.perm_in + i) * ii);
+        return {ldg_c(xin + ldg_v(a.perm_in + i) * ii), at};
       } else {
-        return ldg_c(xin + i * ii);
+        return {ldg_c(xin + i * ii), at};
       }
     };
-    auto consume = [&](int e, cpx<T> v) {
-      int w, i;
-      split_elem(e, W, L, a.wfast, a.wdiv, a.ldiv, w, i);
-      sm[w * slot_len + pp_pos(i)] = v;
-    };
-    chunked_loop<U, cpx<T>>(t0, nt, total, produce, consume);
+    auto consume = [&](int, ElemAt<T> p) { sm[p.at] = p.v; };
+    chunked_loop<U, ElemAt<T>>(t0, nt, total, produce, consume);
     if constexpr (KIND == 2) {
       for (int w = t0; w < W; w += nt) {
         const int wc = w < wlive ? w : wlive - 1;
@@ -466,41 +471,34 @@ FFB_HD void tile_body_pp(const TileArgs<T> &a, long long bx, long long by, cpx<T
   };
   const int nout = KIND == 1 ? n : L;
   const int total = W * nout;
-  auto produce = [&](int e) -> cpx<T> {
+  // produce: the output value and its offset from `out`, or -1 when the
+  // element is not written (a dead transform of the last tile, or a
+  // chirp-on-store position past n)
+  auto produce = [&](int e) -> ElemAt<T> {
     int w, k;
     split_elem(e, W, nout, a.wfast, a.wdiv, KIND == 1 ? a.ndiv : a.ldiv, w, k);
     const int wc = w < wlive ? w : wlive - 1;
+    const int at = w < wlive ? w * og + k * ok : -1;
     const cpx<T> *bw = sm + w * slot_len;
     cpx<T> v = bw[res_off + pp_pos(k)];
     if constexpr (KIND == 0) {
       if (a.chirp_mode == 2) {
         const long long j = (long long)k * a.cj_e + (g0 + wc) * a.cj_g;
-        return j < n ? cmul(v, ldg_c(a.chirp + j)) : v;
+        return j < n ? ElemAt<T>{cmul(v, ldg_c(a.chirp + j)), at} : ElemAt<T>{v, -1};
       }
-      return post_twiddle(v, g0 + wc, k);
+      return {post_twiddle(v, g0 + wc, k), at};
     } else if constexpr (KIND == 1) {
-      return cmul(v, ldg_c(a.chirp + k));
+      return {cmul(v, ldg_c(a.chirp + k)), at};
     } else if constexpr (KIND == 2) {
-      return bw[2 * Lq] + v;
+      return {bw[2 * Lq] + v, w < wlive ? w * og + ldg_v(a.perm_out + k) * ok : -1};
     } else {
-      return post_twiddle(v, g0 + wc, k);
+      return {post_twiddle(v, g0 + wc, k), at};
     }
   };
-  auto consume = [&](int e, cpx<T> v) {
-    int w, k;
-    split_elem(e, W, nout, a.wfast, a.wdiv, KIND == 1 ? a.ndiv : a.ldiv, w, k);
-    if (w >= wlive) return;
-    cpx<T> *yout = out + w * og;
-    if constexpr (KIND == 0) {
-      if (a.chirp_mode == 2 && (long long)k * a.cj_e + (g0 + w) * a.cj_g >= n) return;
-      yout[k * ok] = v;
-    } else if constexpr (KIND == 2) {
-      yout[ldg_v(a.perm_out + k) * ok] = v;
-    } else {
-      yout[k * ok] = v;
-    }
+  auto consume = [&](int, ElemAt<T> p) {
+    if (p.at >= 0) out[p.at] = p.v;
   };
-  chunked_loop<U, cpx<T>>(t0, nt, total, produce, consume);
+  chunked_loop<U, ElemAt<T>>(t0, nt, total, produce, consume);
   if constexpr (KIND == 2) {
     for (int w = t0; w < wlive; w += nt) out[w * og] = sm[w * slot_len + 2 * Lq + 1];
   }
