@@ -31,6 +31,9 @@
 // sequentially (one "thread", barriers as no-ops) to check index arithmetic
 // without a GPU.
 #define FFB_HD __host__ __device__ __forceinline__
+// Lambdas in kernel bodies: always inlined, so shared-memory pointers keep
+// their address space and no call frame appears.
+#define FFB_INL __attribute__((always_inline))
 
 namespace ffb {
 
@@ -269,10 +272,11 @@ constexpr int kMaxStages = 16;
 //   DIT stage s:  span[s] = R0*...*R(s-1)       (sub-transform length before it)
 //   DIF stage s:  span[s] = L / (R0*...*R(s-1)) (sub-length it splits)
 //   twoff[s] is the offset of stage s's twiddle block in the core's table:
-//   R(s)-1 rows of `inner` entries, row r-1 entry j = W_{inner R(s)}^{r j} with
-//   inner = span[s] (DIT / Stockham) or span[s]/R(s) (DIF), so one butterfly
-//   reads its R-1 twiddles from R-1 rows at the same column j and neighbouring
-//   butterflies read neighbouring entries.
+//   R(s)-1 rows of `inner` entries (inner = span[s] for DIT and Stockham
+//   stages, span[s]/R(s) for DIF); entry j of row r-1 is W_{inner R}^{r j},
+//   conjugated in a table built for the inverse direction.  Neighbouring
+//   butterflies read neighbouring entries of each row (one coalesced load per
+//   row across a warp), and no twiddle needs a sign change at run time.
 //   sdiv[s] divides the butterfly index by the inner block length
 //   (DIT: span[s]; DIF: span[s]/R(s)).
 //   rdiv[s] divides by R(s) (digit reversal).
@@ -325,118 +329,86 @@ FFB_HD V ldg_v(const V *p) {
 #endif
 }
 
-// Twiddle tw[m] (forward sign) or its conjugate (inverse).
-template <typename T>
-FFB_HD cpx<T> twiddle(const cpx<T> *__restrict__ tw, int m, bool inv) {
-  cpx<T> w = ldg_c(tw + m);
-  if (inv) w.y = -w.y;
-  return w;
+// w[r-1] = blk[(r-1) * inner + j], r = 1..R-1: the R-1 twiddles of column j
+// of a stage block.
+template <int R, typename T>
+FFB_HD void load_tw_col(const cpx<T> *__restrict__ blk, int inner, int j, cpx<T> *w) {
+  const cpx<T> *p = blk + j;
+#pragma unroll
+  for (int r = 1; r < R; ++r) w[r - 1] = ldg_c(p + (r - 1) * inner);
 }
 
-// Butterflies a thread runs together in one stage: their loads are all issued
-// before any is consumed, so K * R shared-memory (and K * (R - 1) twiddle)
-// loads are in flight at once.  Full groups of K run first, the remaining
-// butterflies one at a time.
-template <int R>
-struct Group {
-  static constexpr int K = 1;
-};
-
-// Runs body.load(u, kk) for K butterflies u = u0 + kk * nthr, then
-// body.finish(kk) for each, over all u < nb: K at a time while whole groups
-// remain, then one at a time.
-template <int K, class Body>
-FFB_HD void grouped_butterflies(int tid, int nthr, int nb, Body &body) {
-  int u0 = tid;
-  if constexpr (K > 1) {
-#pragma unroll 1
-    for (; u0 + (K - 1) * nthr < nb; u0 += K * nthr) {
+// Codelet in a compile-time direction: the inverse is conj(DFT(conj x)); the
+// conjugations fold into the codelet's additions.
+template <int R, bool INV, typename T>
+FFB_HD void dft_fixed(cpx<T> *v) {
+  if constexpr (INV) {
 #pragma unroll
-      for (int kk = 0; kk < K; ++kk) body.load(u0 + kk * nthr, kk);
-#pragma unroll
-      for (int kk = 0; kk < K; ++kk) body.finish(kk);
-    }
+    for (int r = 0; r < R; ++r) v[r].y = -v[r].y;
   }
-#pragma unroll 1
-  for (; u0 < nb; u0 += nthr) {
-    body.load(u0, 0);
-    body.finish(0);
+  Dft<R, T>::run(v);
+  if constexpr (INV) {
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r].y = -v[r].y;
   }
 }
 
-// In-place DIT stage s: combine R sub-transforms of length Ls.  Each of the
-// L/R butterflies reads and writes the same R positions, so a thread may hold
-// several butterflies between their loads and stores.
-template <int R, int K, typename T>
-struct DitBody {
-  cpx<T> *buf;
-  const cpx<T> *__restrict__ tw;
-  int Ls, toff;
-  FastDiv sdiv;
-  bool inv;
-  cpx<T> v[K][R];
-  int base[K];
-  FFB_HD void load(int u, int kk) {
-    const int b = (int)fdiv((uint32_t)u, sdiv);
-    const int j = u - b * Ls;
-    base[kk] = b * Ls * R + j;
-#pragma unroll
-    for (int r = 0; r < R; ++r) v[kk][r] = buf[Swz<T>::phys(base[kk] + r * Ls)];
-    // j == 0 reads W^0 = 1 from the table: no branch
-#pragma unroll
-    for (int r = 1; r < R; ++r) v[kk][r] = cmul(v[kk][r], twiddle(tw, toff + r * Ls + j, inv));
-  }
-  FFB_HD void finish(int kk) {
-    dft_dir<R, T>(v[kk], inv);
-#pragma unroll
-    for (int q = 0; q < R; ++q) buf[Swz<T>::phys(base[kk] + q * Ls)] = v[kk][q];
-  }
-};
-
+// In-place DIT stage s: combine R sub-transforms of length Ls.  The first
+// stage (Ls == 1) has only unit twiddles and skips them.
 template <int R, typename T>
 FFB_HD void dit_stage_r(cpx<T> *buf, const Core &c, int s, int tid, int nthr,
                                             const cpx<T> *__restrict__ tw, bool inv) {
-  constexpr int K = Group<R>::K;
-  // row r of the stage's twiddle block starts at twoff - Ls + r * Ls
-  DitBody<R, K, T> body{buf, tw, c.span[s], c.twoff[s] - c.span[s], c.sdiv[s], inv};
-  grouped_butterflies<K>(tid, nthr, c.L / R, body);
+  const int Ls = c.span[s];
+  const cpx<T> *blk = tw + c.twoff[s];
+  const FastDiv sd = c.sdiv[s];
+  const int nb = c.L / R;
+  for (int u = tid; u < nb; u += nthr) {
+    const int b = (int)fdiv((uint32_t)u, sd);
+    const int j = u - b * Ls;
+    const int base = b * Ls * R + j;
+    cpx<T> v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r] = buf[Swz<T>::phys(base + r * Ls)];
+    if (Ls > 1) {
+      cpx<T> w[R - 1];
+      load_tw_col<R, T>(blk, Ls, j, w);
+#pragma unroll
+      for (int r = 1; r < R; ++r) v[r] = cmul(v[r], w[r - 1]);
+    }
+    dft_dir<R, T>(v, inv);
+#pragma unroll
+    for (int q = 0; q < R; ++q) buf[Swz<T>::phys(base + q * Ls)] = v[q];
+  }
 }
 
 // In-place DIF stage s: split sub-transforms of length Ms into R interleaved
-// parts; outputs are multiplied by W_Ms^{q j} after the butterfly.
-template <int R, int K, typename T>
-struct DifBody {
-  cpx<T> *buf;
-  const cpx<T> *__restrict__ tw;
-  int Ms, stride, toff;
-  FastDiv sdiv;
-  bool inv;
-  cpx<T> v[K][R];
-  int base[K], jj[K];
-  FFB_HD void load(int u, int kk) {
-    const int b = (int)fdiv((uint32_t)u, sdiv);
-    jj[kk] = u - b * stride;
-    base[kk] = b * Ms + jj[kk];
-#pragma unroll
-    for (int r = 0; r < R; ++r) v[kk][r] = buf[Swz<T>::phys(base[kk] + r * stride)];
-  }
-  FFB_HD void finish(int kk) {
-    dft_dir<R, T>(v[kk], inv);
-#pragma unroll
-    for (int q = 1; q < R; ++q) v[kk][q] = cmul(v[kk][q], twiddle(tw, toff + q * stride + jj[kk], inv));
-#pragma unroll
-    for (int q = 0; q < R; ++q) buf[Swz<T>::phys(base[kk] + q * stride)] = v[kk][q];
-  }
-};
-
+// parts; outputs are multiplied by W_Ms^{q j} after the butterfly (none in
+// the last stage, Ms == R).
 template <int R, typename T>
 FFB_HD void dif_stage_r(cpx<T> *buf, const Core &c, int s, int tid, int nthr,
                                             const cpx<T> *__restrict__ tw, bool inv) {
-  constexpr int K = Group<R>::K;
-  const int Ms = c.span[s], stride = Ms / R;
-  // row q of the stage's twiddle block starts at twoff - stride + q * stride
-  DifBody<R, K, T> body{buf, tw, Ms, stride, c.twoff[s] - stride, c.sdiv[s], inv};
-  grouped_butterflies<K>(tid, nthr, c.L / R, body);
+  const int Ms = c.span[s];
+  const int stride = Ms / R;
+  const cpx<T> *blk = tw + c.twoff[s];
+  const FastDiv sd = c.sdiv[s];
+  const int nb = c.L / R;
+  for (int u = tid; u < nb; u += nthr) {
+    const int b = (int)fdiv((uint32_t)u, sd);
+    const int j = u - b * stride;
+    const int base = b * Ms + j;
+    cpx<T> v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r] = buf[Swz<T>::phys(base + r * stride)];
+    dft_dir<R, T>(v, inv);
+    if (stride > 1) {
+      cpx<T> w[R - 1];
+      load_tw_col<R, T>(blk, stride, j, w);
+#pragma unroll
+      for (int q = 1; q < R; ++q) v[q] = cmul(v[q], w[q - 1]);
+    }
+#pragma unroll
+    for (int q = 0; q < R; ++q) buf[Swz<T>::phys(base + q * stride)] = v[q];
+  }
 }
 
 #define FFB_RADIX_SWITCH(R_, CALL)                                     \
@@ -490,11 +462,9 @@ FFB_HD void run_dif(cpx<T> *buf, const Core &c, int tid, int nthr,
 //
 // Stage s with radix R and Ns = R0*...*R(s-1): butterfly j (< L/R) reads
 // elements j + r*L/R, multiplies input r by W_{Ns R}^{r (j mod Ns)}, and writes
-// output q to (j - j mod Ns)*R + j mod Ns + q*Ns.  The first stage reads the
-// caller's source and the last writes the caller's sink directly, so global
-// memory is read and written in the coalesced j + r*L/R pattern and the
-// stages in between ping-pong between two shared-memory buffers.  Uses the
-// DIT core's fields (span = Ns, twiddle block at twoff, sdiv = / Ns).
+// output q to (j - j mod Ns)*R + j mod Ns + q*Ns.  Stages ping-pong between two
+// shared-memory buffers; reads are unit-stride across a warp.  Uses the DIT
+// core's fields (span = Ns, twiddle block at twoff, sdiv = / Ns).
 // ---------------------------------------------------------------------------
 
 // Shared-memory position of element p in a ping-pong buffer: one pad element
@@ -502,53 +472,29 @@ FFB_HD void run_dif(cpx<T> *buf, const Core &c, int tid, int nthr,
 FFB_HD int pp_pos(int p) { return p + (p >> 4); }
 FFB_HD int pp_size(int L) { return ((L + (L >> 4) + 1) + 1) & ~1; }
 
-// Twiddle table reader (read-only data cache).
-template <typename T>
-struct TwGlobal {
-  const cpx<T> *p;
-  FFB_HD cpx<T> operator()(int m) const { return ldg_c(p + m); }
-};
-
-template <int R, int K, typename T, class Src, class Dst, class Tw>
-struct StockhamBody {
-  const Tw &tw;
-  Src &src;
-  Dst &dst;
-  int Ns, toff, nb;
-  FastDiv sdiv;
-  T sgn;
-  bool inv;
-  cpx<T> v[K][R];
-  int jq[K], kq[K];
-  FFB_HD void load(int j, int kk) {
-    jq[kk] = j;
-    kq[kk] = j - (int)fdiv((uint32_t)j, sdiv) * Ns;
-#pragma unroll
-    for (int r = 0; r < R; ++r) v[kk][r] = src(j + r * nb);
-    // k == 0 reads W^0 = 1 from the table: no branch
-#pragma unroll
-    for (int r = 1; r < R; ++r) {
-      cpx<T> w = tw(toff + r * Ns + kq[kk]);
-      w.y *= sgn;
-      v[kk][r] = cmul(v[kk][r], w);
-    }
-  }
-  FFB_HD void finish(int kk) {
-    dft_dir<R, T>(v[kk], inv);
-    const int base = (jq[kk] - kq[kk]) * R + kq[kk];
-#pragma unroll
-    for (int q = 0; q < R; ++q) dst(base + q * Ns, v[kk][q]);
-  }
-};
-
-template <int R, typename T, class Src, class Dst, class Tw>
-FFB_HD void stockham_stage_r(const Core &c, int s, int tid, int nthr, const Tw &tw, bool inv, Src &src, Dst &dst) {
-  constexpr int K = Group<R>::K;
+template <int R, bool INV, typename T, class Src, class Dst>
+FFB_HD void stockham_stage_r(const Core &c, int s, int tid, int nthr, const cpx<T> *__restrict__ tw,
+                             const Src &src, const Dst &dst) {
   const int Ns = c.span[s], nb = c.L / R;
-  // row r of the stage's twiddle block starts at twoff - Ns + r * Ns
-  StockhamBody<R, K, T, Src, Dst, Tw> body{tw, src, dst, Ns, c.twoff[s] - Ns, nb, c.sdiv[s],
-                                           inv ? (T)-1 : (T)1, inv};
-  grouped_butterflies<K>(tid, nthr, nb, body);
+  const cpx<T> *blk = tw + c.twoff[s];
+  const FastDiv sd = c.sdiv[s];
+  for (int j = tid; j < nb; j += nthr) {
+    const int g = (int)fdiv((uint32_t)j, sd);
+    const int k = j - g * Ns;
+    cpx<T> v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r] = src(j + r * nb);
+    if (Ns > 1) {
+      cpx<T> w[R - 1];
+      load_tw_col<R, T>(blk, Ns, k, w);
+#pragma unroll
+      for (int r = 1; r < R; ++r) v[r] = cmul(v[r], w[r - 1]);
+    }
+    dft_fixed<R, INV, T>(v);
+    const int base = g * Ns * R + k;
+#pragma unroll
+    for (int q = 0; q < R; ++q) dst(base + q * Ns, v[q]);
+  }
 }
 
 // Shared-memory reader / writer of a ping-pong buffer.
@@ -562,43 +508,6 @@ struct PPWrite {
   cpx<T> *b;
   FFB_HD void operator()(int p, cpx<T> v) const { b[pp_pos(p)] = v; }
 };
-
-// Runs all stages of `c`: stage 0 reads `src`, the last stage writes `dst`,
-// the others go through b0 / b1 (stage s < last writes b0 for even s, b1 for
-// odd s).  A barrier follows every stage except the last.  The last stage
-// reads the buffer of parity (nst - 2), so the one of parity (nst - 1) is free
-// for the sink to write into.
-template <typename T, class Src, class Dst, class Sync>
-FFB_HD void run_stockham(const Core &c, cpx<T> *b0, cpx<T> *b1, int tid, int nthr, const cpx<T> *__restrict__ tw,
-                         bool inv, Src &src, Dst &dst, Sync sync) {
-  const TwGlobal<T> twl{tw};
-  const int S = c.nst;
-  for (int s = 0; s < S; ++s) {
-    const bool first = s == 0, last = s == S - 1;
-    if (first && last) {
-#define FFB_SS(R) stockham_stage_r<R, T>(c, s, tid, nthr, twl, inv, src, dst)
-      FFB_RADIX_SWITCH(c.radix[s], FFB_SS)
-#undef FFB_SS
-    } else if (first) {
-      PPWrite<T> w{b0};
-#define FFB_SS(R) stockham_stage_r<R, T>(c, s, tid, nthr, twl, inv, src, w)
-      FFB_RADIX_SWITCH(c.radix[s], FFB_SS)
-#undef FFB_SS
-    } else if (last) {
-      PPRead<T> rd{((s - 1) & 1) ? b1 : b0};
-#define FFB_SS(R) stockham_stage_r<R, T>(c, s, tid, nthr, twl, inv, rd, dst)
-      FFB_RADIX_SWITCH(c.radix[s], FFB_SS)
-#undef FFB_SS
-    } else {
-      PPRead<T> rd{((s - 1) & 1) ? b1 : b0};
-      PPWrite<T> w{(s & 1) ? b1 : b0};
-#define FFB_SS(R) stockham_stage_r<R, T>(c, s, tid, nthr, twl, inv, rd, w)
-      FFB_RADIX_SWITCH(c.radix[s], FFB_SS)
-#undef FFB_SS
-    }
-    if (!last) sync();
-  }
-}
 
 // Flat loop over e = t0, t0 + nt, ... < total, U iterations at a time: the U
 // values are all produced (their global loads issued back to back) before
@@ -620,16 +529,16 @@ FFB_HD void chunked_loop(int t0, int nt, int total, Produce &&produce, Consume &
   for (; base < total; base += nt) consume(base, produce(base));
 }
 
-// All stages of `c` shared -> shared: stage s reads buffer (s even ? src : oth)
-// and writes the other; every stage ends with a barrier.  The result is in
-// `src` when nst is even, in `oth` when odd.
-template <typename T, class Tw, class Sync>
-FFB_HD void run_stockham_smem(const Core &c, cpx<T> *src, cpx<T> *oth, int tid, int nthr, const Tw &tw, bool inv,
-                              Sync sync) {
+// All stages of `c` shared -> shared in direction INV: stage s reads buffer
+// (s even ? src : oth) and writes the other; every stage ends with a barrier.
+// The result is in `src` when nst is even, in `oth` when odd.
+template <typename T, bool INV, class Sync>
+FFB_HD void run_stockham_smem(const Core &c, cpx<T> *src, cpx<T> *oth, int tid, int nthr,
+                              const cpx<T> *__restrict__ tw, Sync sync) {
   for (int s = 0; s < c.nst; ++s) {
-    PPRead<T> rd{(s & 1) ? oth : src};
-    PPWrite<T> w{(s & 1) ? src : oth};
-#define FFB_SS(R) stockham_stage_r<R, T>(c, s, tid, nthr, tw, inv, rd, w)
+    const PPRead<T> rd{(s & 1) ? oth : src};
+    const PPWrite<T> w{(s & 1) ? src : oth};
+#define FFB_SS(R) stockham_stage_r<R, INV, T>(c, s, tid, nthr, tw, rd, w)
     FFB_RADIX_SWITCH(c.radix[s], FFB_SS)
 #undef FFB_SS
     sync();

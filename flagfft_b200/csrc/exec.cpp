@@ -232,12 +232,10 @@ static Core make_dit_core(int64_t L, const std::vector<int> &r) {
   Core c{};
   c.L = (int)L;
   c.nst = (int)r.size();
-  int64_t span = 1, off = 0;
+  int64_t span = 1;
   for (size_t s = 0; s < r.size(); ++s) {
     c.radix[s] = r[s];
     c.span[s] = (int)span;
-    c.twoff[s] = (int)off;
-    off += (r[s] - 1) * span;
     c.sdiv[s] = make_fastdiv((uint32_t)span);
     c.rdiv[s] = make_fastdiv((uint32_t)r[s]);
     span *= r[s];
@@ -251,12 +249,10 @@ static Core make_dif_core(int64_t L, const std::vector<int> &r) {
   Core c{};
   c.L = (int)L;
   c.nst = (int)r.size();
-  int64_t span = L, off = 0;
+  int64_t span = L;
   for (size_t s = 0; s < r.size(); ++s) {
     c.radix[s] = r[s];
     c.span[s] = (int)span;
-    c.twoff[s] = (int)off;
-    off += (r[s] - 1) * (span / r[s]);
     c.sdiv[s] = make_fastdiv((uint32_t)(span / r[s]));
     c.rdiv[s] = make_fastdiv((uint32_t)r[s]);
     span /= r[s];
@@ -369,8 +365,13 @@ class Builder {
       prog_.passes.push_back(std::move(p));
       return raw;
     }
-    a.tw = table_stage_twiddles(a.core, a.pp == 0 && spec.kind != CoreKind::Dit);
-    if (spec.kind != CoreKind::Dit) a.tw2 = table_stage_twiddles(a.core2, false);
+    if (spec.kind == CoreKind::Dit) {
+      a.tw = table_stage_twiddles(a.core, false, inverse);
+    } else {
+      // convolution: forward core (DIF in place, DIT for Stockham), inverse core2
+      a.tw = table_stage_twiddles(a.core, a.pp == 0, false);
+      a.tw2 = table_stage_twiddles(a.core2, false, true);
+    }
     // thread and tile shape: column tiles (transform index fastest in memory)
     // take consecutive transforms on consecutive threads
     const bool strided = ii > ig;
@@ -409,25 +410,29 @@ class Builder {
     return raw;
   }
 
-  // Per-stage twiddle blocks of a core (forward sign): stage s's block at
-  // core.twoff[s], entry [r - 1][j] = W_{span R}^{r j} (DIT / Stockham, j <
-  // span) or W_{span}^{r j} (DIF, j < span / R).  A length-L core's blocks
-  // hold L - 1 entries in all.  Cached per radix sequence.
-  const cpx<T> *table_stage_twiddles(const Core &c, bool dif) {
-    std::vector<int64_t> key = {c.L, dif ? 1 : 0};
+  // Per-stage twiddle blocks of a core for one direction; sets c.twoff.
+  // Stage s's block holds R - 1 rows of `inner` entries (inner = span for
+  // DIT / Stockham stages, span / R for DIF): entry j of row r - 1 is
+  // W_{inner R}^{r j} (forward sign, the conjugate for the inverse).  A
+  // length-L core's blocks hold L - 1 entries in all.  Cached per radix
+  // sequence, stage kind and direction.
+  const cpx<T> *table_stage_twiddles(Core &c, bool dif, bool inverse) {
+    int64_t total = 0;
+    for (int s = 0; s < c.nst; ++s) {
+      c.twoff[s] = (int)total;
+      total += (int64_t)(c.radix[s] - 1) * (dif ? c.span[s] / c.radix[s] : c.span[s]);
+    }
+    std::vector<int64_t> key = {c.L, dif ? 1 : 0, inverse ? 1 : 0};
     for (int s = 0; s < c.nst; ++s) key.push_back(c.radix[s]);
     for (auto &e : tw_cache_)
       if (e.first == key) return reinterpret_cast<const cpx<T> *>(e.second->ptr);
-    int64_t total = 0;
-    for (int s = 0; s < c.nst; ++s) total += (int64_t)(c.radix[s] - 1) * (dif ? c.span[s] / c.radix[s] : c.span[s]);
     std::vector<cpx<T>> h((size_t)std::max<int64_t>(total, 1), mk((T)1, (T)0));
     for (int s = 0; s < c.nst; ++s) {
       const int64_t R = c.radix[s];
       const int64_t inner = dif ? c.span[s] / R : c.span[s];
-      const int64_t den = dif ? c.span[s] : c.span[s] * R;
       for (int64_t r = 1; r < R; ++r)
         for (int64_t j = 0; j < inner; ++j) {
-          cld w = unit_root(r * j, den, -1);
+          cld w = unit_root(r * j, inner * R, inverse ? 1 : -1);
           h[(size_t)(c.twoff[s] + (r - 1) * inner + j)] = mk((T)w.real(), (T)w.imag());
         }
     }

@@ -4,7 +4,8 @@
 
 namespace ffb {
 namespace tile {
-template cudaError_t launch_pp<float, 0>(const TileArgs<float> &, size_t, cudaStream_t);
-template cudaError_t launch_pp<float, 1>(const TileArgs<float> &, size_t, cudaStream_t);
+template cudaError_t launch_pp<float, 0, false>(const TileArgs<float> &, size_t, cudaStream_t);
+template cudaError_t launch_pp<float, 0, true>(const TileArgs<float> &, size_t, cudaStream_t);
+template cudaError_t launch_pp<float, 1, false>(const TileArgs<float> &, size_t, cudaStream_t);
 }  // namespace tile
 }  // namespace ffb

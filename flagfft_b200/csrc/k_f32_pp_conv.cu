@@ -4,7 +4,7 @@
 
 namespace ffb {
 namespace tile {
-template cudaError_t launch_pp<float, 2>(const TileArgs<float> &, size_t, cudaStream_t);
-template cudaError_t launch_pp<float, 3>(const TileArgs<float> &, size_t, cudaStream_t);
+template cudaError_t launch_pp<float, 2, false>(const TileArgs<float> &, size_t, cudaStream_t);
+template cudaError_t launch_pp<float, 3, false>(const TileArgs<float> &, size_t, cudaStream_t);
 }  // namespace tile
 }  // namespace ffb

@@ -4,7 +4,8 @@
 
 namespace ffb {
 namespace tile {
-template cudaError_t launch_pp<double, 0>(const TileArgs<double> &, size_t, cudaStream_t);
-template cudaError_t launch_pp<double, 1>(const TileArgs<double> &, size_t, cudaStream_t);
+template cudaError_t launch_pp<double, 0, false>(const TileArgs<double> &, size_t, cudaStream_t);
+template cudaError_t launch_pp<double, 0, true>(const TileArgs<double> &, size_t, cudaStream_t);
+template cudaError_t launch_pp<double, 1, false>(const TileArgs<double> &, size_t, cudaStream_t);
 }  // namespace tile
 }  // namespace ffb

@@ -4,7 +4,7 @@
 
 namespace ffb {
 namespace tile {
-template cudaError_t launch_pp<double, 2>(const TileArgs<double> &, size_t, cudaStream_t);
-template cudaError_t launch_pp<double, 3>(const TileArgs<double> &, size_t, cudaStream_t);
+template cudaError_t launch_pp<double, 2, false>(const TileArgs<double> &, size_t, cudaStream_t);
+template cudaError_t launch_pp<double, 3, false>(const TileArgs<double> &, size_t, cudaStream_t);
 }  // namespace tile
 }  // namespace ffb

@@ -12,7 +12,7 @@ namespace tile {
 // defined in k_*.cu
 template <typename T, int K>
 cudaError_t launch_group(const TileArgs<T> &a, int io, size_t smem, cudaStream_t s);
-template <typename T, int K>
+template <typename T, int K, bool INV>
 cudaError_t launch_pp(const TileArgs<T> &a, size_t smem, cudaStream_t s);
 template <typename T, int KIND, int IO>
 cudaError_t launch_one(const TileArgs<T> &a, size_t smem, cudaStream_t s);
@@ -114,10 +114,10 @@ cudaError_t launch_tile(const TileArgs<T> &a, CoreKind kind, IoKind io, size_t s
   if (a.regcol) return launch_regcol<T>(a, s);
   if (a.pp && o == 0) {
     switch (k) {
-      case 0: return tile::launch_pp<T, 0>(a, smem, s);
-      case 1: return tile::launch_pp<T, 1>(a, smem, s);
-      case 2: return tile::launch_pp<T, 2>(a, smem, s);
-      case 3: return tile::launch_pp<T, 3>(a, smem, s);
+      case 0: return a.inv ? tile::launch_pp<T, 0, true>(a, smem, s) : tile::launch_pp<T, 0, false>(a, smem, s);
+      case 1: return tile::launch_pp<T, 1, false>(a, smem, s);
+      case 2: return tile::launch_pp<T, 2, false>(a, smem, s);
+      case 3: return tile::launch_pp<T, 3, false>(a, smem, s);
       default: return cudaErrorInvalidValue;
     }
   }

@@ -20,8 +20,9 @@ namespace {
 
 // Workspace: up to 2^22 complex64 elements (32 MiB) of batch * n.
 constexpr long long kNoAllocMaxElems = 1ll << 22;
-// Per-stage twiddle blocks of the radix-16 cores of every power of two 2..4096
-// (the block set of length 2^l at offset 2^l - l - 1; 8178 entries in all).
+// Per-stage twiddle blocks of the radix-16 cores of every power of two
+// 2..4096, one table per direction (the length-2^l core's blocks, 2^l - 1
+// entries, at offset 2^l - l - 1; 8178 entries in all).
 constexpr int kRootLen = 4096;
 constexpr int kStageTableLen = 8192;
 // Four-step twiddle W_n^m = hi[m >> 12] * lo[m & 4095] for n <= 2^24.
@@ -29,7 +30,7 @@ constexpr int kSplitBits = 12;
 constexpr int kSplit = 1 << kSplitBits;
 
 static __device__ __align__(256) cpx<float> g_scratch[kNoAllocMaxElems];
-static __device__ __align__(256) cpx<float> g_roots[kStageTableLen];
+static __device__ __align__(256) cpx<float> g_roots[2 * kStageTableLen];  // forward, inverse
 static __device__ __align__(256) cpx<float> g_ptw_lo[kSplit];
 static __device__ __align__(256) cpx<float> g_ptw_hi[kSplit];
 
@@ -51,13 +52,13 @@ __global__ void k_fill_roots(cpx<float> *dst, int count, long long n, long long 
   }
 }
 
-// Offset of the length-2^l core's stage blocks in g_roots.
+// Offset of the length-2^l core's stage blocks in one direction's table.
 __host__ __device__ inline int stage_table_offset(int l) { return (1 << l) - l - 1; }
 
-// Fills the per-stage twiddle blocks of pow2_core(2^l), l = 1..12: entry
-// [r - 1][k] of stage s is W_{span R}^{r k} (span = 16^s, R = 16 or the
-// smaller last radix), k < span.
-__global__ void k_fill_stage_tables(cpx<float> *dst) {
+// Fills one direction's stage blocks of pow2_core(2^l), l = 1..12: entry k of
+// row r - 1 of stage s is W_{span R}^{r k} (conjugated when inverse), span =
+// 16^s, R = 16 or the smaller last radix.
+__global__ void k_fill_stage_tables(cpx<float> *dst, int inverse) {
   for (int l = 1; l <= 12; ++l) {
     const int L = 1 << l;
     cpx<float> *t = dst + stage_table_offset(l);
@@ -65,15 +66,14 @@ __global__ void k_fill_stage_tables(cpx<float> *dst) {
       int span = 1, rem = L, off = 0;
       while (rem > 1) {
         const int R = rem >= 16 ? 16 : rem;
-        const int size = (R - 1) * span;
-        if (e < off + size) {
+        if (e < off + (R - 1) * span) {
           const int r = 1 + (e - off) / span, k = (e - off) % span;
           double sn, cs;
-          sincospi(-2.0 * (double)(r * k) / (double)(span * R), &sn, &cs);
+          sincospi((inverse ? 2.0 : -2.0) * (double)(r * k) / (double)(span * R), &sn, &cs);
           t[e] = mk((float)cs, (float)sn);
           break;
         }
-        off += size;
+        off += (R - 1) * span;
         span *= R;
         rem /= R;
       }
@@ -95,7 +95,9 @@ cudaError_t device_state(DeviceState **out) {
     if ((e = cudaGetSymbolAddress(reinterpret_cast<void **>(&st.roots), g_roots)) != cudaSuccess) return e;
     if ((e = cudaGetSymbolAddress(reinterpret_cast<void **>(&st.lo), g_ptw_lo)) != cudaSuccess) return e;
     if ((e = cudaGetSymbolAddress(reinterpret_cast<void **>(&st.hi), g_ptw_hi)) != cudaSuccess) return e;
-    k_fill_stage_tables<<<16, 256>>>(st.roots);
+    k_fill_stage_tables<<<16, 256>>>(st.roots, 0);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    k_fill_stage_tables<<<16, 256>>>(st.roots + kStageTableLen, 1);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if ((e = cudaDeviceSynchronize()) != cudaSuccess) return e;
     st.ready = true;
@@ -141,7 +143,7 @@ TileArgs<float> pass_args(int L, int G, long long nbatch, long long ib, long lon
   a.core = pow2_core(L);
   int l = 0;
   while ((1 << l) < L) ++l;
-  a.tw = roots + stage_table_offset(l);
+  a.tw = roots + (inverse ? kStageTableLen : 0) + stage_table_offset(l);
   a.pp = 1;
   a.wfast = ii > ig ? 1 : 0;
   const int rmax = L >= 16 ? 16 : L;

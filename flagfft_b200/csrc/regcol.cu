@@ -13,7 +13,7 @@
 namespace ffb {
 namespace {
 
-template <typename T, int R>
+template <typename T, int R, bool INV>
 FFB_HD void regcol_transform(const TileArgs<T> &a, long long by, long long g) {
   const cpx<T> *in = reinterpret_cast<const cpx<T> *>(a.in) + by * a.ib + g * a.ig;
   cpx<T> *out = reinterpret_cast<cpx<T> *>(a.out) + by * a.ob + g * a.og;
@@ -28,7 +28,7 @@ FFB_HD void regcol_transform(const TileArgs<T> &a, long long by, long long g) {
 #pragma unroll
     for (int i = 0; i < R; ++i) v[i] = ldg_c(in + i * a.ii);
   }
-  dft_dir<R, T>(v, a.inv != 0);
+  dft_fixed<R, INV, T>(v);
   if (a.chirp_mode == 2) {
 #pragma unroll
     for (int k = 0; k < R; ++k) {
@@ -42,7 +42,7 @@ FFB_HD void regcol_transform(const TileArgs<T> &a, long long by, long long g) {
       const uint32_t m = (uint32_t)(g * k);
       const uint32_t hi = fdiv(m, a.ptw_div);
       cpx<T> t = cmul(ldg_c(a.ptw_hi + hi), ldg_c(a.ptw_lo + (m - hi * a.ptw_div.d)));
-      if (a.inv) t.y = -t.y;
+      if constexpr (INV) t.y = -t.y;
       out[k * a.ok] = cmul(v[k], t);
     }
   } else {
@@ -53,24 +53,29 @@ FFB_HD void regcol_transform(const TileArgs<T> &a, long long by, long long g) {
 
 constexpr int kRegcolThreads = 128;
 
-template <typename T, int R>
+template <typename T, int R, bool INV>
 __global__ void __launch_bounds__(kRegcolThreads) k_regcol(const __grid_constant__ TileArgs<T> a) {
   const long long g = (long long)blockIdx.x * kRegcolThreads + threadIdx.x;
-  if (g < a.G) regcol_transform<T, R>(a, (long long)blockIdx.y, g);
+  if (g < a.G) regcol_transform<T, R, INV>(a, (long long)blockIdx.y, g);
 }
 
-template <typename T, int R>
-cudaError_t launch_r(const TileArgs<T> &a, cudaStream_t s) {
+template <typename T, int R, bool INV>
+cudaError_t launch_dir(const TileArgs<T> &a, cudaStream_t s) {
 #ifndef FFB_HOST_EMULATION
   dim3 grid((unsigned)((a.G + kRegcolThreads - 1) / kRegcolThreads), (unsigned)a.nbatch, 1);
-  k_regcol<T, R><<<grid, kRegcolThreads, 0, s>>>(a);
+  k_regcol<T, R, INV><<<grid, kRegcolThreads, 0, s>>>(a);
   return cudaGetLastError();
 #else
   (void)s;
   for (long long by = 0; by < a.nbatch; ++by)
-    for (long long g = 0; g < a.G; ++g) regcol_transform<T, R>(a, by, g);
+    for (long long g = 0; g < a.G; ++g) regcol_transform<T, R, INV>(a, by, g);
   return cudaSuccess;
 #endif
+}
+
+template <typename T, int R>
+cudaError_t launch_r(const TileArgs<T> &a, cudaStream_t s) {
+  return a.inv ? launch_dir<T, R, true>(a, s) : launch_dir<T, R, false>(a, s);
 }
 
 }  // namespace

@@ -126,7 +126,7 @@ FFB_HD void tile_body(const TileArgs<T> &a, long long bx, long long by, cpx<T> *
   const int t0 = x.tid(), nt = x.nthreads();
 
   // Logical input element i of the core's transform g.
-  auto core_input = [&](long long g, int i) -> cpx<T> {
+  auto core_input = [&](long long g, int i) FFB_INL -> cpx<T> {
     const long long base = g * a.ig;
     if constexpr (IO == 0 || IO == 6) {
       return ld_cpx<T>(in, base + (long long)i * a.ii);
@@ -162,7 +162,7 @@ FFB_HD void tile_body(const TileArgs<T> &a, long long bx, long long by, cpx<T> *
   {
     const int total = W * L;
     const int nl = (IO == 1 || IO == 2) ? half_n : n;  // Bluestein logical length
-    auto produce = [&](int e) -> cpx<T> {
+    auto produce = [&](int e) FFB_INL -> cpx<T> {
       int w, i;
       split_elem(e, W, L, a.wfast, a.wdiv, a.ldiv, w, i);
       const long long g = g0 + w;
@@ -183,7 +183,7 @@ FFB_HD void tile_body(const TileArgs<T> &a, long long bx, long long by, cpx<T> *
       }
       return v;
     };
-    auto consume = [&](int e, cpx<T> v) {
+    auto consume = [&](int e, cpx<T> v) FFB_INL {
       int w, i;
       split_elem(e, W, L, a.wfast, a.wdiv, a.ldiv, w, i);
       if constexpr (KIND == 0) {
@@ -203,8 +203,8 @@ FFB_HD void tile_body(const TileArgs<T> &a, long long bx, long long by, cpx<T> *
   x.sync();
 
   // ---------------------------------------------------------------- core
-  auto sync = [&]() { x.sync(); };
-  x.per_slot(W, [&](int slot, int tid, int tpt) {
+  auto sync = [&]() FFB_INL { x.sync(); };
+  x.per_slot(W, [&](int slot, int tid, int tpt) FFB_INL {
     cpx<T> *buf = sm + slot * Lp;
     if constexpr (KIND == 0) {
       run_dit<T>(buf, a.core, tid, tpt, a.tw, a.inv != 0, sync);
@@ -226,7 +226,7 @@ FFB_HD void tile_body(const TileArgs<T> &a, long long bx, long long by, cpx<T> *
 
   // Four-step column passes multiply output k of transform g by W_N^{g k}
   // (forward sign; conjugated for the inverse), g*k < N < 2^31.
-  auto post_twiddle = [&](cpx<T> v, long long g, int k) -> cpx<T> {
+  auto post_twiddle = [&](cpx<T> v, long long g, int k) FFB_INL -> cpx<T> {
     if (!a.post_twiddle) return v;
     const uint32_t m = (uint32_t)(g * (long long)k);
     const uint32_t hi = fdiv(m, a.ptw_div);
@@ -237,7 +237,7 @@ FFB_HD void tile_body(const TileArgs<T> &a, long long bx, long long by, cpx<T> *
   };
 
   // Natural-order output element k of the core's transform in slot w.
-  auto out_elem = [&](int w, int k) -> cpx<T> {
+  auto out_elem = [&](int w, int k) FFB_INL -> cpx<T> {
     const cpx<T> *bw = sm + w * Lp;
     if constexpr (KIND == 0 || KIND == 3) {
       return bw[Swz<T>::phys(k)];
@@ -272,7 +272,7 @@ FFB_HD void tile_body(const TileArgs<T> &a, long long bx, long long by, cpx<T> *
     } else {
       const int nout = KIND == 1 ? n : L;
       const int total = W * nout;
-      auto produce = [&](int e) -> cpx<T> {
+      auto produce = [&](int e) FFB_INL -> cpx<T> {
         int w, k;
         split_elem(e, W, nout, a.wfast, a.wdiv, KIND == 1 ? a.ndiv : a.ldiv, w, k);
         const long long g = g0 + w;
@@ -286,7 +286,7 @@ FFB_HD void tile_body(const TileArgs<T> &a, long long bx, long long by, cpx<T> *
         }
         return post_twiddle(v, gc, k);
       };
-      auto consume = [&](int e, cpx<T> v) {
+      auto consume = [&](int e, cpx<T> v) FFB_INL {
         int w, k;
         split_elem(e, W, nout, a.wfast, a.wdiv, KIND == 1 ? a.ndiv : a.ldiv, w, k);
         const long long g = g0 + w;
@@ -379,7 +379,9 @@ FFB_HD int pp_slot_len(int L) {
   return 2 * pp_size(L) + 3;
 }
 
-template <typename T, int KIND, class X>
+// INV: direction of a Dit core (KIND 0); convolutions (KIND 1-3) run their
+// forward core and inverse core2 whatever INV is.
+template <typename T, int KIND, bool INV, class X>
 FFB_HD void tile_body_pp(const TileArgs<T> &a, long long bx, long long by, cpx<T> *sm, const X &x) {
   const int L = a.core.L;
   const int Lq = pp_size(L);
@@ -399,7 +401,7 @@ FFB_HD void tile_body_pp(const TileArgs<T> &a, long long bx, long long by, cpx<T
   {
     const int total = W * L;
     // produce: the element's value and its shared-memory position
-    auto produce = [&](int e) -> ElemAt<T> {
+    auto produce = [&](int e) FFB_INL -> ElemAt<T> {
       int w, i;
       split_elem(e, W, L, a.wfast, a.wdiv, a.ldiv, w, i);
       const int wc = w < wlive ? w : wlive - 1;
@@ -419,7 +421,7 @@ FFB_HD void tile_body_pp(const TileArgs<T> &a, long long bx, long long by, cpx<T
         return {ldg_c(xin + i * ii), at};
       }
     };
-    auto consume = [&](int, ElemAt<T> p) { sm[p.at] = p.v; };
+    auto consume = [&](int, ElemAt<T> p) FFB_INL { sm[p.at] = p.v; };
     chunked_loop<U, ElemAt<T>>(t0, nt, total, produce, consume);
     if constexpr (KIND == 2) {
       for (int w = t0; w < W; w += nt) {
@@ -431,13 +433,12 @@ FFB_HD void tile_body_pp(const TileArgs<T> &a, long long bx, long long by, cpx<T
   x.sync();
 
   // ---- stages
-  auto sync = [&]() { x.sync(); };
+  auto sync = [&]() FFB_INL { x.sync(); };
   {
-    const TwGlobal<T> tw{a.tw}, tw2{a.tw2};
-    x.per_slot(W, [&](int slot, int tid, int tpt) {
+    x.per_slot(W, [&](int slot, int tid, int tpt) FFB_INL {
       cpx<T> *const b0 = sm + slot * slot_len, *const b1 = b0 + Lq;
       const int S = a.core.nst;
-      run_stockham_smem<T>(a.core, b0, b1, tid, tpt, tw, KIND == 0 ? a.inv != 0 : false, sync);
+      run_stockham_smem<T, KIND == 0 && INV>(a.core, b0, b1, tid, tpt, a.tw, sync);
       if constexpr (KIND != 0) {
         // kernel product on the forward result (natural order), then the inverse
         const int wc = slot < wlive ? slot : wlive - 1;
@@ -452,7 +453,7 @@ FFB_HD void tile_body_pp(const TileArgs<T> &a, long long bx, long long by, cpx<T
           r[pp_pos(p)] = cmul(v, ldg_c(kern + p));
         }
         sync();
-        run_stockham_smem<T>(a.core2, r, (S & 1) ? b0 : b1, tid, tpt, tw2, true, sync);
+        run_stockham_smem<T, true>(a.core2, r, (S & 1) ? b0 : b1, tid, tpt, a.tw2, sync);
       }
     });
   }
@@ -460,7 +461,7 @@ FFB_HD void tile_body_pp(const TileArgs<T> &a, long long bx, long long by, cpx<T
   // ---- store
   const int S_total = a.core.nst + (KIND == 0 ? 0 : a.core2.nst);
   const int res_off = (S_total & 1) ? Lq : 0;
-  auto post_twiddle = [&](cpx<T> v, long long g, int k) -> cpx<T> {
+  auto post_twiddle = [&](cpx<T> v, long long g, int k) FFB_INL -> cpx<T> {
     if (!a.post_twiddle) return v;
     const uint32_t m = (uint32_t)(g * (long long)k);
     const uint32_t hi = fdiv(m, a.ptw_div);
@@ -474,7 +475,7 @@ FFB_HD void tile_body_pp(const TileArgs<T> &a, long long bx, long long by, cpx<T
   // produce: the output value and its offset from `out`, or -1 when the
   // element is not written (a dead transform of the last tile, or a
   // chirp-on-store position past n)
-  auto produce = [&](int e) -> ElemAt<T> {
+  auto produce = [&](int e) FFB_INL -> ElemAt<T> {
     int w, k;
     split_elem(e, W, nout, a.wfast, a.wdiv, KIND == 1 ? a.ndiv : a.ldiv, w, k);
     const int wc = w < wlive ? w : wlive - 1;
@@ -495,7 +496,7 @@ FFB_HD void tile_body_pp(const TileArgs<T> &a, long long bx, long long by, cpx<T
       return {post_twiddle(v, g0 + wc, k), at};
     }
   };
-  auto consume = [&](int, ElemAt<T> p) {
+  auto consume = [&](int, ElemAt<T> p) FFB_INL {
     if (p.at >= 0) out[p.at] = p.v;
   };
   chunked_loop<U, ElemAt<T>>(t0, nt, total, produce, consume);
@@ -517,11 +518,11 @@ __global__ void __launch_bounds__(TileBounds<T>::kMaxThreads) k_tile(const __gri
   tile_body<T, KIND, IO>(a, (long long)blockIdx.x, (long long)blockIdx.y, reinterpret_cast<cpx<T> *>(smraw), x);
 }
 
-template <typename T, int KIND>
+template <typename T, int KIND, bool INV>
 __global__ void __launch_bounds__(TileBounds<T>::kMaxThreads) k_tile_pp(const __grid_constant__ TileArgs<T> a) {
   extern __shared__ __align__(16) unsigned char smraw[];
   DevX x{a.tpt, a.wfast};
-  tile_body_pp<T, KIND>(a, (long long)blockIdx.x, (long long)blockIdx.y, reinterpret_cast<cpx<T> *>(smraw), x);
+  tile_body_pp<T, KIND, INV>(a, (long long)blockIdx.x, (long long)blockIdx.y, reinterpret_cast<cpx<T> *>(smraw), x);
 }
 
 #ifndef FFB_HOST_EMULATION
@@ -538,21 +539,22 @@ cudaError_t launch_one(const TileArgs<T> &a, size_t smem, cudaStream_t s) {
   k_tile<T, KIND, IO><<<grid, block, smem, s>>>(a);
   return cudaGetLastError();
 }
-template <typename T, int KIND>
+template <typename T, int KIND, bool INV>
 cudaError_t launch_pp(const TileArgs<T> &a, size_t smem, cudaStream_t s) {
   static bool configured = false;
   if (!configured) {
-    cudaError_t e = cudaFuncSetAttribute(k_tile_pp<T, KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize, 232448);
+    cudaError_t e =
+        cudaFuncSetAttribute(k_tile_pp<T, KIND, INV>, cudaFuncAttributeMaxDynamicSharedMemorySize, 232448);
     if (e != cudaSuccess) return e;
     configured = true;
   }
   dim3 grid((unsigned)((a.G + a.W - 1) / a.W), (unsigned)a.nbatch, 1);
   dim3 block((unsigned)(a.W * a.tpt), 1, 1);
-  k_tile_pp<T, KIND><<<grid, block, smem, s>>>(a);
+  k_tile_pp<T, KIND, INV><<<grid, block, smem, s>>>(a);
   return cudaGetLastError();
 }
 #else
-template <typename T, int KIND>
+template <typename T, int KIND, bool INV>
 cudaError_t launch_pp(const TileArgs<T> &a, size_t smem, cudaStream_t) {
   std::vector<unsigned char> buf(smem + 64);
   cpx<T> *sm = reinterpret_cast<cpx<T> *>(buf.data());
@@ -561,7 +563,7 @@ cudaError_t launch_pp(const TileArgs<T> &a, size_t smem, cudaStream_t) {
   for (long long by = 0; by < a.nbatch; ++by)
     for (long long bx = 0; bx < tiles; ++bx) {
       std::memset(buf.data(), 0xff, buf.size());
-      tile_body_pp<T, KIND>(a, bx, by, sm, x);
+      tile_body_pp<T, KIND, INV>(a, bx, by, sm, x);
     }
   return cudaSuccess;
 }
