@@ -1,24 +1,29 @@
 #!/usr/bin/env python
 """Benchmark of the flagfft.h Exec hot path on B200.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload NAME]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload NAME | --problem TYPE:N:BATCH[:MODE]]
 
-Default workload ("arbitrary_1d"): the arbitrary-length 1-D configuration --
-C2C (complex64) N = 1701, 1009, 10007 at batch 1024 and Z2Z (complex128) at the
-same lengths at batch 256, forward, out of place.  One step executes all six
-plans once.  Inputs are seeded iid uniform[-1, 1) re/im (synthetic; no
-dataset).  Each step touches ~312 MB (inputs + outputs), more than the 126 MB
-L2, so consecutive uses of a buffer come from HBM.
+Workloads (one step executes every call of the workload once):
+  arbitrary_1d (default): C2C (complex64) N = 1701, 1009, 10007 at batch 1024
+      and Z2Z (complex128) at the same lengths at batch 256, forward, out of
+      place.  ~312 MB of inputs + outputs per step, above the 126 MB L2, so a
+      buffer's next use comes from HBM.
+  plain_c2c_4096: C2C N = 4096 x 256, forward then inverse, out of place.
+  real_large: R2C -> C2R round trip N = 2^24 x 4 (float), D2Z N = 3*2^20 x 2,
+      2-D C2C 4096 x 4096 (complex64), forward.
+Inputs are seeded uniform[-1, 1) (synthetic; no dataset).
 
-Metric: GFLOP/s at 5 N log2 N per complex transform, whole job (all ranks).
-The JSON line also carries, per N, the device time, GFLOP/s and GB/s against
-the algorithmic bytes (passes x batch x (N_in e_in + N_out e_out), passes = 1
-when one transform fits on chip), the roofline of the dominant kernel, the
-end-to-end figure through the public API with host buffers, cuFFT (torch.fft)
-on the same problems as a comparator, and the CPU baseline.
+Metric: GFLOP/s at 5 N log2 N per complex transform (2-D: 5 n0 n1 log2(n0 n1);
+real transforms quoted at the same 5 N log2 N), whole job over all ranks.  The
+JSON line also carries, per call, the device time, GFLOP/s and GB/s of
+algorithmic bytes (P x batch x (N_in e_in + N_out e_out), P = 1 when one
+transform fits on chip, else 2); the roofline of the dominant kernel; the
+end-to-end figure through the public API with host buffers; cuFFT (torch.fft)
+on the same calls; and the CPU baseline (the oracle port on the host cores).
 
-Multi-GPU (torchrun): every rank runs the same per-GPU workload on its own
-GPU (independent transforms: no collective on the data path, weak scaling);
+Multi-GPU (torchrun): every rank runs the same per-GPU workload on its own GPU
+(independent transforms: no collective on the data path, weak scaling); the
 timing is the max over ranks.
 """
 from __future__ import annotations
@@ -36,38 +41,42 @@ from pathlib import Path
 
 ROOT = Path(__file__).resolve().parent
 
+# (type, N, batch, mode): mode "f" forward; "fi" forward then inverse back;
+# "rt" R2C then C2R back.  Type "C2C2D" is an N x N 2-D C2C.
 WORKLOADS = {
-    # (type, N, batch)
-    "arbitrary_1d": [("C2C", 1701, 1024), ("C2C", 1009, 1024), ("C2C", 10007, 1024),
-                     ("Z2Z", 1701, 256), ("Z2Z", 1009, 256), ("Z2Z", 10007, 256)],
-    "plain_c2c_4096": [("C2C", 4096, 256)],
-    "real_large": [("R2C", 1 << 24, 4), ("D2Z", 3 << 20, 2)],
+    "arbitrary_1d": [("C2C", 1701, 1024, "f"), ("C2C", 1009, 1024, "f"), ("C2C", 10007, 1024, "f"),
+                     ("Z2Z", 1701, 256, "f"), ("Z2Z", 1009, 256, "f"), ("Z2Z", 10007, 256, "f")],
+    "plain_c2c_4096": [("C2C", 4096, 256, "fi")],
+    "real_large": [("R2C", 1 << 24, 4, "rt"), ("D2Z", 3 << 20, 2, "f"), ("C2C2D", 4096, 1, "f")],
 }
 WORKLOAD_DESC = {
     "arbitrary_1d": "C2C N=1701,1009,10007 x1024 + Z2Z same N x256, forward, out-of-place",
-    "plain_c2c_4096": "C2C N=4096 x256, forward, out-of-place",
-    "real_large": "R2C N=2^24 x4 + D2Z N=3*2^20 x2, out-of-place",
+    "plain_c2c_4096": "C2C N=4096 x256, forward + inverse, out-of-place",
+    "real_large": "R2C->C2R N=2^24 x4, D2Z N=3*2^20 x2, 2-D C2C 4096x4096, out-of-place",
 }
+TYPES = ("C2C", "Z2Z", "R2C", "D2Z", "C2R", "Z2D", "C2C2D")
 
 
 def parse_args():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="arbitrary_1d")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="budget of the CPU baseline sample")
     ap.add_argument("--no-cufft", action="store_true")
-    ap.add_argument("--problem", default=None, metavar="TYPE:N:BATCH",
+    ap.add_argument("--problem", default=None, metavar="TYPE:N:BATCH[:MODE]",
                     help="run one problem instead of a named workload (profiling captures), e.g. C2C:10007:1024")
     args = ap.parse_args()
     if args.problem:
-        t, n, b = args.problem.split(":")
-        if t not in ("C2C", "Z2Z", "R2C", "D2Z", "C2R", "Z2D"):
-            ap.error(f"unknown transform type {t}")
-        WORKLOADS["problem"] = [(t, int(n), int(b))]
-        WORKLOAD_DESC["problem"] = f"{t} N={n} x{b}, forward, out-of-place"
+        parts = args.problem.split(":")
+        t, n, b = parts[0], int(parts[1]), int(parts[2])
+        mode = parts[3] if len(parts) > 3 else "f"
+        if t not in TYPES or mode not in ("f", "fi", "rt") or (mode == "rt" and t not in ("R2C", "D2Z")):
+            ap.error(f"bad problem {args.problem}")
+        WORKLOADS["problem"] = [(t, n, b, mode)]
+        WORKLOAD_DESC["problem"] = f"{t} N={n} x{b} mode {mode}, out-of-place"
         args.workload = "problem"
     return args
 
@@ -78,24 +87,55 @@ def parse_args():
 
 def elem_bytes(t: str) -> tuple[int, int]:
     """(input element bytes, output element bytes)."""
-    return {"C2C": (8, 8), "Z2Z": (16, 16), "R2C": (4, 8), "D2Z": (8, 16), "C2R": (8, 4), "Z2D": (16, 8)}[t]
+    return {"C2C": (8, 8), "C2C2D": (8, 8), "Z2Z": (16, 16), "R2C": (4, 8), "D2Z": (8, 16), "C2R": (8, 4),
+            "Z2D": (16, 8)}[t]
 
 
-def flops(t: str, n: int, batch: int) -> float:
-    """5 N log2 N per transform (real transforms quoted at the same 5 N log2 N)."""
+def flops_one(t: str, n: int, batch: int) -> float:
+    """5 N log2 N per transform (real transforms quoted at the same figure;
+    2-D N x N: 5 N^2 log2 N^2)."""
+    if t == "C2C2D":
+        return 5.0 * n * n * math.log2(n * n) * batch
     return 5.0 * n * math.log2(n) * batch
+
+
+def calls_of(problem) -> list[tuple[str, int]]:
+    """(type, direction) of each Exec call one step of the problem makes."""
+    t, n, b, mode = problem
+    if mode == "f":
+        return [(t, -1)]
+    if mode == "fi":
+        return [(t, -1), (t, 1)]
+    return [(t, -1), ({"R2C": "C2R", "D2Z": "Z2D"}[t], 1)]
+
+
+def problem_flops(problem) -> float:
+    t, n, b, mode = problem
+    return flops_one(t, n, b) * len(calls_of(problem))
 
 
 def measured_peaks() -> dict:
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
         d = json.loads(p.read_text())
-        return {"hbm_gbs": float(d["hbm_gbs"]), "source": "measured (MEASURED_PEAKS.json)"}
+        return {"hbm_gbs": float(d["hbm_gbs"]), "source": "measured (MEASURED_PEAKS.json hbm_gbs)"}
     return {"hbm_gbs": 6650.0, "source": "fallback 6.65 TB/s"}
 
 
+def profiled_traffic() -> dict:
+    """DRAM bytes per launch from committed ncu captures, keyed by call."""
+    p = ROOT / "profiles" / "traffic.json"
+    if not p.exists():
+        return {}
+    try:
+        return json.loads(p.read_text())
+    except ValueError:
+        return {}
+
+
 class ClockSampler:
-    """nvidia-smi SM clock / throttle-reason samples while the timed region runs."""
+    """nvidia-smi SM clock / throttle-reason samples; only samples that arrive
+    inside the timed window are kept."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -104,29 +144,33 @@ class ClockSampler:
     def __init__(self, device_index: int):
         self.dev = device_index
         self.proc = None
-        self.lines: list[str] = []
+        self.lines: list[tuple[float, str]] = []
         self.thread = None
+        self.window = (0.0, 0.0)
 
     def start(self):
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", "50"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except (OSError, FileNotFoundError):
             self.proc = None
             return
 
         def reader():
             for line in self.proc.stdout:
-                self.lines.append(line.strip())
+                self.lines.append((time.time(), line.strip()))
 
         self.thread = threading.Thread(target=reader, daemon=True)
         self.thread.start()
+        time.sleep(0.3)  # first sample before the timed window opens
+
+    def mark(self, t0: float, t1: float):
+        self.window = (t0, t1)
 
     def stop(self) -> dict:
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        time.sleep(0.15)
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
@@ -134,9 +178,12 @@ class ClockSampler:
             self.proc.kill()
         if self.thread:
             self.thread.join(timeout=2)
+        t0, t1 = self.window
         sm, smax, reasons, power = [], [], set(), []
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        for ts, ln in self.lines:
+            if not (t0 <= ts <= t1 + 0.06):
+                continue
             parts = [p.strip() for p in ln.split(",")]
             if len(parts) < 9:
                 continue
@@ -150,7 +197,7 @@ class ClockSampler:
                 if flag.lower() == "active":
                     reasons.add(name)
         if not sm:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples inside the timed window"]}
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
                 "samples": len(sm), "power_w_max": max(power) if power else None}
 
@@ -159,60 +206,76 @@ class ClockSampler:
 # our arm
 # ---------------------------------------------------------------------------
 
+def build_calls(problems, dev, rank, torch, ffb):
+    """Plans and device buffers of every Exec call of one step."""
+    cdt = {"C2C": torch.complex64, "C2C2D": torch.complex64, "Z2Z": torch.complex128, "R2C": torch.float32,
+           "D2Z": torch.float64, "C2R": torch.complex64, "Z2D": torch.complex128}
+    odt = {"C2C": torch.complex64, "C2C2D": torch.complex64, "Z2Z": torch.complex128, "R2C": torch.complex64,
+           "D2Z": torch.complex128, "C2R": torch.float32, "Z2D": torch.float64}
+    tcode = {"C2C": ffb.C2C, "C2C2D": ffb.C2C, "Z2Z": ffb.Z2Z, "R2C": ffb.R2C, "D2Z": ffb.D2Z, "C2R": ffb.C2R,
+             "Z2D": ffb.Z2D}
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(0x46544646 + rank)
+
+    def rand(shape, dt):
+        if dt.is_complex:
+            real = torch.float32 if dt == torch.complex64 else torch.float64
+            return torch.view_as_complex((torch.rand((*shape, 2), generator=gen, device=dev, dtype=real) * 2 - 1)
+                                         .contiguous())
+        return torch.rand(shape, generator=gen, device=dev, dtype=dt) * 2 - 1
+
+    calls = []
+    for prob in problems:
+        t0, n, b, mode = prob
+        src = None
+        for i, (t, direction) in enumerate(calls_of(prob)):
+            in_n = n // 2 + 1 if t in ("C2R", "Z2D") else n
+            out_n = n // 2 + 1 if t in ("R2C", "D2Z") else n
+            shape_in = (n, n) if t == "C2C2D" else (b, in_n)
+            shape_out = (n, n) if t == "C2C2D" else (b, out_n)
+            x = rand(shape_in, cdt[t]) if src is None else src
+            y = torch.empty(shape_out, dtype=odt[t], device=dev)
+            plan = ffb.plan2d(n, n, tcode[t]) if t == "C2C2D" else ffb.plan1d(n, tcode[t], b)
+            launches = plan.launch_count(direction)
+            ib, ob = elem_bytes(t)
+            elems_in = n * n if t == "C2C2D" else b * in_n
+            elems_out = n * n if t == "C2C2D" else b * out_n
+            calls.append({"t": t, "n": n, "b": b, "dir": direction, "x": x, "y": y, "plan": plan,
+                          "key": f"{t}:{n}:{b}:{'fwd' if direction < 0 else 'inv'}",
+                          "first": i == 0, "launches": launches,
+                          "flop": flops_one(t, n, b),
+                          "alg_bytes": (1 if launches == 1 else 2) * (elems_in * ib + elems_out * ob)})
+            src = y
+    return calls
+
+
 def run_ours(args, rank: int, world: int, local_rank: int):
-    import numpy as np
     import torch
 
     import flagfft_b200 as ffb
 
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
-    problems = WORKLOADS[args.workload]
     stream = torch.cuda.Stream(device=dev)
-
-    cdt = {"C2C": torch.complex64, "Z2Z": torch.complex128, "R2C": torch.float32, "D2Z": torch.float64,
-           "C2R": torch.complex64, "Z2D": torch.complex128}
-    odt = {"C2C": torch.complex64, "Z2Z": torch.complex128, "R2C": torch.complex64, "D2Z": torch.complex128,
-           "C2R": torch.float32, "Z2D": torch.float64}
-    tcode = {"C2C": ffb.C2C, "Z2Z": ffb.Z2Z, "R2C": ffb.R2C, "D2Z": ffb.D2Z, "C2R": ffb.C2R, "Z2D": ffb.Z2D}
-
-    gen = torch.Generator(device=dev)
-    gen.manual_seed(0x46544646 + rank)
-    items = []
-    for (t, n, b) in problems:
-        in_n = n // 2 + 1 if t in ("C2R", "Z2D") else n
-        out_n = n // 2 + 1 if t in ("R2C", "D2Z") else n
-        dt = cdt[t]
-        if dt.is_complex:
-            real = torch.float32 if dt == torch.complex64 else torch.float64
-            x = torch.view_as_complex((torch.rand((b, in_n, 2), generator=gen, device=dev, dtype=real) * 2 - 1)
-                                      .contiguous())
-        else:
-            x = torch.rand((b, in_n), generator=gen, device=dev, dtype=dt) * 2 - 1
-        y = torch.empty((b, out_n), dtype=odt[t], device=dev)
-        plan = ffb.plan1d(n, tcode[t], b)
-        plan.set_stream(stream)
-        ib, ob = elem_bytes(t)
-        onchip = plan.launch_count(-1 if t not in ("C2R", "Z2D") else 1) == 1
-        items.append({"t": t, "n": n, "b": b, "x": x, "y": y, "plan": plan, "in_n": in_n, "out_n": out_n,
-                      "alg_bytes": (1 if onchip else 2) * b * (in_n * ib + out_n * ob),
-                      "launches": plan.launch_count(1 if t in ("C2R", "Z2D") else -1)})
+    calls = build_calls(WORKLOADS[args.workload], dev, rank, torch, ffb)
+    for c in calls:
+        c["plan"].set_stream(stream)
 
     def step():
-        for it in items:
-            it["plan"].execute(it["x"], it["y"], -1)
+        for c in calls:
+            c["plan"].execute(c["x"], c["y"], c["dir"])
 
-    # correctness spot check against cuFFT (torch.fft) on the first problem, untimed
+    # correctness spot check against cuFFT (torch.fft, FP64) on the first call, untimed
     check = None
-    it0 = items[0]
-    if it0["t"] in ("C2C", "Z2Z"):
+    c0 = calls[0]
+    if c0["t"] in ("C2C", "Z2Z"):
         with torch.cuda.stream(stream):
-            it0["plan"].execute(it0["x"], it0["y"], -1)
+            c0["plan"].execute(c0["x"], c0["y"], c0["dir"])
         stream.synchronize()
-        ref = torch.fft.fft(it0["x"].to(torch.complex128), dim=-1)
-        err = (torch.linalg.vector_norm(it0["y"].to(torch.complex128) - ref, dim=-1) /
+        ref = torch.fft.fft(c0["x"].to(torch.complex128), dim=-1)
+        err = (torch.linalg.vector_norm(c0["y"].to(torch.complex128) - ref, dim=-1) /
                torch.linalg.vector_norm(ref, dim=-1)).max().item()
-        check = {"problem": f"{it0['t']} N={it0['n']}", "max_rel_l2_vs_cufft_fp64": err}
+        check = {"problem": c0["key"], "max_rel_l2_vs_cufft_fp64": err}
 
     def barrier():
         if world > 1:
@@ -231,55 +294,58 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     torch.cuda.synchronize()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
+    w0 = time.time()
     e0.record(stream)
     with torch.cuda.stream(stream):
         for _ in range(args.steps):
             step()
     e1.record(stream)
     torch.cuda.synchronize()
+    w1 = time.time()
     barrier()
+    sampler.mark(w0, w1)
     clocks = sampler.stop()
     total_ms = e0.elapsed_time(e1)
 
-    # ---- per-problem timing (same stream, events around each exec)
-    per = []
-    reps = max(3, args.steps)
-    for it in items:
+    # ---- per-call timing (same stream, events around repeated execs)
+    reps = max(5, min(args.steps, 50))
+    for c in calls:
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
         torch.cuda.synchronize()
         ev[0].record(stream)
         with torch.cuda.stream(stream):
             for _ in range(reps):
-                it["plan"].execute(it["x"], it["y"], -1)
+                c["plan"].execute(c["x"], c["y"], c["dir"])
         ev[1].record(stream)
         torch.cuda.synchronize()
-        ms = ev[0].elapsed_time(ev[1]) / reps
-        it["ms"] = ms
-        per.append(it)
+        c["ms"] = ev[0].elapsed_time(ev[1]) / reps
 
-    # ---- cuFFT comparator (torch.fft, same problems, same stream)
+    # ---- cuFFT comparator (torch.fft, same calls, same stream)
     cufft = None
     if not args.no_cufft:
         cufft = {}
-        for it in items:
-            fn = {"C2C": torch.fft.fft, "Z2Z": torch.fft.fft, "R2C": torch.fft.rfft, "D2Z": torch.fft.rfft}.get(it["t"])
-            if fn is None:
-                continue
+        for c in calls:
+            t, n = c["t"], c["n"]
+            fn = {"C2C": lambda x: torch.fft.fft(x, dim=-1) if c["dir"] < 0 else torch.fft.ifft(x, dim=-1),
+                  "Z2Z": lambda x: torch.fft.fft(x, dim=-1) if c["dir"] < 0 else torch.fft.ifft(x, dim=-1),
+                  "R2C": lambda x: torch.fft.rfft(x, dim=-1), "D2Z": lambda x: torch.fft.rfft(x, dim=-1),
+                  "C2R": lambda x: torch.fft.irfft(x, n=n, dim=-1), "Z2D": lambda x: torch.fft.irfft(x, n=n, dim=-1),
+                  "C2C2D": lambda x: torch.fft.fft2(x)}[t]
             with torch.cuda.stream(stream):
                 for _ in range(3):
-                    fn(it["x"], dim=-1)
+                    fn(c["x"])
                 ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
                 torch.cuda.synchronize()
                 ev[0].record(stream)
                 for _ in range(reps):
-                    fn(it["x"], dim=-1)
+                    fn(c["x"])
                 ev[1].record(stream)
             torch.cuda.synchronize()
             ms = ev[0].elapsed_time(ev[1]) / reps
-            cufft[f"{it['t']}_{it['n']}"] = {"ms": ms, "gflops": flops(it["t"], it["n"], it["b"]) / ms / 1e6}
+            cufft[c["key"]] = {"ms": ms, "gflops": c["flop"] / ms / 1e6}
 
     # ---- end-to-end through the public API with host buffers
-    e2e = run_e2e(args, items, stream, torch)
+    e2e = run_e2e(args, calls, stream, torch)
 
     # ---- max over ranks
     if world > 1:
@@ -288,34 +354,40 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         total_ms, e2e_ms = tt.tolist()
         e2e["ms_per_step"] = e2e_ms
-    for it in items:
-        it["plan"].destroy()
-    return {"total_ms": total_ms, "per": per, "clocks": clocks, "check": check, "cufft": cufft, "e2e": e2e}
+    for c in calls:
+        c["plan"].destroy()
+    return {"total_ms": total_ms, "calls": calls, "clocks": clocks, "check": check, "cufft": cufft, "e2e": e2e}
 
 
-def run_e2e(args, items, stream, torch):
-    """Same step through the public API with host buffers: per step the inputs
-    are copied from pinned host memory and the results read back."""
-    hosts = []
-    for it in items:
-        hin = torch.empty(it["x"].shape, dtype=it["x"].dtype, pin_memory=True)
-        hin.copy_(it["x"].cpu())
-        hout = torch.empty(it["y"].shape, dtype=it["y"].dtype, pin_memory=True)
-        hosts.append((hin, hout))
-    h2d = sum(h[0].numel() * h[0].element_size() for h in hosts)
-    d2h = sum(h[1].numel() * h[1].element_size() for h in hosts)
+def run_e2e(args, calls, stream, torch):
+    """Same step through the public API with host buffers: per step each
+    problem's input is copied from pinned host memory, its calls run, and its
+    final result is read back into pinned host memory."""
+    firsts = [c for c in calls if c["first"]]
+    lasts = [calls[i] for i in range(len(calls)) if i + 1 == len(calls) or calls[i + 1]["first"]]
+    hin = [torch.empty(c["x"].shape, dtype=c["x"].dtype, pin_memory=True) for c in firsts]
+    for h, c in zip(hin, firsts):
+        h.copy_(c["x"].cpu())
+    hout = [torch.empty(c["y"].shape, dtype=c["y"].dtype, pin_memory=True) for c in lasts]
+    h2d = sum(h.numel() * h.element_size() for h in hin)
+    d2h = sum(h.numel() * h.element_size() for h in hout)
 
     def step():
         with torch.cuda.stream(stream):
-            for it, (hin, hout) in zip(items, hosts):
-                it["x"].copy_(hin, non_blocking=True)
-                it["plan"].execute(it["x"], it["y"], -1)
-                hout.copy_(it["y"], non_blocking=True)
+            fi = li = 0
+            for i, c in enumerate(calls):
+                if c["first"]:
+                    c["x"].copy_(hin[fi], non_blocking=True)
+                    fi += 1
+                c["plan"].execute(c["x"], c["y"], c["dir"])
+                if i + 1 == len(calls) or calls[i + 1]["first"]:
+                    hout[li].copy_(c["y"], non_blocking=True)
+                    li += 1
 
     for _ in range(max(1, args.warmup // 2)):
         step()
     torch.cuda.synchronize()
-    steps = max(3, args.steps // 4)
+    steps = max(3, min(args.steps // 4, 50))
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
@@ -331,48 +403,65 @@ def run_e2e(args, items, stream, torch):
 # CPU baseline / reference arm: the oracle port of the reference algorithm
 # ---------------------------------------------------------------------------
 
-def _cpu_sample_problem(job):
-    """One bounded CPU job: (type, n, rows).  Returns (seconds, flop)."""
-    t, n, rows = job
+def _cpu_sample_job(job):
+    """One bounded CPU job: (kind, type, n, rows).  kind "port" runs the oracle
+    restatement of the reference's algorithm; kind "scipy" runs scipy's FP64
+    FFT on the same rows.  Returns (seconds, flop)."""
+    kind, t, n, rows = job
     import numpy as np
     sys.path.insert(0, str(ROOT))
     from oracle import oracle as O
-    O.build()
-    plans = O.ref_plans()
-    double = t == "Z2Z"
-    plan = plans.get(f"{n}:{'z' if double else 'c'}") or O.default_plan(n)
-    x = O.random_complex(n * rows, n + rows, double).reshape(rows, n).astype(np.complex128)
+    double = t in ("Z2Z", "D2Z")
+    if t in ("C2C", "Z2Z"):
+        x = O.random_complex(n * rows, n + rows, double).reshape(rows, n).astype(np.complex128)
+    else:
+        x = O.random_real(n * rows, n + rows, double).reshape(rows, n).astype(np.float64)
     t0 = time.perf_counter()
-    O.c2c(x, -1, plan, precision="f64" if double else "f32")
-    return time.perf_counter() - t0, flops(t, n, rows)
+    if kind == "scipy":
+        import scipy.fft
+        (scipy.fft.fft if t in ("C2C", "Z2Z") else scipy.fft.rfft)(x, axis=-1, workers=1)
+    else:
+        O.build()
+        plan = O.ref_plans().get(f"{n}:{'z' if double else 'c'}") or O.default_plan(n)
+        if t in ("C2C", "Z2Z"):
+            O.c2c(x, -1, plan, precision="f64" if double else "f32")
+        else:
+            O.r2c(x, precision="f64" if double else "f32")
+    return time.perf_counter() - t0, flops_one(t, n, rows)
 
 
-def cpu_baseline(problems, budget_s: float, threads: int) -> dict:
-    """Times the oracle (a CPU port of the reference's Exec algorithms, float
-    arithmetic for C2C and double for Z2Z) on a bounded sample of the workload:
-    a few rows of each problem, run as one process per core."""
+def cpu_baseline(problems, budget_s: float, threads: int, kind: str = "port") -> dict:
+    """Times the oracle port (the reference's Exec algorithms restated in C;
+    float arithmetic for single-precision types, double for Z2Z / D2Z) on a
+    bounded sample of the workload: a few rows of each 1-D problem up to 2^20
+    points, one process per core, for about budget_s seconds."""
     import multiprocessing as mp
 
     jobs = []
-    for (t, n, b) in problems:
-        if t not in ("C2C", "Z2Z"):
+    for (t, n, b, mode) in problems:
+        if t == "C2C2D" or n > (1 << 20):
             continue
         rows = 2 if n > 5000 else 4
-        jobs += [(t, n, rows)] * threads
+        jobs += [(kind, t, n, rows)] * threads
+    if not jobs:
+        return {"value": None, "unit": "GFLOP/s", "cores": threads, "kind": kind,
+                "sample": "no problem of the workload fits the bounded CPU sample"}
     ctx = mp.get_context("spawn")
     t0 = time.perf_counter()
-    done_flop, busy = 0.0, 0.0
+    done_flop, njobs = 0.0, 0
     with ctx.Pool(threads) as pool:
-        for sec, fl in pool.imap_unordered(_cpu_sample_problem, jobs):
+        for sec, fl in pool.imap_unordered(_cpu_sample_job, jobs * 64):
             done_flop += fl
-            busy += sec
+            njobs += 1
             if time.perf_counter() - t0 > budget_s:
                 break
+        pool.terminate()
     wall = time.perf_counter() - t0
-    return {"value": done_flop / wall / 1e9, "unit": "GFLOP/s", "cores": threads, "kind": "port",
-            "sample": f"{len(jobs)} jobs of 2-4 rows of each problem of the workload, oracle port (reference "
-                      f"algorithm restated in C; float for C2C, double for Z2Z), {threads} processes, "
-                      f"{wall:.1f}s wall"}
+    what = ("oracle port (reference algorithm restated in C; float for single precision, double for "
+            "Z2Z/D2Z)" if kind == "port" else "scipy.fft FP64, 1 worker per process")
+    return {"value": done_flop / wall / 1e9, "unit": "GFLOP/s", "cores": threads, "kind": kind,
+            "sample": f"{njobs} jobs of 2-4 rows of each 1-D problem of the workload (N <= 2^20), {what}, "
+                      f"{threads} processes, {wall:.1f}s wall"}
 
 
 def run_reference(args, rank: int, world: int):
@@ -381,17 +470,16 @@ def run_reference(args, rank: int, world: int):
     problems = WORKLOADS[args.workload]
     threads = os.cpu_count() or 1
     vals = []
-    for _ in range(args.warmup):
-        pass
     for _ in range(max(1, min(args.steps, 3))):
         vals.append(cpu_baseline(problems, min(args.cpu_seconds, 20.0), threads))
-    v = statistics.median(x["value"] for x in vals)
-    total_flop = sum(flops(t, n, b) for (t, n, b) in problems)
-    ms = total_flop / (v * 1e9) * 1e3 if v > 0 else None
+    good = [x["value"] for x in vals if x["value"]]
+    v = statistics.median(good) if good else None
+    total_flop = sum(problem_flops(p) for p in problems)
+    ms = total_flop / (v * 1e9) * 1e3 if v else None
     line = {
         "impl": "reference", "metric": "gflops_5nlog2n", "value": v, "unit": "GFLOP/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "c64+c128", "data": "synthetic",
+        "scaling": "weak", "vs_baseline": None, "dtype": dtype_of(problems), "data": "synthetic",
         "config": {"workload": args.workload, "problems": WORKLOAD_DESC[args.workload]},
         "cpu_baseline": {**vals[-1], "value": v},
         "e2e": {"value": v, "unit": "GFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -401,6 +489,11 @@ def run_reference(args, rank: int, world: int):
     }
     print(json.dumps(line))
     return 0
+
+
+def dtype_of(problems) -> str:
+    names = {"C2C": "c64", "C2C2D": "c64", "Z2Z": "c128", "R2C": "f32", "D2Z": "f64"}
+    return "+".join(sorted({names[p[0]] for p in problems}))
 
 
 # ---------------------------------------------------------------------------
@@ -423,38 +516,44 @@ def main():
                                 device_id=torch.device("cuda", local_rank))
     res = run_ours(args, rank, world, local_rank)
     problems = WORKLOADS[args.workload]
-    step_flop = sum(flops(t, n, b) for (t, n, b) in problems)
+    step_flop = sum(problem_flops(p) for p in problems)
     ms_step = res["total_ms"] / args.steps
     value = step_flop * world / (ms_step * 1e-3) / 1e9
     peaks = measured_peaks()
+    traffic = profiled_traffic()
 
-    per_n = []
+    per_call = []
     dominant = None
-    for it in res["per"]:
-        gbs = it["alg_bytes"] / (it["ms"] * 1e-3) / 1e9
-        row = {"type": it["t"], "N": it["n"], "batch": it["b"], "ms": it["ms"],
-               "gflops": flops(it["t"], it["n"], it["b"]) / it["ms"] / 1e6, "alg_GBs": gbs,
-               "hbm_frac": gbs / peaks["hbm_gbs"], "launches": it["launches"], "alg_bytes": it["alg_bytes"]}
-        per_n.append(row)
-        if dominant is None or row["ms"] > dominant["ms"]:
+    for c in res["calls"]:
+        gbs = c["alg_bytes"] / (c["ms"] * 1e-3) / 1e9
+        row = {"call": c["key"], "ms": c["ms"], "gflops": c["flop"] / c["ms"] / 1e6, "alg_GBs": gbs,
+               "hbm_frac": gbs / peaks["hbm_gbs"], "launches": c["launches"], "alg_bytes": c["alg_bytes"],
+               "ms_per_launch": c["ms"] / max(1, c["launches"])}
+        per_call.append(row)
+        if dominant is None or row["ms_per_launch"] > dominant["ms_per_launch"]:
             dominant = row
-    launches_per_step = sum(it["launches"] for it in res["per"])
+    launches_per_step = sum(c["launches"] for c in res["calls"])
 
     if rank == 0:
         e2e_ms = res["e2e"]["ms_per_step"]
+        alg_per_launch = dominant["alg_bytes"] / max(1, dominant["launches"])
+        achieved = alg_per_launch / (dominant["ms_per_launch"] * 1e-3) / 1e9
+        tr = traffic.get(dominant["call"])
         line = {
             "metric": "gflops_5nlog2n", "value": value, "unit": "GFLOP/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "c64+c128" if args.workload == "arbitrary_1d" else "mixed",
+            "scaling": "weak", "vs_baseline": None, "dtype": dtype_of(problems),
             "data": "synthetic (seeded uniform[-1,1) re/im)",
             "config": {"workload": args.workload, "problems": WORKLOAD_DESC[args.workload],
-                       "l2": "per-step footprint above the 126 MB L2 (inputs+outputs)",
+                       "l2": "inputs larger than the 126 MB L2 across a step (no flush)",
                        "parallelism": f"replicas over batch, {world} GPU"},
-            "per_n": per_n,
-            "roofline": {"bound": "hbm", "kernel": f"{dominant['type']} N={dominant['N']}",
-                         "achieved": dominant["alg_GBs"], "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                         "frac": dominant["hbm_frac"], "traffic": None, "peak_source": peaks["source"],
-                         "alg_bytes_per_launch": dominant["alg_bytes"] / max(1, dominant["launches"])},
+            "per_call": per_call,
+            "roofline": {"bound": "hbm", "kernel": dominant["call"], "achieved": achieved,
+                         "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
+                         "traffic": tr["dram_bytes_per_launch"] if tr else None,
+                         "traffic_source": tr["source"] if tr else None,
+                         "peak_source": peaks["source"], "alg_bytes_per_launch": alg_per_launch,
+                         "ms_per_launch": dominant["ms_per_launch"]},
             "e2e": {"value": step_flop * world / (e2e_ms * 1e-3) / 1e9, "unit": "GFLOP/s",
                     "h2d_bytes_per_step": res["e2e"]["h2d_bytes_per_step"],
                     "d2h_bytes_per_step": res["e2e"]["d2h_bytes_per_step"], "ms_per_step": e2e_ms},
