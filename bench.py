@@ -134,72 +134,93 @@ def profiled_traffic() -> dict:
 
 
 class ClockSampler:
-    """nvidia-smi SM clock / throttle-reason samples; only samples that arrive
-    inside the timed window are kept."""
+    """SM clock / throttle-reason samples (NVML, read only, every ~2 ms) while
+    the timed region runs; only samples taken inside the timed window are
+    kept.  Falls back to `nvidia-smi -lms 50` when NVML is unavailable."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = {"hw_slowdown": 0x8, "hw_thermal_slowdown": 0x40, "sw_thermal_slowdown": 0x20, "sw_power_cap": 0x4}
 
-    def __init__(self, device_index: int):
+    def __init__(self, device_index: int, pci_bus_id: str | None = None):
         self.dev = device_index
-        self.proc = None
-        self.lines: list[tuple[float, str]] = []
+        self.pci = pci_bus_id
+        self.samples: list[tuple[float, float, float, int]] = []  # (time, sm MHz, power W, reasons)
+        self.sm_max = None
+        self.stop_flag = threading.Event()
         self.thread = None
+        self.proc = None
         self.window = (0.0, 0.0)
 
     def start(self):
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "50"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            import pynvml
+            pynvml.nvmlInit()
+            h = (pynvml.nvmlDeviceGetHandleByPciBusId(self.pci) if self.pci
+                 else pynvml.nvmlDeviceGetHandleByIndex(self.dev))
+            self.sm_max = float(pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM))
+
+            def poll():
+                while not self.stop_flag.is_set():
+                    try:
+                        self.samples.append((time.time(), float(pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)),
+                                             pynvml.nvmlDeviceGetPowerUsage(h) / 1000.0,
+                                             int(pynvml.nvmlDeviceGetCurrentClocksEventReasons(h))))
+                    except pynvml.NVMLError:
+                        pass
+                    time.sleep(0.002)
+
+            self.thread = threading.Thread(target=poll, daemon=True)
+            self.thread.start()
+        except Exception:
+            self._start_smi()
+        time.sleep(0.1)
+
+    def _start_smi(self):
+        fields = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+                  "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+                  "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.dev}", f"--query-gpu={fields}",
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except (OSError, FileNotFoundError):
             self.proc = None
             return
 
         def reader():
+            bits = list(self.REASONS.values())
             for line in self.proc.stdout:
-                self.lines.append((time.time(), line.strip()))
+                parts = [p.strip() for p in line.split(",")]
+                try:
+                    r = sum(b for b, f in zip(bits, parts[3:7]) if f.lower() == "active")
+                    self.sm_max = float(parts[1])
+                    self.samples.append((time.time(), float(parts[0]), float(parts[2]), r))
+                except (ValueError, IndexError):
+                    continue
 
         self.thread = threading.Thread(target=reader, daemon=True)
         self.thread.start()
-        time.sleep(0.3)  # first sample before the timed window opens
 
     def mark(self, t0: float, t1: float):
         self.window = (t0, t1)
 
     def stop(self) -> dict:
-        if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.proc.kill()
+        self.stop_flag.set()
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
         if self.thread:
             self.thread.join(timeout=2)
         t0, t1 = self.window
-        sm, smax, reasons, power = [], [], set(), []
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ts, ln in self.lines:
-            if not (t0 <= ts <= t1 + 0.06):
-                continue
-            parts = [p.strip() for p in ln.split(",")]
-            if len(parts) < 9:
-                continue
-            try:
-                sm.append(float(parts[1]))
-                smax.append(float(parts[2]))
-                power.append(float(parts[3]))
-            except ValueError:
-                continue
-            for name, flag in zip(names, parts[5:9]):
-                if flag.lower() == "active":
-                    reasons.add(name)
-        if not sm:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples inside the timed window"]}
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
-                "samples": len(sm), "power_w_max": max(power) if power else None}
+        inside = [s for s in self.samples if t0 <= s[0] <= t1]
+        if not inside:
+            return {"sm_mhz": None, "sm_max_mhz": self.sm_max, "reasons": ["no samples inside the timed window"]}
+        reasons = sorted(name for name, bit in self.REASONS.items() if any(s[3] & bit for s in inside))
+        return {"sm_mhz": statistics.median(s[1] for s in inside), "sm_max_mhz": self.sm_max, "reasons": reasons,
+                "samples": len(inside), "power_w_max": max(s[2] for s in inside),
+                "source": "nvml" if self.proc is None else "nvidia-smi"}
 
 
 # ---------------------------------------------------------------------------
@@ -288,7 +309,11 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     torch.cuda.synchronize()
 
     # ---- whole-step timing
-    sampler = ClockSampler(torch.cuda.current_device())
+    props = torch.cuda.get_device_properties(dev)
+    pci = None
+    if all(hasattr(props, f) for f in ("pci_domain_id", "pci_bus_id", "pci_device_id")):
+        pci = f"{props.pci_domain_id:08X}:{props.pci_bus_id:02X}:{props.pci_device_id:02X}.0"
+    sampler = ClockSampler(torch.cuda.current_device(), pci)
     sampler.start()
     barrier()
     torch.cuda.synchronize()
