@@ -97,7 +97,8 @@ def build_hostcheck(force: bool = False, jobs: int | None = None, verbose: bool 
             todo.append((src, obj))
 
     def comp(src, obj):
-        cmd = [nvcc(), "-x", "cu", *NVCC_COMMON, "-O2", "-DFFB_HOST_EMULATION", *ARCH, "-c", str(src), "-o", str(obj)]
+        common = [f for f in NVCC_COMMON if f != "-O3"]
+        cmd = [nvcc(), "-x", "cu", *common, "-O2", "-DFFB_HOST_EMULATION", *ARCH, "-c", str(src), "-o", str(obj)]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)

@@ -20,6 +20,7 @@
 #include "exec.hpp"
 
 #include <algorithm>
+#include <unordered_map>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -227,6 +228,118 @@ static std::vector<int> flatten(const NodePtr &node) {
   return {};
 }
 
+// ---------------------------------------------------------------------------
+// Convolution length of a Bluestein node.  Any M >= 2n - 1 gives the same
+// DFT; the plan's M is the reference planner's choice for its own kernels.
+// The executor runs the convolution at the length its own stages do fastest:
+// the one minimising M x (per-element cost of its cheapest radix chain).
+// Per element-stage cost in instructions: a fixed part for addressing, the
+// two shared-memory accesses, loop control and twiddle (kStageFixed), plus the
+// codelet's and the twiddle multiply's arithmetic (~0.6 instructions per flop
+// with fused multiply-adds).
+// ---------------------------------------------------------------------------
+namespace {
+constexpr double kStageFixed = 28.0;
+
+// flops of the forward codelet of radix R (engine.cuh's Dft / DftPrime /
+// DftSplit structure)
+double codelet_flops(int R) {
+  switch (R) {
+    case 2: return 4;
+    case 3: return 12;
+    case 4: return 16;
+    case 6: return 48;
+    case 8: return 56;
+    case 9: return 96;
+    case 10: return 148;
+    case 12: return 132;
+    case 15: return 264;
+    case 16: return 173;
+    default: {  // odd prime: pairs, then (R-1)/2 outputs of (R-1)/2 fused terms each
+      const double H = (R - 1) / 2.0;
+      return 8 * H * H + 10 * H;
+    }
+  }
+}
+
+double stage_cost(int R) { return kStageFixed + 0.6 * (codelet_flops(R) / R + 6.0 * (R - 1) / R); }
+
+// Cheapest chain of supported radices with product m (per element), radices
+// largest first; infinite when m has a prime factor above 19.
+double chain_cost(int64_t m, std::vector<int> *radices, std::unordered_map<int64_t, std::pair<double, int>> &memo) {
+  if (m == 1) {
+    if (radices) radices->clear();
+    return 0.0;
+  }
+  auto it = memo.find(m);
+  if (it == memo.end()) {
+    double best = 1e30;
+    int best_r = 0;
+    for (int64_t R : kSupportedRadices) {
+      if (m % R) continue;
+      const double c = stage_cost((int)R) + chain_cost(m / R, nullptr, memo);
+      if (c < best) {
+        best = c;
+        best_r = (int)R;
+      }
+    }
+    it = memo.emplace(m, std::make_pair(best, best_r)).first;
+  }
+  const double cost = it->second.first;
+  if (radices) {
+    // every value on the best chain was memoised by the recursion above
+    radices->clear();
+    for (int64_t v = m; v > 1 && memo.at(v).second != 0; v /= memo.at(v).second) radices->push_back(memo.at(v).second);
+    std::sort(radices->rbegin(), radices->rend());
+  }
+  return cost;
+}
+
+// On-chip convolution length for a length-n Bluestein: the M in
+// [2n - 1, maxL] with the least M x chain cost; 0 if none fits.
+int64_t choose_conv_length(int64_t n, int64_t maxL, std::vector<int> *radices) {
+  std::unordered_map<int64_t, std::pair<double, int>> memo;
+  int64_t best_m = 0;
+  double best = 1e30;
+  const int64_t lo = 2 * n - 1, hi = std::min<int64_t>(maxL, 2 * lo + 64);
+  for (int64_t m = lo; m <= hi; ++m) {
+    const double c = (double)m * chain_cost(m, nullptr, memo);
+    if (c < best) {
+      best = c;
+      best_m = m;
+    }
+  }
+  if (best_m) chain_cost(best_m, radices, memo);
+  return best_m;
+}
+
+// Three-pass convolution M = n1 * n2: n1 one codelet (the register-column
+// passes), n2 on chip (the convolution rows).  Minimises M x chain cost of n2
+// (the column passes cost about the same for every n1).
+int64_t choose_split_conv(int64_t n, int64_t maxL, int64_t *n1_out, std::vector<int> *row_radices) {
+  std::unordered_map<int64_t, std::pair<double, int>> memo;
+  static const int kCols[] = {16, 15, 13, 12, 11, 10, 9, 8};
+  int64_t best_m = 0, best_n1 = 0;
+  double best = 1e30;
+  const int64_t lo = 2 * n - 1, hi = lo + lo / 4 + 64;
+  for (int64_t m = lo; m <= hi; ++m)
+    for (int n1 : kCols) {
+      if (m % n1 || m / n1 > maxL) continue;
+      const double c = (double)m * chain_cost(m / n1, nullptr, memo);
+      if (c < best) {
+        best = c;
+        best_m = m;
+        best_n1 = n1;
+      }
+    }
+  if (best_m) {
+    *n1_out = best_n1;
+    chain_cost(best_m / best_n1, row_radices, memo);
+  }
+  return best_m;
+}
+}  // namespace
+
 static Core make_dit_core(int64_t L, const std::vector<int> &r) {
   if ((int)r.size() > kMaxStages) throw std::runtime_error("too many radix stages");
   Core c{};
@@ -287,9 +400,10 @@ class Builder {
       return true;
     }
     if (node->kind == NodeKind::Bluestein) {
-      auto rc = flatten(node->child);
-      if (!rc.empty() && node->conv_length <= maxL) {
-        spec = {CoreKind::Bluestein, node->length, node->conv_length, rc, node};
+      std::vector<int> rc;
+      const int64_t m = choose_conv_length(node->length, maxL, &rc);
+      if (m) {
+        spec = {CoreKind::Bluestein, node->length, m, rc, node};
         return true;
       }
     }
@@ -469,9 +583,9 @@ class Builder {
   // Bluestein kernel spectrum B[k] / M laid out per row k1 of an n1 x n2
   // four-step: entry k1 * n2 + p holds B[k1 + n1 k2] for p = k2 (Stockham
   // passes) or the n2-point DIF position of k2 (in-place passes).
-  const cpx<T> *table_bluestein_rows(const NodePtr &node, const std::vector<int> &col_radices, int64_t n1,
-                                     int64_t n2, bool inverse, bool natural) {
-    const int64_t n = node->length, M = node->conv_length;
+  const cpx<T> *table_bluestein_rows(int64_t n, const std::vector<int> &col_radices, int64_t n1, int64_t n2,
+                                     bool inverse, bool natural) {
+    const int64_t M = n1 * n2;
     const int sign = inverse ? 1 : -1;
     std::vector<cld> b((size_t)M, cld(0));
     for (int64_t k = 0; k < n; ++k) {
@@ -573,9 +687,11 @@ class Builder {
 // from `src` to `dst`; `ws` is a workspace of batch * (n or the Bluestein
 // convolution length) elements when the plan needs more than one pass.
 // On-chip policy ($FLAGFFT_ONCHIP_POLICY): by default a transform that fits
-// one CTA (two Stockham buffers, or in place) runs as one pass; "multipass"
-// splits every tree that has a multi-pass lowering instead (one HBM round
-// trip more, but smaller, more numerous CTAs).
+// one CTA (two Stockham buffers, or in place) runs as one pass, except a
+// Bluestein convolution that fits only in place, which takes the three-pass
+// chain; "multipass" splits every tree that has a multi-pass lowering (one
+// HBM round trip more, but smaller, more numerous CTAs); "inplace" keeps
+// every transform that fits one CTA in one pass.
 static int onchip_policy() {
   const char *v = std::getenv("FLAGFFT_ONCHIP_POLICY");
   if (!v) return 0;
@@ -590,11 +706,15 @@ void lower_c2c(Builder<T> &bld, Program &prog, const NodePtr &root, bool inverse
   const bool onchip = bld.core_for(root, spec);
   CoreSpec ca, cb;
   const bool mp_four = root->kind == NodeKind::FourStep && bld.core_for(root->row, ca) && bld.core_for(root->col, cb);
-  const bool mp_blue = root->kind == NodeKind::Bluestein && root->child->kind == NodeKind::FourStep &&
-                       bld.core_for(root->child->row, ca) && bld.core_for(root->child->col, cb) &&
-                       ca.kind == CoreKind::Dit && cb.kind == CoreKind::Dit;
+  const bool mp_blue = root->kind == NodeKind::Bluestein;  // three-pass chain at an executor-chosen split
   const int policy = onchip_policy();
-  const bool use_onchip = onchip && (policy != 2 || !(mp_four || mp_blue));
+  // A Bluestein convolution that fits one CTA only in place (not as two
+  // ping-pong buffers) runs faster as the three-pass chain: its 1-CTA-per-SM
+  // in-place pass is latency-bound (C2C N=10007 on B200: 440 us fused vs
+  // 414 us in three passes).
+  const bool blue_in_place = onchip && spec.kind == CoreKind::Bluestein && !Builder<T>::pp_fits(spec.L);
+  const bool use_onchip =
+      onchip && (policy == 1 || ((policy != 2 || !(mp_four || mp_blue)) && !blue_in_place));
   if (use_onchip) {
     bld.add_pass(spec, IoKind::C2C, inverse, 1, batch, 0, idist, 1, 0, odist, 1, src, dst, n);
     return;
@@ -613,16 +733,18 @@ void lower_c2c(Builder<T> &bld, Program &prog, const NodePtr &root, bool inverse
       return;
     }
   }
-  if (root->kind == NodeKind::Bluestein && root->child->kind == NodeKind::FourStep) {
-    // Convolution of length M = n1 * n2 too long for one CTA: three passes
-    // through an M-point workspace, with the chirps, the kernel product and
-    // both four-step twiddles fused (src/exec/raw_nodes.cpp:153-204 runs the
-    // same chain as 7 launches).
-    const NodePtr &fs = root->child;
-    CoreSpec sa, sb;
-    if (bld.core_for(fs->row, sa) && bld.core_for(fs->col, sb) && sa.kind == CoreKind::Dit &&
-        sb.kind == CoreKind::Dit) {
-      const int64_t M = root->conv_length, n1 = fs->n1, n2 = fs->n2;
+  if (root->kind == NodeKind::Bluestein) {
+    // Convolution too long for one CTA: three passes through an M-point
+    // workspace, M = n1 x n2 chosen by the executor (n1 one codelet, n2 on
+    // chip), with the chirps, the kernel product and both four-step twiddles
+    // fused (src/exec/raw_nodes.cpp:153-204 runs the same chain as 7 launches).
+    int64_t n1 = 0;
+    std::vector<int> row_radices;
+    const int64_t M = choose_split_conv(n, max_onchip_length(sizeof(T) == 8), &n1, &row_radices);
+    if (M) {
+      const int64_t n2 = M / n1;
+      const CoreSpec sa{CoreKind::Dit, n1, n1, {(int)n1}, nullptr};
+      const CoreSpec sb{CoreKind::Dit, n2, n2, row_radices, nullptr};
       prog.scratch0 = std::make_shared<DevMem>((size_t)(batch * M) * sizeof(cpx<T>));
       const cpx<T> *chirp = bld.table_chirp(n, inverse);
       // A: a_j = x_j c_j (j = j1 n2 + j2 < n), FFT over j1, x W_M^{j2 k1} -> Y[k1][j2]
@@ -637,7 +759,7 @@ void lower_c2c(Builder<T> &bld, Program &prog, const NodePtr &root, bool inverse
       CoreSpec sc = sb;
       sc.kind = CoreKind::Conv;
       auto *pb = bld.add_pass(sc, IoKind::C2C, true, batch, n1, M, n2, 1, M, n2, 1, Buf::Scratch0, Buf::Scratch0, n2);
-      pb->a.kern = bld.table_bluestein_rows(root, sb.radices, n1, n2, inverse, pb->a.pp != 0);
+      pb->a.kern = bld.table_bluestein_rows(n, sb.radices, n1, n2, inverse, pb->a.pp != 0);
       pb->a.kern_stride = n2;
       bld.set_post_twiddle(pb->a, M);
       pb->note = "bluestein 2/3: row convolution";

@@ -167,3 +167,19 @@ def test_2d_vs_oracle(ffb, torch_cuda, shape, batch):
     torch.cuda.synchronize()
     _check(O.error_stats(back.cpu().numpy().reshape(batch, -1), (xr * n0 * n1).reshape(batch, -1)), O.C2R, n0 * n1)
     pc.destroy()
+
+
+@pytest.mark.parametrize("policy", ["inplace", "multipass"])
+@pytest.mark.parametrize("double", [False, True], ids=["C2C", "Z2Z"])
+@pytest.mark.parametrize("n", [1009, 1701, 4096, 10007, 20020])
+def test_lowering_policies(ffb, torch_cuda, plans, monkeypatch, policy, double, n):
+    """Every lowering of a tree (one fused pass in place, or the multi-pass
+    chain) meets the same bounds; FLAGFFT_ONCHIP_POLICY is read at plan time."""
+    monkeypatch.setenv("FLAGFFT_ONCHIP_POLICY", policy)
+    batch = 3
+    ftype = O.Z2Z if double else O.C2C
+    x = O.random_complex(n * batch, O.accuracy_seed(ftype, n, batch, 2), double).reshape(batch, n)
+    plan = _ref_plan(plans, n, double)
+    for direction in (-1, 1):
+        got = _run_c2c(ffb, torch_cuda, x, direction, double)
+        _check(O.error_stats(got, O.c2c(x.astype(np.complex128), direction, plan)), ftype, n)
