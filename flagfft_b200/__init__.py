@@ -17,7 +17,7 @@ import os
 from pathlib import Path
 
 __all__ = [
-    "FlagFFTError", "Plan", "plan1d", "plan2d", "plan3d", "plan_many", "planner_tree", "library_path",
+    "FlagFFTError", "Plan", "plan1d", "plan2d", "plan3d", "plan_many", "plan_batch", "planner_tree", "library_path",
     "C2C", "Z2Z", "R2C", "D2Z", "C2R", "Z2D", "FORWARD", "INVERSE", "STATUS",
 ]
 
@@ -71,6 +71,7 @@ def _load():
         "flagfftB200PlannerTree": (i, [i, i, ctypes.c_longlong, cp, i]),
         "flagfftB200PlanJson": (cp, [H]),
         "flagfftB200LaunchCount": (i, [H, i]),
+        "flagfftB200PlanBatch": (i, [PH, i, ip, ip, i]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name)
@@ -234,6 +235,20 @@ def plan_many(n, inembed, istride: int, idist: int, onembed, ostride: int, odist
     _check(_lib().flagfftPlanMany(ctypes.byref(h), rank, arr(n), arr(inembed), istride, idist, arr(onembed), ostride,
                                odist, ftype, batch), "flagfftPlanMany")
     return Plan(h.value, ftype, tuple(n), batch)
+
+
+def plan_batch(lengths, counts, ftype: int = C2C) -> Plan:
+    """Batch plan (flagfftB200PlanBatch): counts[g] transforms of length
+    lengths[g], packed group after group; execute() runs all of them."""
+    lengths, counts = list(lengths), list(counts)
+    if len(lengths) != len(counts) or not lengths:
+        raise ValueError("lengths and counts must be non-empty and of equal length")
+    g = len(lengths)
+    h = ctypes.c_void_p(0)
+    _check(_lib().flagfftB200PlanBatch(ctypes.byref(h), g, (ctypes.c_int * g)(*lengths), (ctypes.c_int * g)(*counts),
+                                       ftype), "flagfftB200PlanBatch")
+    total = sum(l * c for l, c in zip(lengths, counts))
+    return Plan(h.value, ftype, (total,), 1)
 
 
 def planner_tree(n: int, is_double: bool = False, smem_bytes: int = 0) -> dict:

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -48,6 +49,10 @@ struct Plan {
   // 1-D real plans executed in place read / write padded rows of 2(n/2+1)
   // reals (src/exec/raw_nodes.cpp:425-429, 466-470)
   std::unique_ptr<Program> fwd_ip, inv_ip;
+  // batch plans (flagfftB200PlanBatch): groups of uneven lengths
+  bool is_batch = false;
+  std::vector<BatchGroup> groups;
+  std::unique_ptr<BatchProgram> bfwd, binv;
   std::string description;
   std::string json;
   std::mutex mutex;
@@ -217,6 +222,24 @@ flagfftResult exec_common(flagfftHandle h, const void *in, void *out, flagfftTyp
   if (plan->desc.type != want) return FLAGFFT_INVALID_TYPE;
   if (has_dir && dir != FLAGFFT_FORWARD && dir != FLAGFFT_INVERSE) return FLAGFFT_INVALID_VALUE;
   std::lock_guard<std::mutex> lock(plan->mutex);
+  if (plan->is_batch) {
+    BatchProgram *bp = dir == FLAGFFT_INVERSE ? plan->binv.get() : plan->bfwd.get();
+    cudaError_t e = cudaErrorInvalidValue;
+    try {
+      if (bp) e = bp->run(in, out, plan->stream);
+    } catch (const std::bad_alloc &) {
+      return FLAGFFT_ALLOC_FAILED;
+    } catch (const std::exception &ex) {
+      std::fprintf(stderr, "[flagfft] batch Exec failed: %s\n", ex.what());
+      return FLAGFFT_EXEC_FAILED;
+    }
+    if (e != cudaSuccess) {
+      std::fprintf(stderr, "[flagfft] batch Exec failed: %s\n", cudaGetErrorString(e));
+      std::fflush(stderr);
+      return FLAGFFT_EXEC_FAILED;
+    }
+    return FLAGFFT_SUCCESS;
+  }
   const Program *prog = pick(plan, in == out);
   if (prog == nullptr) return FLAGFFT_EXEC_FAILED;
   return run(plan, prog, in, out);
@@ -350,6 +373,15 @@ extern "C" const char *flagfftGetPlanDescription(flagfftHandle h) {  // c_api_ex
   o << "rank=" << d.rank << " n=[" << d.n[0];
   for (size_t i = 1; i < d.n.size(); ++i) o << "," << d.n[i];
   o << "] batch=" << d.batch << " type=" << (int)d.type << "\n";
+  if (plan->is_batch) {
+    o << "\n-- Batch --\n" << plan->groups.size() << " groups\n";
+    o << "\n-- Forward execution --\nB200BatchProgram(launches=" << plan->bfwd->launches() << ")\n"
+      << plan->bfwd->describe() << "\n";
+    o << "\n-- Inverse execution --\nB200BatchProgram(launches=" << plan->binv->launches() << ")\n"
+      << plan->binv->describe() << "\n";
+    plan->description = o.str();
+    return plan->description.c_str();
+  }
   o << "\n-- Plan tree --\n" << plan->root->describe() << "\n";
   o << "\n-- Forward execution --\n";
   if (plan->fwd)
@@ -390,6 +422,57 @@ extern "C" const char *flagfftB200PlanJson(flagfftHandle h) {
 extern "C" int flagfftB200LaunchCount(flagfftHandle h, int direction) {
   Plan *plan = checked(h);
   if (plan == nullptr || plan->destroyed || !plan->initialized) return -1;
+  if (plan->is_batch) {
+    const BatchProgram *bp = direction == FLAGFFT_INVERSE ? plan->binv.get() : plan->bfwd.get();
+    return bp ? bp->launches() : -1;
+  }
   const Program *p = direction == FLAGFFT_INVERSE ? plan->inv.get() : plan->fwd.get();
   return p ? p->launches() : -1;
+}
+
+extern "C" flagfftResult flagfftB200PlanBatch(flagfftHandle *out, int ngroups, const int *lengths, const int *counts,
+                                             flagfftType type) {
+  if (out == nullptr) return FLAGFFT_INVALID_VALUE;
+  *out = nullptr;
+  if (ngroups <= 0 || lengths == nullptr || counts == nullptr) return FLAGFFT_INVALID_VALUE;
+  if (type != FLAGFFT_C2C && type != FLAGFFT_Z2Z) return FLAGFFT_INVALID_TYPE;
+  PlanDesc d;
+  d.rank = 1;
+  d.type = type;
+  d.is_double = type == FLAGFFT_Z2Z;
+  int64_t total = 0;
+  std::vector<BatchGroup> groups;
+  for (int g = 0; g < ngroups; ++g) {
+    if (lengths[g] <= 0) return FLAGFFT_INVALID_SIZE;
+    if (counts[g] <= 0) return FLAGFFT_INVALID_VALUE;
+    groups.push_back({lengths[g], counts[g]});
+    total += (int64_t)lengths[g] * counts[g];
+  }
+  d.n = {total};
+  d.batch = 1;
+  flagfftResult dr = ensure_device(d);
+  if (dr != FLAGFFT_SUCCESS) return dr;
+  try {
+    auto plan = std::make_unique<Plan>();
+    plan->desc = d;
+    plan->is_batch = true;
+    plan->groups = groups;
+    Planner planner(d.is_double, d.smem_optin);
+    const char *g = std::getenv("FLAGFFT_BATCH_GRAPH");
+    const bool graphs = g == nullptr || std::string(g) != "0";
+    plan->bfwd = lower_batch(groups, planner, d.is_double, false, graphs);
+    plan->binv = lower_batch(groups, planner, d.is_double, true, graphs);
+    plan->root = make_direct_node(total);  // placeholder: a batch plan has one tree per group
+    plan->json = "{\"batch_groups\": " + std::to_string(ngroups) + "}";
+    plan->initialized = true;
+    auto h = std::make_unique<flagfftPlan_t>();
+    h->impl = plan.release();
+    *out = h.release();
+    return FLAGFFT_SUCCESS;
+  } catch (const std::bad_alloc &) {
+    return FLAGFFT_ALLOC_FAILED;
+  } catch (const std::exception &e) {
+    std::fprintf(stderr, "[flagfft] batch plan setup failed: %s\n", e.what());
+    return FLAGFFT_SETUP_FAILED;
+  }
 }

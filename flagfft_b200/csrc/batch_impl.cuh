@@ -1,0 +1,80 @@
+// Definitions of the batch launchers, instantiated per precision in
+// k_f32_batch.cu / k_f64_batch.cu.
+#pragma once
+
+#include "batch.cuh"
+
+namespace ffb {
+
+#ifndef FFB_HOST_EMULATION
+template <typename T>
+static cudaError_t batch_configure() {
+  static bool done = false;
+  if (!done) {
+    cudaError_t e = cudaFuncSetAttribute(batch::k_batch<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 232448);
+    if (e != cudaSuccess) return e;
+    done = true;
+  }
+  return cudaSuccess;
+}
+
+template <typename T>
+cudaError_t launch_batch(const TileArgs<T> *args, const int *kinds, const BatchItem *items, int nitems, int *next,
+                         int threads, size_t smem, int ctas, cudaStream_t s) {
+  cudaError_t e = batch_configure<T>();
+  if (e != cudaSuccess) return e;
+  batch::k_batch<T><<<ctas, threads, smem + kBatchSmemHeader, s>>>(args, kinds, items, nitems, next);
+  return cudaGetLastError();
+}
+
+template <typename T>
+int batch_resident_ctas(int threads, size_t smem) {
+  if (batch_configure<T>() != cudaSuccess) return 0;
+  int per_sm = 0, dev = 0, sms = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch::k_batch<T>, threads, smem + kBatchSmemHeader) !=
+          cudaSuccess ||
+      cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return per_sm * sms;
+}
+#else
+// Sequential host run: the ping-pong bodies with one "thread" per slot
+// (HostX), every transform of a register-column chunk in turn.
+template <typename T>
+cudaError_t launch_batch(const TileArgs<T> *args, const int *kinds, const BatchItem *items, int nitems, int *next,
+                         int threads, size_t smem, int, cudaStream_t) {
+  std::vector<unsigned char> buf(smem + 64);
+  cpx<T> *sm = reinterpret_cast<cpx<T> *>(buf.data());
+  for (int i = *next; i < nitems; ++i) {
+    const BatchItem w = items[i];
+    const TileArgs<T> &a = args[w.args];
+    if (kinds[w.args] == kBatchRegcol) {
+      const int chunks = (a.G + threads - 1) / threads;
+      const int by = w.tile / chunks;
+      for (int t = 0; t < threads; ++t) {
+        const long long g = (long long)(w.tile - by * chunks) * threads + t;
+        if (g >= a.G) break;
+        if (a.inv)
+          batch::regcol_one<T, true>(a, by, g);
+        else
+          batch::regcol_one<T, false>(a, by, g);
+      }
+    } else {
+      std::memset(buf.data(), 0xff, buf.size());
+      batch::run_item<T>(a, kinds[w.args], w.tile, sm, tile::HostX{});
+    }
+  }
+  *next = nitems;
+  return cudaSuccess;
+}
+
+template <typename T>
+int batch_resident_ctas(int, size_t) {
+  return 1;
+}
+#endif
+
+}  // namespace ffb

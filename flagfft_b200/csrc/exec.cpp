@@ -20,13 +20,18 @@
 #include "exec.hpp"
 
 #include <algorithm>
+#include <functional>
+#include <map>
+#include <mutex>
 #include <unordered_map>
 #include <cmath>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <sstream>
 #include <stdexcept>
 
+#include "batch.cuh"
 #include "tables.hpp"
 
 namespace ffb {
@@ -70,6 +75,39 @@ DevPtr upload(const void *host, size_t bytes) {
   return m;
 }
 #endif
+
+// Process-wide cache of plan tables (twiddles, chirps, kernel spectra,
+// permutations) keyed by device and content: plans of the same lengths share
+// one device copy, and a table lives while any plan holds it.
+namespace {
+std::mutex g_table_mu;
+std::map<std::string, std::weak_ptr<DevMem>> g_tables;
+
+int current_device() {
+#ifdef FFB_HOST_EMULATION
+  return 0;
+#else
+  int d = 0;
+  if (cudaGetDevice(&d) != cudaSuccess) {
+    cudaGetLastError();
+    return -1;
+  }
+  return d;
+#endif
+}
+}  // namespace
+
+DevPtr shared_table(const std::string &key, const std::function<DevPtr()> &make) {
+  const std::string k = std::to_string(current_device()) + "|" + key;
+  std::lock_guard<std::mutex> lock(g_table_mu);
+  auto it = g_tables.find(k);
+  if (it != g_tables.end()) {
+    if (DevPtr d = it->second.lock()) return d;
+  }
+  DevPtr d = make();
+  g_tables[k] = d;
+  return d;
+}
 
 cudaError_t Program::run(const void *in, void *out, cudaStream_t st) const {
   void *s0 = scratch0 ? scratch0->ptr : nullptr;
@@ -379,6 +417,24 @@ class Builder {
  public:
   Builder(Program &prog, Planner &planner) : prog_(prog), planner_(planner) {}
 
+  // A device table from the process-wide cache (built by `make` on a miss);
+  // the program keeps a reference for its lifetime.
+  template <typename V, class Make>
+  const V *cached(const std::string &key, Make make) {
+    DevPtr d = shared_table(std::string(sizeof(T) == 4 ? "f32|" : "f64|") + key, [&]() {
+      std::vector<V> h = make();
+      return upload(h.data(), h.size() * sizeof(V));
+    });
+    prog_.owned.push_back(d);
+    return reinterpret_cast<const V *>(d->ptr);
+  }
+
+  static std::string radix_key(const std::vector<int> &r) {
+    std::string k;
+    for (int v : r) k += std::to_string(v) + ",";
+    return k;
+  }
+
   static constexpr int kMaxThreads = sizeof(T) == 4 ? 512 : 256;
   static constexpr int64_t kSMs = 148;
 
@@ -532,52 +588,50 @@ class Builder {
   // sequence, stage kind and direction.
   const cpx<T> *table_stage_twiddles(Core &c, bool dif, bool inverse) {
     int64_t total = 0;
+    std::string key = "tw|" + std::to_string(c.L) + (dif ? "|dif|" : "|dit|") + (inverse ? "inv|" : "fwd|");
     for (int s = 0; s < c.nst; ++s) {
       c.twoff[s] = (int)total;
       total += (int64_t)(c.radix[s] - 1) * (dif ? c.span[s] / c.radix[s] : c.span[s]);
+      key += std::to_string(c.radix[s]) + ",";
     }
-    std::vector<int64_t> key = {c.L, dif ? 1 : 0, inverse ? 1 : 0};
-    for (int s = 0; s < c.nst; ++s) key.push_back(c.radix[s]);
-    for (auto &e : tw_cache_)
-      if (e.first == key) return reinterpret_cast<const cpx<T> *>(e.second->ptr);
-    std::vector<cpx<T>> h((size_t)std::max<int64_t>(total, 1), mk((T)1, (T)0));
-    for (int s = 0; s < c.nst; ++s) {
-      const int64_t R = c.radix[s];
-      const int64_t inner = dif ? c.span[s] / R : c.span[s];
-      for (int64_t r = 1; r < R; ++r)
-        for (int64_t j = 0; j < inner; ++j) {
-          cld w = unit_root(r * j, inner * R, inverse ? 1 : -1);
-          h[(size_t)(c.twoff[s] + (r - 1) * inner + j)] = mk((T)w.real(), (T)w.imag());
-        }
-    }
-    DevPtr d = upload(h.data(), h.size() * sizeof(cpx<T>));
-    prog_.owned.push_back(d);
-    tw_cache_.push_back({key, d});
-    return reinterpret_cast<const cpx<T> *>(d->ptr);
+    const Core cc = c;
+    return cached<cpx<T>>(key, [&]() {
+      std::vector<cpx<T>> h((size_t)std::max<int64_t>(total, 1), mk((T)1, (T)0));
+      for (int s = 0; s < cc.nst; ++s) {
+        const int64_t R = cc.radix[s];
+        const int64_t inner = dif ? cc.span[s] / R : cc.span[s];
+        for (int64_t r = 1; r < R; ++r)
+          for (int64_t j = 0; j < inner; ++j) {
+            cld w = unit_root(r * j, inner * R, inverse ? 1 : -1);
+            h[(size_t)(cc.twoff[s] + (r - 1) * inner + j)] = mk((T)w.real(), (T)w.imag());
+          }
+      }
+      return h;
+    });
   }
 
   // Real-transform twiddles W_n^k, k <= n/2.
   const cpx<T> *table_rtw(int64_t n) {
-    std::vector<cpx<T>> h((size_t)(n / 2 + 1));
-    for (int64_t k = 0; k <= n / 2; ++k) {
-      cld w = unit_root(k, n, -1);
-      h[(size_t)k] = mk((T)w.real(), (T)w.imag());
-    }
-    DevPtr d = upload(h.data(), h.size() * sizeof(cpx<T>));
-    prog_.owned.push_back(d);
-    return reinterpret_cast<const cpx<T> *>(d->ptr);
+    return cached<cpx<T>>("rtw|" + std::to_string(n), [&]() {
+      std::vector<cpx<T>> h((size_t)(n / 2 + 1));
+      for (int64_t k = 0; k <= n / 2; ++k) {
+        cld w = unit_root(k, n, -1);
+        h[(size_t)k] = mk((T)w.real(), (T)w.imag());
+      }
+      return h;
+    });
   }
 
   // Bluestein chirp exp(-+ i pi (j^2 mod 2n) / n), j < n (+ for the inverse).
   const cpx<T> *table_chirp(int64_t n, bool inverse) {
-    std::vector<cpx<T>> h((size_t)n);
-    for (int64_t j = 0; j < n; ++j) {
-      cld c = chirp_value(j, n, inverse ? 1 : -1);
-      h[(size_t)j] = mk((T)c.real(), (T)c.imag());
-    }
-    DevPtr d = upload(h.data(), h.size() * sizeof(cpx<T>));
-    prog_.owned.push_back(d);
-    return reinterpret_cast<const cpx<T> *>(d->ptr);
+    return cached<cpx<T>>("chirp|" + std::to_string(n) + (inverse ? "|inv" : "|fwd"), [&]() {
+      std::vector<cpx<T>> h((size_t)n);
+      for (int64_t j = 0; j < n; ++j) {
+        cld c = chirp_value(j, n, inverse ? 1 : -1);
+        h[(size_t)j] = mk((T)c.real(), (T)c.imag());
+      }
+      return h;
+    });
   }
 
   // Bluestein kernel spectrum B[k] / M laid out per row k1 of an n1 x n2
@@ -587,45 +641,48 @@ class Builder {
                                      bool inverse, bool natural) {
     const int64_t M = n1 * n2;
     const int sign = inverse ? 1 : -1;
-    std::vector<cld> b((size_t)M, cld(0));
-    for (int64_t k = 0; k < n; ++k) {
-      cld bc = chirp_value(k, n, -sign);
-      b[(size_t)k] = bc;
-      if (k) b[(size_t)(M - k)] = bc;
-    }
-    host_fft(b, -1);
-    std::vector<cpx<T>> h((size_t)M);
-    for (int64_t k1 = 0; k1 < n1; ++k1)
-      for (int64_t k2 = 0; k2 < n2; ++k2) {
-        cld v = b[(size_t)(k1 + n1 * k2)] / (long double)M;
-        const int64_t p = natural ? k2 : dif_position(k2, col_radices);
-        h[(size_t)(k1 * n2 + p)] = mk((T)v.real(), (T)v.imag());
+    const std::string key = "bsrows|" + std::to_string(n) + "|" + std::to_string(n1) + "x" + std::to_string(n2) +
+                            (inverse ? "|inv|" : "|fwd|") + (natural ? "nat|" : "dif|") + radix_key(col_radices);
+    return cached<cpx<T>>(key, [&]() {
+      std::vector<cld> b((size_t)M, cld(0));
+      for (int64_t k = 0; k < n; ++k) {
+        cld bc = chirp_value(k, n, -sign);
+        b[(size_t)k] = bc;
+        if (k) b[(size_t)(M - k)] = bc;
       }
-    DevPtr d = upload(h.data(), h.size() * sizeof(cpx<T>));
-    prog_.owned.push_back(d);
-    return reinterpret_cast<const cpx<T> *>(d->ptr);
+      host_fft(b, -1);
+      std::vector<cpx<T>> h((size_t)M);
+      for (int64_t k1 = 0; k1 < n1; ++k1)
+        for (int64_t k2 = 0; k2 < n2; ++k2) {
+          cld v = b[(size_t)(k1 + n1 * k2)] / (long double)M;
+          const int64_t p = natural ? k2 : dif_position(k2, col_radices);
+          h[(size_t)(k1 * n2 + p)] = mk((T)v.real(), (T)v.imag());
+        }
+      return h;
+    });
   }
 
   // Four-step post-twiddle W_N^m = hi[m / split] * lo[m % split].
   void set_post_twiddle(TileArgs<T> &a, int64_t N) {
-    int64_t split = (int64_t)std::ceil(std::sqrt((double)N));
-    int64_t nhi = (N + split - 1) / split;
-    std::vector<cpx<T>> lo((size_t)split), hi((size_t)nhi);
-    for (int64_t m = 0; m < split; ++m) {
-      cld w = unit_root(m, N, -1);
-      lo[(size_t)m] = mk((T)w.real(), (T)w.imag());
-    }
-    for (int64_t m = 0; m < nhi; ++m) {
-      cld w = unit_root(m * split, N, -1);
-      hi[(size_t)m] = mk((T)w.real(), (T)w.imag());
-    }
-    DevPtr dl = upload(lo.data(), lo.size() * sizeof(cpx<T>));
-    DevPtr dh = upload(hi.data(), hi.size() * sizeof(cpx<T>));
-    prog_.owned.push_back(dl);
-    prog_.owned.push_back(dh);
+    const int64_t split = (int64_t)std::ceil(std::sqrt((double)N));
+    const int64_t nhi = (N + split - 1) / split;
     a.post_twiddle = 1;
-    a.ptw_lo = reinterpret_cast<const cpx<T> *>(dl->ptr);
-    a.ptw_hi = reinterpret_cast<const cpx<T> *>(dh->ptr);
+    a.ptw_lo = cached<cpx<T>>("ptwlo|" + std::to_string(N), [&]() {
+      std::vector<cpx<T>> lo((size_t)split);
+      for (int64_t m = 0; m < split; ++m) {
+        cld w = unit_root(m, N, -1);
+        lo[(size_t)m] = mk((T)w.real(), (T)w.imag());
+      }
+      return lo;
+    });
+    a.ptw_hi = cached<cpx<T>>("ptwhi|" + std::to_string(N), [&]() {
+      std::vector<cpx<T>> hi((size_t)nhi);
+      for (int64_t m = 0; m < nhi; ++m) {
+        cld w = unit_root(m * split, N, -1);
+        hi[(size_t)m] = mk((T)w.real(), (T)w.imag());
+      }
+      return hi;
+    });
     a.ptw_div = make_fastdiv((uint32_t)split);
   }
 
@@ -634,53 +691,62 @@ class Builder {
   void fill_convolution(TileArgs<T> &a, const CoreSpec &spec, bool inverse) {
     const int sign = inverse ? 1 : -1;
     const int64_t L = spec.L;
-    std::vector<cld> b((size_t)L, cld(0));
+    const std::string layout = std::string(a.pp ? "|nat|" : "|dif|") + radix_key(spec.radices);
     if (spec.kind == CoreKind::Bluestein) {
       const int64_t n = spec.n;
-      std::vector<cpx<T>> ch((size_t)n);
-      for (int64_t k = 0; k < n; ++k) {
-        cld c = chirp_value(k, n, sign);
-        ch[(size_t)k] = mk((T)c.real(), (T)c.imag());
-        cld bc = chirp_value(k, n, -sign);
-        b[(size_t)k] = bc;
-        if (k) b[(size_t)(L - k)] = bc;
-      }
-      DevPtr d = upload(ch.data(), ch.size() * sizeof(cpx<T>));
-      prog_.owned.push_back(d);
-      a.chirp = reinterpret_cast<const cpx<T> *>(d->ptr);
+      a.chirp = table_chirp(n, inverse);
+      a.kern = cached<cpx<T>>("bkern|" + std::to_string(n) + "|" + std::to_string(L) + (inverse ? "|inv" : "|fwd") +
+                                  layout,
+                              [&]() {
+                                std::vector<cld> b((size_t)L, cld(0));
+                                for (int64_t k = 0; k < n; ++k) {
+                                  cld bc = chirp_value(k, n, -sign);
+                                  b[(size_t)k] = bc;
+                                  if (k) b[(size_t)(L - k)] = bc;
+                                }
+                                return kernel_spectrum(b, a.pp != 0, spec.radices);
+                              });
     } else {
       const int64_t p = spec.n, m = p - 1;
       const int64_t g = spec.node->root;
+      const std::string pk = std::to_string(p) + "|g" + std::to_string(g);
       auto idx = rader_index_table(p, g);
       // perm_in: q -> g^-q (m entries), then the log table k -> q (p entries)
-      std::vector<int> pin((size_t)(m + p), 0), pout((size_t)m);
-      for (int64_t q = 0; q < m; ++q) {
-        pin[(size_t)q] = (int)idx[(size_t)(q == 0 ? 0 : m - q)];
-        pout[(size_t)q] = (int)idx[(size_t)q];
-        pin[(size_t)(m + idx[(size_t)q])] = (int)q;
-      }
-      for (int64_t q = 0; q < m; ++q) b[(size_t)q] = unit_root(idx[(size_t)q], p, sign);
-      DevPtr di = upload(pin.data(), pin.size() * sizeof(int));
-      DevPtr dout = upload(pout.data(), pout.size() * sizeof(int));
-      prog_.owned.push_back(di);
-      prog_.owned.push_back(dout);
-      a.perm_in = reinterpret_cast<const int *>(di->ptr);
-      a.perm_out = reinterpret_cast<const int *>(dout->ptr);
+      a.perm_in = cached<int>("rpin|" + pk, [&]() {
+        std::vector<int> pin((size_t)(m + p), 0);
+        for (int64_t q = 0; q < m; ++q) {
+          pin[(size_t)q] = (int)idx[(size_t)(q == 0 ? 0 : m - q)];
+          pin[(size_t)(m + idx[(size_t)q])] = (int)q;
+        }
+        return pin;
+      });
+      a.perm_out = cached<int>("rpout|" + pk, [&]() {
+        std::vector<int> pout((size_t)m);
+        for (int64_t q = 0; q < m; ++q) pout[(size_t)q] = (int)idx[(size_t)q];
+        return pout;
+      });
+      a.kern = cached<cpx<T>>("rkern|" + pk + "|" + std::to_string(L) + (inverse ? "|inv" : "|fwd") + layout, [&]() {
+        std::vector<cld> b((size_t)L, cld(0));
+        for (int64_t q = 0; q < m; ++q) b[(size_t)q] = unit_root(idx[(size_t)q], p, sign);
+        return kernel_spectrum(b, a.pp != 0, spec.radices);
+      });
     }
+  }
+
+  // FFT(b) / L in natural order (Stockham cores) or DIF position order.
+  static std::vector<cpx<T>> kernel_spectrum(std::vector<cld> &b, bool natural, const std::vector<int> &radices) {
+    const int64_t L = (int64_t)b.size();
     host_fft(b, -1);
     std::vector<cpx<T>> kern((size_t)L);
     for (int64_t k = 0; k < L; ++k) {
       cld v = b[(size_t)k] / (long double)L;
-      kern[(size_t)(a.pp ? k : dif_position(k, spec.radices))] = mk((T)v.real(), (T)v.imag());
+      kern[(size_t)(natural ? k : dif_position(k, radices))] = mk((T)v.real(), (T)v.imag());
     }
-    DevPtr dk = upload(kern.data(), kern.size() * sizeof(cpx<T>));
-    prog_.owned.push_back(dk);
-    a.kern = reinterpret_cast<const cpx<T> *>(dk->ptr);
+    return kern;
   }
 
   Program &prog_;
   Planner &planner_;
-  std::vector<std::pair<std::vector<int64_t>, DevPtr>> tw_cache_;
 };
 
 // A length-n complex transform over `batch` rows (row distances idist / odist)
@@ -692,7 +758,10 @@ class Builder {
 // chain; "multipass" splits every tree that has a multi-pass lowering (one
 // HBM round trip more, but smaller, more numerous CTAs); "inplace" keeps
 // every transform that fits one CTA in one pass.
+thread_local int t_policy_override = -1;  // set while lowering batch groups
+
 static int onchip_policy() {
+  if (t_policy_override >= 0) return t_policy_override;
   const char *v = std::getenv("FLAGFFT_ONCHIP_POLICY");
   if (!v) return 0;
   std::string s(v);
@@ -886,6 +955,313 @@ std::unique_ptr<Program> lower_2d(const NodePtr &root, Planner &planner, bool is
                                   int64_t n0, int64_t n1, int64_t batch) {
   return is_double ? lower_2d_t<double>(root, planner, t, inverse, n0, n1, batch)
                    : lower_2d_t<float>(root, planner, t, inverse, n0, n1, batch);
+}
+
+// ---------------------------------------------------------------------------
+// Batch programs
+// ---------------------------------------------------------------------------
+namespace {
+
+template <typename T>
+struct BatchProgramT final : BatchProgram {
+  struct Group {
+    int64_t n = 0, count = 0, offset = 0;
+    std::unique_ptr<Program> prog;
+  };
+  struct PassRef {
+    int group, pass, kind;  // kind: a BatchKind, or -1 for a pass launched on its own
+  };
+  struct Phase {
+    std::vector<PassRef> passes;
+    int threads = 0;
+    size_t smem = 0;
+  };
+  // Device state for one (input, output) pair: resolved pass arguments, the
+  // work items of every phase, the queue counters and the captured graph.
+  struct Bound {
+    const void *in = nullptr;
+    void *out = nullptr;
+    DevPtr args, kinds, items, counters;
+    std::vector<int> first_item, nitems, ctas;
+    std::vector<TileArgs<T>> host_args;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    ~Bound() {
+#ifndef FFB_HOST_EMULATION
+      if (exec) cudaGraphExecDestroy(exec);
+      if (graph) cudaGraphDestroy(graph);
+#endif
+    }
+  };
+
+  bool inverse = false, graphs = true;
+  std::vector<Group> groups;
+  std::vector<Phase> phases;
+  std::vector<std::unique_ptr<Bound>> bound;  // most recent last
+  std::mutex mu;
+
+  static constexpr size_t kMaxBound = 4;
+
+  const TilePass<T> *tile_pass(const PassRef &r) const {
+    return dynamic_cast<const TilePass<T> *>(groups[(size_t)r.group].prog->passes[(size_t)r.pass].get());
+  }
+
+  std::unique_ptr<Bound> bind(const void *in, void *out) {
+    auto b = std::make_unique<Bound>();
+    b->in = in;
+    b->out = out;
+    std::vector<int> kinds;
+    std::vector<BatchItem> items;
+    for (const Phase &ph : phases) {
+      b->first_item.push_back((int)items.size());
+      struct Cost {
+        double c;
+        int args, tiles;
+      };
+      std::vector<Cost> order;
+      for (const PassRef &r : ph.passes) {
+        if (r.kind < 0) continue;
+        const Group &g = groups[(size_t)r.group];
+        const TilePass<T> *tp = tile_pass(r);
+        TileArgs<T> a = tp->a;
+        const cpx<T> *gin = reinterpret_cast<const cpx<T> *>(in) + g.offset;
+        cpx<T> *gout = reinterpret_cast<cpx<T> *>(out) + g.offset;
+        void *s0 = g.prog->scratch0 ? g.prog->scratch0->ptr : nullptr;
+        void *s1 = g.prog->scratch1 ? g.prog->scratch1->ptr : nullptr;
+        a.in = TilePass<T>::pick(tp->src, gin, gout, s0, s1);
+        a.out = TilePass<T>::pick(tp->dst, gin, gout, s0, s1);
+        const int idx = (int)b->host_args.size();
+        b->host_args.push_back(a);
+        kinds.push_back(r.kind);
+        const int width = r.kind == kBatchRegcol ? ph.threads : a.W;
+        const int tiles = (int)(((int64_t)a.G + width - 1) / width * a.nbatch);
+        // longest items first: per-tile work ~ transforms x length x stages
+        const double c = r.kind == kBatchRegcol ? 0.0 : (double)a.W * a.core.L * (a.core.nst + a.core2.nst);
+        order.push_back({c, idx, tiles});
+      }
+      std::stable_sort(order.begin(), order.end(), [](const Cost &x, const Cost &y) { return x.c > y.c; });
+      for (const Cost &o : order)
+        for (int t = 0; t < o.tiles; ++t) items.push_back({o.args, t});
+      b->nitems.push_back((int)items.size() - b->first_item.back());
+      b->ctas.push_back(std::max(1, batch_resident_ctas<T>(std::max(ph.threads, 32), ph.smem)));
+    }
+    // (a phase of passes that all launch on their own has no items; keep the
+    // uploads non-empty)
+    std::vector<TileArgs<T>> args_up = b->host_args;
+    if (args_up.empty()) args_up.push_back(TileArgs<T>{});
+    if (kinds.empty()) kinds.push_back(-1);
+    if (items.empty()) items.push_back({0, 0});
+    b->args = upload(args_up.data(), args_up.size() * sizeof(TileArgs<T>));
+    b->kinds = upload(kinds.data(), kinds.size() * sizeof(int));
+    b->items = upload(items.data(), items.size() * sizeof(BatchItem));
+    std::vector<int> zeros(phases.size() + 1, 0);
+    b->counters = upload(zeros.data(), zeros.size() * sizeof(int));
+    return b;
+  }
+
+  // The launches of every phase, in order, on stream st.
+  cudaError_t enqueue(const Bound &b, cudaStream_t st) {
+    for (size_t p = 0; p < phases.size(); ++p) {
+      const Phase &ph = phases[p];
+      for (const PassRef &r : ph.passes) {
+        if (r.kind >= 0) continue;
+        const Group &g = groups[(size_t)r.group];
+        const cpx<T> *gin = reinterpret_cast<const cpx<T> *>(b.in) + g.offset;
+        cpx<T> *gout = reinterpret_cast<cpx<T> *>(b.out) + g.offset;
+        void *s0 = g.prog->scratch0 ? g.prog->scratch0->ptr : nullptr;
+        void *s1 = g.prog->scratch1 ? g.prog->scratch1->ptr : nullptr;
+        cudaError_t e = g.prog->passes[(size_t)r.pass]->run(gin, gout, s0, s1, st);
+        if (e != cudaSuccess) {
+          std::fprintf(stderr, "[flagfft] batch phase %zu: own launch of group %d pass %d: %s\n", p, r.group, r.pass,
+                       cudaGetErrorString(e));
+          return e;
+        }
+      }
+      if (b.nitems[p] == 0) continue;
+      int *counter = reinterpret_cast<int *>(b.counters->ptr) + p;
+#ifndef FFB_HOST_EMULATION
+      cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(int), st);
+      if (e != cudaSuccess) return e;
+#else
+      cudaError_t e = cudaSuccess;
+      *counter = 0;
+#endif
+      e = launch_batch<T>(reinterpret_cast<const TileArgs<T> *>(b.args->ptr), reinterpret_cast<const int *>(b.kinds->ptr),
+                          reinterpret_cast<const BatchItem *>(b.items->ptr) + b.first_item[p], b.nitems[p], counter,
+                          std::max(ph.threads, 32), ph.smem, b.ctas[p], st);
+      if (e != cudaSuccess) {
+        std::fprintf(stderr, "[flagfft] batch phase %zu launch (%d CTAs x %d threads, %zu B shared): %s\n", p,
+                     b.ctas[p], std::max(ph.threads, 32), ph.smem, cudaGetErrorString(e));
+        return e;
+      }
+    }
+    return cudaSuccess;
+  }
+
+  cudaError_t run(const void *in, void *out, cudaStream_t st) override {
+    std::lock_guard<std::mutex> lock(mu);
+    Bound *b = nullptr;
+    for (size_t i = 0; i < bound.size(); ++i)
+      if (bound[i]->in == in && bound[i]->out == out) {
+        std::unique_ptr<Bound> hit = std::move(bound[i]);
+        bound.erase(bound.begin() + (long)i);
+        bound.push_back(std::move(hit));
+        b = bound.back().get();
+        break;
+      }
+    if (b == nullptr) {
+      if (bound.size() >= kMaxBound) {
+#ifndef FFB_HOST_EMULATION
+        cudaStreamSynchronize(st);  // the oldest binding's buffers may still be in use
+#endif
+        bound.erase(bound.begin());
+      }
+      bound.push_back(bind(in, out));
+      b = bound.back().get();
+    }
+#ifndef FFB_HOST_EMULATION
+    if (graphs) {
+      if (b->exec == nullptr) {
+        cudaStream_t cap = nullptr;
+        cudaError_t e = cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking);
+        if (e != cudaSuccess) return e;
+        const char *step = "begin capture";
+        e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+          cudaError_t le = enqueue(*b, cap);
+          step = "end capture";
+          e = cudaStreamEndCapture(cap, &b->graph);
+          if (le != cudaSuccess) {
+            e = le;
+            step = "captured launches";
+          }
+        }
+        if (e == cudaSuccess) {
+          step = "instantiate";
+          e = cudaGraphInstantiate(&b->exec, b->graph, 0);
+        }
+        cudaStreamDestroy(cap);
+        if (e != cudaSuccess) {
+          std::fprintf(stderr, "[flagfft] batch graph %s: %s\n", step, cudaGetErrorString(e));
+          cudaGetLastError();
+          return e;
+        }
+      }
+      return cudaGraphLaunch(b->exec, st);
+    }
+#endif
+    return enqueue(*b, st);
+  }
+
+  std::string describe() const override {
+    std::ostringstream o;
+    o << "  " << groups.size() << " length groups, " << phases.size() << " phases (" << (graphs ? "CUDA graph" : "direct")
+      << ")";
+    for (size_t p = 0; p < phases.size(); ++p) {
+      int persistent = 0, own = 0;
+      for (const PassRef &r : phases[p].passes) (r.kind >= 0 ? persistent : own)++;
+      o << "\n  phase " << p << ": " << persistent << " passes in one persistent launch (" << phases[p].threads
+        << " threads, " << phases[p].smem << " B shared), " << own << " launched on their own";
+    }
+    const size_t show = std::min<size_t>(groups.size(), 16);
+    for (size_t g = 0; g < show; ++g)
+      o << "\n  group " << g << ": n=" << groups[g].n << " x" << groups[g].count << " at element " << groups[g].offset
+        << "\n" << groups[g].prog->describe();
+    if (show < groups.size()) o << "\n  ... " << groups.size() - show << " more groups";
+    return o.str();
+  }
+
+  int launches() const override {
+    int n = 0;
+    for (const Phase &ph : phases) {
+      bool any = false;
+      for (const PassRef &r : ph.passes) {
+        if (r.kind >= 0)
+          any = true;
+        else
+          ++n;
+      }
+      n += any ? 1 : 0;
+    }
+    return n;
+  }
+};
+
+template <typename T>
+std::unique_ptr<BatchProgram> lower_batch_t(const std::vector<BatchGroup> &groups, Planner &planner, bool inverse,
+                                            bool use_graphs) {
+  auto bp = std::make_unique<BatchProgramT<T>>();
+  bp->inverse = inverse;
+  bp->graphs = use_graphs;
+  int64_t offset = 0;
+  for (const BatchGroup &g : groups) {
+    if (g.n <= 0 || g.count <= 0) throw std::runtime_error("batch group with a non-positive length or count");
+    typename BatchProgramT<T>::Group grp;
+    grp.n = g.n;
+    grp.count = g.count;
+    grp.offset = offset;
+    offset += g.n * g.count;
+    NodePtr root = build_raw_root(planner, g.n, nullptr, nullptr);
+    Layout lay;
+    lay.batch = g.count;
+    lay.idist = g.n;
+    lay.odist = g.n;
+    grp.prog = lower_t<T>(root, planner, Transform::C2C, inverse, g.n, lay, false);
+    // in-place passes cannot join a persistent launch: prefer a multi-pass lowering
+    bool in_place = false;
+    for (const auto &ps : grp.prog->passes) {
+      auto *tp = dynamic_cast<const TilePass<T> *>(ps.get());
+      if (tp && !tp->a.pp && !tp->a.regcol) in_place = true;
+    }
+    if (in_place) {
+      t_policy_override = 2;
+      try {
+        grp.prog = lower_t<T>(root, planner, Transform::C2C, inverse, g.n, lay, false);
+      } catch (...) {
+        t_policy_override = -1;
+        throw;
+      }
+      t_policy_override = -1;
+    }
+    bp->groups.push_back(std::move(grp));
+  }
+  size_t nph = 0;
+  for (const auto &g : bp->groups) nph = std::max(nph, g.prog->passes.size());
+  bp->phases.resize(nph);
+  for (size_t gi = 0; gi < bp->groups.size(); ++gi) {
+    const auto &g = bp->groups[gi];
+    for (size_t pi = 0; pi < g.prog->passes.size(); ++pi) {
+      auto &ph = bp->phases[pi];
+      int kind = -1;
+      if (auto *tp = dynamic_cast<const TilePass<T> *>(g.prog->passes[pi].get())) {
+        if (tp->a.regcol) {
+          kind = kBatchRegcol;
+        } else if (tp->a.pp && tp->io == IoKind::C2C) {
+          kind = tp->kind == CoreKind::Dit         ? kBatchPpDit
+                 : tp->kind == CoreKind::Bluestein ? kBatchPpBluestein
+                 : tp->kind == CoreKind::Conv      ? kBatchPpConv
+                                                   : -1;
+        }
+        if (kind >= 0 && kind != kBatchRegcol && tp->smem + kBatchSmemHeader > 232448) kind = -1;
+        if (kind >= 0 && kind != kBatchRegcol) {
+          ph.threads = std::max(ph.threads, tp->a.W * tp->a.tpt);
+          ph.smem = std::max(ph.smem, tp->smem);
+        }
+      }
+      ph.passes.push_back({(int)gi, (int)pi, kind});
+    }
+  }
+  for (auto &ph : bp->phases)
+    if (ph.threads == 0) ph.threads = 128;  // register-column items only
+  return bp;
+}
+
+}  // namespace
+
+std::unique_ptr<BatchProgram> lower_batch(const std::vector<BatchGroup> &groups, Planner &planner, bool is_double,
+                                          bool inverse, bool use_graphs) {
+  return is_double ? lower_batch_t<double>(groups, planner, inverse, use_graphs)
+                   : lower_batch_t<float>(groups, planner, inverse, use_graphs);
 }
 
 }  // namespace ffb

@@ -66,4 +66,25 @@ std::unique_ptr<Program> lower_2d(const NodePtr &root, Planner &planner, bool is
 // Largest core length one CTA can hold.
 int64_t max_onchip_length(bool is_double);
 
+// Batched complex transforms of uneven lengths: `count` transforms of length
+// `n` per group, groups packed back to back (group g starts at element
+// sum_{h<g} count_h n_h of the input and of the output).
+struct BatchGroup {
+  int64_t n = 0;
+  int64_t count = 0;
+};
+
+// One direction of a batch plan: every group's passes gathered into phases
+// (phase p holds the p-th pass of every group) that each run as one
+// persistent launch over a work queue, replayed through a CUDA graph.
+struct BatchProgram {
+  virtual ~BatchProgram() = default;
+  virtual cudaError_t run(const void *in, void *out, cudaStream_t st) = 0;
+  virtual std::string describe() const = 0;
+  virtual int launches() const = 0;
+};
+
+std::unique_ptr<BatchProgram> lower_batch(const std::vector<BatchGroup> &groups, Planner &planner, bool is_double,
+                                          bool inverse, bool use_graphs);
+
 }  // namespace ffb

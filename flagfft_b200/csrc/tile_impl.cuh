@@ -66,16 +66,13 @@ struct DevX {
   int wfast;
   // Runs f(slot, tid-in-slot, threads-per-slot) for this thread's transform.
   // Column tiles put consecutive transforms on consecutive threads.
+  // f has one call site (its barriers must be the same instructions for
+  // every thread of a warp).
   template <class F>
   FFB_HD void per_slot(int W, F f) const {
     const int t = tid();
-    if (wfast) {
-      const int slot = t % W;
-      f(slot, t / W, tpt);
-    } else {
-      const int slot = t / tpt;
-      f(slot, t - slot * tpt, tpt);
-    }
+    const int slot = wfast ? t % W : t / tpt;
+    f(slot, wfast ? t / W : t - slot * tpt, tpt);
   }
 };
 

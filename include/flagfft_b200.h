@@ -40,6 +40,26 @@ FLAGFFT_API const char *flagfftB200PlanJson(flagfftHandle plan);
  * counterpart. */
 FLAGFFT_API int flagfftB200LaunchCount(flagfftHandle plan, int direction);
 
+/* Batch plan over transforms of uneven lengths.  No counterpart in the
+ * reference.
+ *
+ * counts[g] transforms of length lengths[g] for g < ngroups, packed group
+ * after group: group g's transforms start at element sum_{h<g} counts[h] *
+ * lengths[h] of the input and of the output, each transform contiguous.  type
+ * is FLAGFFT_C2C or FLAGFFT_Z2Z; execute with flagfftExecC2C / flagfftExecZ2Z
+ * (either direction; out-of-place, or in place when idata == odata).
+ *
+ * Every group is planned as flagfftPlan1d(lengths[g], type, counts[g]) would
+ * be, but the passes of all groups run together: pass p of every group forms
+ * one phase, and each phase is one persistent launch whose CTAs take work
+ * items (tiles of transforms) from a device queue, longest first.  The
+ * launches of an Exec are captured into a CUDA graph on the first Exec with a
+ * given (idata, odata) pair and replayed afterwards (the plan keeps up to four
+ * such bindings; FLAGFFT_BATCH_GRAPH=0 launches them directly).  Like other
+ * plans, one batch plan must not run on two streams at once. */
+FLAGFFT_API flagfftResult flagfftB200PlanBatch(flagfftHandle *plan, int ngroups, const int *lengths, const int *counts,
+                                              flagfftType type);
+
 /* Batched complex64 FFT of power-of-two length n (8192 <= n <= 2^24) that
  * allocates no memory.  No counterpart in the reference.
  *

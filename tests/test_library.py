@@ -83,3 +83,17 @@ def test_exec_on_null_plan(ffb):
 
 def test_version_string(ffb):
     assert "sm_100a" in ffb.version()
+
+
+def test_batch_plan_argument_checks(ffb):
+    """flagfftB200PlanBatch rejects bad arguments before touching a device."""
+    import ctypes as C
+    h = C.c_void_p(7)
+    ints = lambda *v: (C.c_int * len(v))(*v)  # noqa: E731
+    L = ffb.LIB
+    assert L.flagfftB200PlanBatch(None, 1, ints(16), ints(1), ffb.C2C) == 4
+    assert L.flagfftB200PlanBatch(C.byref(h), 0, ints(16), ints(1), ffb.C2C) == 4 and h.value is None
+    assert L.flagfftB200PlanBatch(C.byref(h), 1, None, ints(1), ffb.C2C) == 4
+    assert L.flagfftB200PlanBatch(C.byref(h), 1, ints(16), ints(1), ffb.R2C) == 3
+    assert L.flagfftB200PlanBatch(C.byref(h), 2, ints(16, 0), ints(1, 1), ffb.C2C) == 8
+    assert L.flagfftB200PlanBatch(C.byref(h), 2, ints(16, 32), ints(1, 0), ffb.Z2Z) == 4
