@@ -257,11 +257,12 @@ static std::vector<int> flatten(const NodePtr &node) {
     return r;
   }
   if (node->kind == NodeKind::FourStep) {
-    auto a = flatten(node->row);
-    auto b = flatten(node->col);
+    const auto a = flatten(node->row);
+    const auto b = flatten(node->col);
     if (a.empty() || b.empty()) return {};
-    a.insert(a.end(), b.begin(), b.end());
-    return a;
+    std::vector<int> r(a);
+    for (int v : b) r.push_back(v);
+    return r;
   }
   return {};
 }
@@ -376,6 +377,38 @@ int64_t choose_split_conv(int64_t n, int64_t maxL, int64_t *n1_out, std::vector<
   }
   return best_m;
 }
+
+// The executor's own radix chain for length n (false when n has a prime
+// factor above 19).
+bool radix_chain(int64_t n, std::vector<int> *radices) {
+  std::unordered_map<int64_t, std::pair<double, int>> memo;
+  return chain_cost(n, radices, memo) < 1e29;
+}
+
+// The executor's own four-step split n = n1 x n2 (both chains, both on chip)
+// with the least n x (chain cost of n1 + chain cost of n2); false if none.
+bool own_four_step(int64_t n, int64_t maxL, int64_t *n1_out, std::vector<int> *r1, std::vector<int> *r2) {
+  std::unordered_map<int64_t, std::pair<double, int>> memo;
+  double best = 1e29;
+  int64_t best_n1 = 0;
+  for (int64_t a = 2; a * a <= n; ++a) {
+    if (n % a) continue;
+    for (int64_t n1 : {a, n / a}) {
+      const int64_t n2 = n / n1;
+      if (n1 > maxL || n2 > maxL) continue;
+      const double c = chain_cost(n1, nullptr, memo) + chain_cost(n2, nullptr, memo);
+      if (c < best) {
+        best = c;
+        best_n1 = n1;
+      }
+    }
+  }
+  if (!best_n1) return false;
+  *n1_out = best_n1;
+  chain_cost(best_n1, r1, memo);
+  chain_cost(n / best_n1, r2, memo);
+  return true;
+}
 }  // namespace
 
 static Core make_dit_core(int64_t L, const std::vector<int> &r) {
@@ -455,6 +488,13 @@ class Builder {
       spec = {CoreKind::Dit, node->length, node->length, r, node};
       return true;
     }
+    // a tree whose nodes do not flatten into one radix chain (a four-step
+    // over Bluestein / Rader children): the executor's own chain when the
+    // length has one and fits
+    if (node->kind == NodeKind::FourStep && node->length <= maxL && radix_chain(node->length, &r)) {
+      spec = {CoreKind::Dit, node->length, node->length, r, node};
+      return true;
+    }
     if (node->kind == NodeKind::Bluestein) {
       std::vector<int> rc;
       const int64_t m = choose_conv_length(node->length, maxL, &rc);
@@ -465,8 +505,17 @@ class Builder {
     }
     if (node->kind == NodeKind::Rader) {
       auto rc = flatten(node->child);
+      if (rc.empty()) radix_chain(node->length - 1, &rc);  // the child tree is not one chain
       if (!rc.empty() && node->length - 1 <= maxL) {
         spec = {CoreKind::Rader, node->length, node->length - 1, rc, node};
+        return true;
+      }
+      // p - 1 without a radix chain (a prime factor above 19): the same DFT
+      // through a Bluestein convolution
+      std::vector<int> bc;
+      const int64_t m = rc.empty() ? choose_conv_length(node->length, maxL, &bc) : 0;
+      if (m) {
+        spec = {CoreKind::Bluestein, node->length, m, bc, node};
         return true;
       }
     }
@@ -789,10 +838,21 @@ void lower_c2c(Builder<T> &bld, Program &prog, const NodePtr &root, bool inverse
     return;
   }
   if (batch > 65535) throw std::runtime_error("multi-pass batch above 65535");
-  if (root->kind == NodeKind::FourStep) {
-    CoreSpec sa, sb;
-    if (bld.core_for(root->row, sa) && bld.core_for(root->col, sb)) {
-      const int64_t n1 = root->n1, n2 = root->n2;
+  CoreSpec sa, sb;
+  int64_t f1 = 0;
+  if (root->kind == NodeKind::FourStep && bld.core_for(root->row, sa) && bld.core_for(root->col, sb)) {
+    f1 = root->n1;
+  } else if (root->kind != NodeKind::Bluestein && root->kind != NodeKind::Rader) {
+    // the executor's own split when the tree's children cannot run as cores
+    std::vector<int> r1, r2;
+    if (own_four_step(n, max_onchip_length(sizeof(T) == 8), &f1, &r1, &r2)) {
+      sa = {CoreKind::Dit, f1, f1, r1, nullptr};
+      sb = {CoreKind::Dit, n / f1, n / f1, r2, nullptr};
+    }
+  }
+  if (f1) {
+    {
+      const int64_t n1 = f1, n2 = n / f1;
       prog.scratch0 = std::make_shared<DevMem>((size_t)(batch * n) * sizeof(cpx<T>));
       // pass A: columns j2 (stride n2) of length n1, x W_n^{j2 k1}, rows Y[j2][k1]
       auto *pa = bld.add_pass(sa, IoKind::C2C, inverse, batch, n2, idist, 1, n2, n, n1, 1, src, Buf::Scratch0, n1);
@@ -802,8 +862,11 @@ void lower_c2c(Builder<T> &bld, Program &prog, const NodePtr &root, bool inverse
       return;
     }
   }
-  if (root->kind == NodeKind::Bluestein) {
-    // Convolution too long for one CTA: three passes through an M-point
+  {
+    // A Bluestein node whose convolution is too long for one CTA, or any
+    // length the lowerings above cannot run (a Rader prime too long for one
+    // CTA, a length whose factors are neither chains nor a split): three
+    // passes through an M-point
     // workspace, M = n1 x n2 chosen by the executor (n1 one codelet, n2 on
     // chip), with the chirps, the kernel product and both four-step twiddles
     // fused (src/exec/raw_nodes.cpp:153-204 runs the same chain as 7 launches).

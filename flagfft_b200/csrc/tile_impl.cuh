@@ -486,9 +486,10 @@ FFB_HD void tile_body_pp(const TileArgs<T> &a, long long bx, long long by, cpx<T
       }
       return {post_twiddle(v, g0 + wc, k), at};
     } else if constexpr (KIND == 1) {
-      return {cmul(v, ldg_c(a.chirp + k)), at};
+      return {post_twiddle(cmul(v, ldg_c(a.chirp + k)), g0 + wc, k), at};
     } else if constexpr (KIND == 2) {
-      return {bw[2 * Lq] + v, w < wlive ? w * og + ldg_v(a.perm_out + k) * ok : -1};
+      const int ko = ldg_v(a.perm_out + k);  // frequency index of output k
+      return {post_twiddle(bw[2 * Lq] + v, g0 + wc, ko), w < wlive ? w * og + ko * ok : -1};
     } else {
       return {post_twiddle(v, g0 + wc, k), at};
     }

@@ -18,6 +18,10 @@ pytestmark = pytest.mark.gpu
 CT = [16, 64, 81, 243, 256, 361, 512, 2048, 4096, 8192, 16384]
 BS = [23, 67, 997, 1009]
 EXTRA = [2, 3, 5, 7, 11, 13, 17, 19, 6, 10, 12, 15, 1701, 2023, 10007, 20020, 65536, 30030]
+# four-step plans whose passes are fused Bluestein / Rader cores (the four-step
+# twiddle applied in their stores), and a Rader prime whose p - 1 has a prime
+# factor above 19 (2099: p - 1 = 2 x 1049, run through a Bluestein core)
+COMPOSITE = [11573, 19549, 32980, 61423, 2099]
 
 
 def _ref_plan(plans, n, double):
@@ -56,10 +60,12 @@ def _check(err, ftype, n, est=None):
 
 
 @pytest.mark.parametrize("double", [False, True], ids=["C2C", "Z2Z"])
-@pytest.mark.parametrize("n", CT + BS + EXTRA)
+@pytest.mark.parametrize("n", CT + BS + EXTRA + COMPOSITE)
 def test_c2c_z2z_vs_oracle(ffb, torch_cuda, plans, n, double):
     torch = torch_cuda
     batch = 4 if n <= 20020 else 2
+    if n in COMPOSITE:
+        batch = 2
     ftype = O.Z2Z if double else O.C2C
     x = O.random_complex(n * batch, O.accuracy_seed(ftype, n, batch), double).reshape(batch, n)
     plan = _ref_plan(plans, n, double)
