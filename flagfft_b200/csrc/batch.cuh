@@ -4,7 +4,7 @@
 // the same tile bodies as the per-plan kernels, and loops until the queue is
 // empty, so lengths of very different cost share the GPU without a launch per
 // length.  An item is (index of its pass's TileArgs, tile index):
-//   ping-pong passes (kinds 0, 1, 3 = Dit, Bluestein, Conv): tile =
+//   ping-pong passes (kinds 0-3 = Dit, Bluestein, Rader, Conv): tile =
 //     by * ceil(G / W) + bx, the CTA tile of the per-plan launch;
 //   register-column passes (kind 8): tile = by * ceil(G / blockDim) + chunk,
 //     blockDim consecutive transforms, one per thread.
@@ -19,7 +19,7 @@
 
 namespace ffb {
 
-enum BatchKind : int { kBatchPpDit = 0, kBatchPpBluestein = 1, kBatchPpConv = 3, kBatchRegcol = 8 };
+enum BatchKind : int { kBatchPpDit = 0, kBatchPpBluestein = 1, kBatchPpRader = 2, kBatchPpConv = 3, kBatchRegcol = 8 };
 
 struct BatchItem {
   int args;
@@ -104,6 +104,8 @@ FFB_HD void run_item(const TileArgs<T> &a, int kind, int tile, cpx<T> *sm, const
       tile::tile_body_pp<T, 0, false>(a, bx, by, sm, x);
   } else if (kind == kBatchPpBluestein) {
     tile::tile_body_pp<T, 1, false>(a, bx, by, sm, x);
+  } else if (kind == kBatchPpRader) {
+    tile::tile_body_pp<T, 2, false>(a, bx, by, sm, x);
   } else {
     tile::tile_body_pp<T, 3, false>(a, bx, by, sm, x);
   }

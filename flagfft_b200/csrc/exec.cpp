@@ -824,13 +824,16 @@ void lower_c2c(Builder<T> &bld, Program &prog, const NodePtr &root, bool inverse
   const bool onchip = bld.core_for(root, spec);
   CoreSpec ca, cb;
   const bool mp_four = root->kind == NodeKind::FourStep && bld.core_for(root->row, ca) && bld.core_for(root->col, cb);
-  const bool mp_blue = root->kind == NodeKind::Bluestein;  // three-pass chain at an executor-chosen split
+  // three-pass Bluestein chain at an executor-chosen split (also the
+  // multi-pass lowering of a Rader prime)
+  const bool mp_blue = root->kind == NodeKind::Bluestein || root->kind == NodeKind::Rader;
   const int policy = onchip_policy();
   // A Bluestein convolution that fits one CTA only in place (not as two
   // ping-pong buffers) runs faster as the three-pass chain: its 1-CTA-per-SM
   // in-place pass is latency-bound (C2C N=10007 on B200: 440 us fused vs
   // 414 us in three passes).
-  const bool blue_in_place = onchip && spec.kind == CoreKind::Bluestein && !Builder<T>::pp_fits(spec.L);
+  const bool blue_in_place = onchip && (spec.kind == CoreKind::Bluestein || spec.kind == CoreKind::Rader) &&
+                             !Builder<T>::pp_fits(spec.L);
   const bool use_onchip =
       onchip && (policy == 1 || ((policy != 2 || !(mp_four || mp_blue)) && !blue_in_place));
   if (use_onchip) {
@@ -1025,6 +1028,17 @@ std::unique_ptr<Program> lower_2d(const NodePtr &root, Planner &planner, bool is
 // ---------------------------------------------------------------------------
 namespace {
 
+// Shared-memory classes of the persistent launches of a phase: items are
+// grouped by the shared memory their tiles need, so small items get many CTAs
+// per SM instead of the one a 227 KB item allows; the classes of a phase run
+// concurrently on their own streams.  Class 4 holds register-column items.
+constexpr int kBatchClasses = 5;
+static int batch_class(size_t smem, bool regcol) {
+  if (regcol) return 4;
+  const size_t s = smem + kBatchSmemHeader;
+  return s <= 32 * 1024 ? 0 : s <= 76 * 1024 ? 1 : s <= 113 * 1024 ? 2 : 3;
+}
+
 template <typename T>
 struct BatchProgramT final : BatchProgram {
   struct Group {
@@ -1033,19 +1047,23 @@ struct BatchProgramT final : BatchProgram {
   };
   struct PassRef {
     int group, pass, kind;  // kind: a BatchKind, or -1 for a pass launched on its own
+    int cls;                // shared-memory class of a persistent pass
   };
-  struct Phase {
-    std::vector<PassRef> passes;
+  struct Launch {  // one persistent launch: the passes of one class of one phase
     int threads = 0;
     size_t smem = 0;
   };
+  struct Phase {
+    std::vector<PassRef> passes;
+    Launch cls[kBatchClasses];
+  };
   // Device state for one (input, output) pair: resolved pass arguments, the
-  // work items of every phase, the queue counters and the captured graph.
+  // work items of every launch, the queue counters and the captured graph.
   struct Bound {
     const void *in = nullptr;
     void *out = nullptr;
     DevPtr args, kinds, items, counters;
-    std::vector<int> first_item, nitems, ctas;
+    std::vector<int> first_item, nitems, ctas;  // per (phase, class)
     std::vector<TileArgs<T>> host_args;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -1062,8 +1080,23 @@ struct BatchProgramT final : BatchProgram {
   std::vector<Phase> phases;
   std::vector<std::unique_ptr<Bound>> bound;  // most recent last
   std::mutex mu;
+#ifndef FFB_HOST_EMULATION
+  cudaStream_t side[kBatchClasses] = {};
+  cudaEvent_t fork = nullptr, join[kBatchClasses] = {};
+#endif
 
   static constexpr size_t kMaxBound = 4;
+
+  ~BatchProgramT() override {
+    bound.clear();
+#ifndef FFB_HOST_EMULATION
+    for (int c = 0; c < kBatchClasses; ++c) {
+      if (side[c]) cudaStreamDestroy(side[c]);
+      if (join[c]) cudaEventDestroy(join[c]);
+    }
+    if (fork) cudaEventDestroy(fork);
+#endif
+  }
 
   const TilePass<T> *tile_pass(const PassRef &r) const {
     return dynamic_cast<const TilePass<T> *>(groups[(size_t)r.group].prog->passes[(size_t)r.pass].get());
@@ -1076,12 +1109,11 @@ struct BatchProgramT final : BatchProgram {
     std::vector<int> kinds;
     std::vector<BatchItem> items;
     for (const Phase &ph : phases) {
-      b->first_item.push_back((int)items.size());
       struct Cost {
         double c;
         int args, tiles;
       };
-      std::vector<Cost> order;
+      std::vector<Cost> order[kBatchClasses];
       for (const PassRef &r : ph.passes) {
         if (r.kind < 0) continue;
         const Group &g = groups[(size_t)r.group];
@@ -1096,17 +1128,22 @@ struct BatchProgramT final : BatchProgram {
         const int idx = (int)b->host_args.size();
         b->host_args.push_back(a);
         kinds.push_back(r.kind);
-        const int width = r.kind == kBatchRegcol ? ph.threads : a.W;
+        const int width = r.kind == kBatchRegcol ? std::max(ph.cls[r.cls].threads, 32) : a.W;
         const int tiles = (int)(((int64_t)a.G + width - 1) / width * a.nbatch);
         // longest items first: per-tile work ~ transforms x length x stages
         const double c = r.kind == kBatchRegcol ? 0.0 : (double)a.W * a.core.L * (a.core.nst + a.core2.nst);
-        order.push_back({c, idx, tiles});
+        order[r.cls].push_back({c, idx, tiles});
       }
-      std::stable_sort(order.begin(), order.end(), [](const Cost &x, const Cost &y) { return x.c > y.c; });
-      for (const Cost &o : order)
-        for (int t = 0; t < o.tiles; ++t) items.push_back({o.args, t});
-      b->nitems.push_back((int)items.size() - b->first_item.back());
-      b->ctas.push_back(std::max(1, batch_resident_ctas<T>(std::max(ph.threads, 32), ph.smem)));
+      for (int c = 0; c < kBatchClasses; ++c) {
+        std::stable_sort(order[c].begin(), order[c].end(), [](const Cost &x, const Cost &y) { return x.c > y.c; });
+        b->first_item.push_back((int)items.size());
+        for (const Cost &o : order[c])
+          for (int t = 0; t < o.tiles; ++t) items.push_back({o.args, t});
+        b->nitems.push_back((int)items.size() - b->first_item.back());
+        b->ctas.push_back(std::max(1, b->nitems.back() ? batch_resident_ctas<T>(std::max(ph.cls[c].threads, 32),
+                                                                                ph.cls[c].smem)
+                                                       : 1));
+      }
     }
     // (a phase of passes that all launch on their own has no items; keep the
     // uploads non-empty)
@@ -1117,15 +1154,53 @@ struct BatchProgramT final : BatchProgram {
     b->args = upload(args_up.data(), args_up.size() * sizeof(TileArgs<T>));
     b->kinds = upload(kinds.data(), kinds.size() * sizeof(int));
     b->items = upload(items.data(), items.size() * sizeof(BatchItem));
-    std::vector<int> zeros(phases.size() + 1, 0);
+    std::vector<int> zeros(phases.size() * kBatchClasses + 1, 0);
     b->counters = upload(zeros.data(), zeros.size() * sizeof(int));
     return b;
   }
 
-  // The launches of every phase, in order, on stream st.
+  cudaError_t launch_class(const Bound &b, size_t p, int c, cudaStream_t st) {
+    const size_t k = p * kBatchClasses + (size_t)c;
+    if (b.nitems[k] == 0) return cudaSuccess;
+    const Launch &L = phases[p].cls[c];
+    int *counter = reinterpret_cast<int *>(b.counters->ptr) + k;
+#ifndef FFB_HOST_EMULATION
+    cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(int), st);
+    if (e != cudaSuccess) return e;
+#else
+    cudaError_t e = cudaSuccess;
+    *counter = 0;
+#endif
+    e = launch_batch<T>(reinterpret_cast<const TileArgs<T> *>(b.args->ptr), reinterpret_cast<const int *>(b.kinds->ptr),
+                        reinterpret_cast<const BatchItem *>(b.items->ptr) + b.first_item[k], b.nitems[k], counter,
+                        std::max(L.threads, 32), L.smem, b.ctas[k], st);
+    if (e != cudaSuccess)
+      std::fprintf(stderr, "[flagfft] batch phase %zu class %d launch (%d CTAs x %d threads, %zu B shared): %s\n", p, c,
+                   b.ctas[k], std::max(L.threads, 32), L.smem, cudaGetErrorString(e));
+    return e;
+  }
+
+  // The launches of every phase on stream st: the persistent launches of a
+  // phase's classes run concurrently on side streams (forked from and joined
+  // back into st), the passes launched on their own run on st meanwhile.
   cudaError_t enqueue(const Bound &b, cudaStream_t st) {
     for (size_t p = 0; p < phases.size(); ++p) {
       const Phase &ph = phases[p];
+#ifndef FFB_HOST_EMULATION
+      cudaError_t e = cudaEventRecord(fork, st);
+      if (e != cudaSuccess) return e;
+      for (int c = 0; c < kBatchClasses; ++c) {
+        if (b.nitems[p * kBatchClasses + (size_t)c] == 0) continue;
+        if ((e = cudaStreamWaitEvent(side[c], fork, 0)) != cudaSuccess) return e;
+        if ((e = launch_class(b, p, c, side[c])) != cudaSuccess) return e;
+        if ((e = cudaEventRecord(join[c], side[c])) != cudaSuccess) return e;
+      }
+#else
+      for (int c = 0; c < kBatchClasses; ++c) {
+        cudaError_t e = launch_class(b, p, c, st);
+        if (e != cudaSuccess) return e;
+      }
+#endif
       for (const PassRef &r : ph.passes) {
         if (r.kind >= 0) continue;
         const Group &g = groups[(size_t)r.group];
@@ -1133,36 +1208,41 @@ struct BatchProgramT final : BatchProgram {
         cpx<T> *gout = reinterpret_cast<cpx<T> *>(b.out) + g.offset;
         void *s0 = g.prog->scratch0 ? g.prog->scratch0->ptr : nullptr;
         void *s1 = g.prog->scratch1 ? g.prog->scratch1->ptr : nullptr;
-        cudaError_t e = g.prog->passes[(size_t)r.pass]->run(gin, gout, s0, s1, st);
-        if (e != cudaSuccess) {
+        cudaError_t e2 = g.prog->passes[(size_t)r.pass]->run(gin, gout, s0, s1, st);
+        if (e2 != cudaSuccess) {
           std::fprintf(stderr, "[flagfft] batch phase %zu: own launch of group %d pass %d: %s\n", p, r.group, r.pass,
-                       cudaGetErrorString(e));
-          return e;
+                       cudaGetErrorString(e2));
+          return e2;
         }
       }
-      if (b.nitems[p] == 0) continue;
-      int *counter = reinterpret_cast<int *>(b.counters->ptr) + p;
 #ifndef FFB_HOST_EMULATION
-      cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(int), st);
-      if (e != cudaSuccess) return e;
-#else
-      cudaError_t e = cudaSuccess;
-      *counter = 0;
-#endif
-      e = launch_batch<T>(reinterpret_cast<const TileArgs<T> *>(b.args->ptr), reinterpret_cast<const int *>(b.kinds->ptr),
-                          reinterpret_cast<const BatchItem *>(b.items->ptr) + b.first_item[p], b.nitems[p], counter,
-                          std::max(ph.threads, 32), ph.smem, b.ctas[p], st);
-      if (e != cudaSuccess) {
-        std::fprintf(stderr, "[flagfft] batch phase %zu launch (%d CTAs x %d threads, %zu B shared): %s\n", p,
-                     b.ctas[p], std::max(ph.threads, 32), ph.smem, cudaGetErrorString(e));
-        return e;
+      for (int c = 0; c < kBatchClasses; ++c) {
+        if (b.nitems[p * kBatchClasses + (size_t)c] == 0) continue;
+        if ((e = cudaStreamWaitEvent(st, join[c], 0)) != cudaSuccess) return e;
       }
+#endif
     }
     return cudaSuccess;
   }
 
+  cudaError_t ensure_streams() {
+#ifndef FFB_HOST_EMULATION
+    if (fork) return cudaSuccess;
+    cudaError_t e = cudaEventCreateWithFlags(&fork, cudaEventDisableTiming);
+    for (int c = 0; c < kBatchClasses && e == cudaSuccess; ++c) {
+      e = cudaStreamCreateWithFlags(&side[c], cudaStreamNonBlocking);
+      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&join[c], cudaEventDisableTiming);
+    }
+    return e;
+#else
+    return cudaSuccess;
+#endif
+  }
+
   cudaError_t run(const void *in, void *out, cudaStream_t st) override {
     std::lock_guard<std::mutex> lock(mu);
+    cudaError_t se = ensure_streams();
+    if (se != cudaSuccess) return se;
     Bound *b = nullptr;
     for (size_t i = 0; i < bound.size(); ++i)
       if (bound[i]->in == in && bound[i]->out == out) {
@@ -1221,10 +1301,19 @@ struct BatchProgramT final : BatchProgram {
     o << "  " << groups.size() << " length groups, " << phases.size() << " phases (" << (graphs ? "CUDA graph" : "direct")
       << ")";
     for (size_t p = 0; p < phases.size(); ++p) {
-      int persistent = 0, own = 0;
-      for (const PassRef &r : phases[p].passes) (r.kind >= 0 ? persistent : own)++;
-      o << "\n  phase " << p << ": " << persistent << " passes in one persistent launch (" << phases[p].threads
-        << " threads, " << phases[p].smem << " B shared), " << own << " launched on their own";
+      int persistent[kBatchClasses] = {}, own = 0;
+      for (const PassRef &r : phases[p].passes) {
+        if (r.kind >= 0)
+          persistent[r.cls]++;
+        else
+          ++own;
+      }
+      o << "\n  phase " << p << ":";
+      for (int c = 0; c < kBatchClasses; ++c)
+        if (persistent[c])
+          o << " [" << persistent[c] << " passes, one persistent launch of " << std::max(phases[p].cls[c].threads, 32)
+            << " threads, " << phases[p].cls[c].smem << " B shared]";
+      o << " " << own << " launched on their own";
     }
     const size_t show = std::min<size_t>(groups.size(), 16);
     for (size_t g = 0; g < show; ++g)
@@ -1237,14 +1326,14 @@ struct BatchProgramT final : BatchProgram {
   int launches() const override {
     int n = 0;
     for (const Phase &ph : phases) {
-      bool any = false;
+      bool any[kBatchClasses] = {};
       for (const PassRef &r : ph.passes) {
         if (r.kind >= 0)
-          any = true;
+          any[r.cls] = true;
         else
           ++n;
       }
-      n += any ? 1 : 0;
+      for (bool a : any) n += a ? 1 : 0;
     }
     return n;
   }
@@ -1295,27 +1384,27 @@ std::unique_ptr<BatchProgram> lower_batch_t(const std::vector<BatchGroup> &group
     const auto &g = bp->groups[gi];
     for (size_t pi = 0; pi < g.prog->passes.size(); ++pi) {
       auto &ph = bp->phases[pi];
-      int kind = -1;
+      int kind = -1, cls = 0;
       if (auto *tp = dynamic_cast<const TilePass<T> *>(g.prog->passes[pi].get())) {
         if (tp->a.regcol) {
           kind = kBatchRegcol;
         } else if (tp->a.pp && tp->io == IoKind::C2C) {
           kind = tp->kind == CoreKind::Dit         ? kBatchPpDit
                  : tp->kind == CoreKind::Bluestein ? kBatchPpBluestein
-                 : tp->kind == CoreKind::Conv      ? kBatchPpConv
-                                                   : -1;
+                 : tp->kind == CoreKind::Rader     ? kBatchPpRader
+                                                   : kBatchPpConv;
         }
         if (kind >= 0 && kind != kBatchRegcol && tp->smem + kBatchSmemHeader > 232448) kind = -1;
-        if (kind >= 0 && kind != kBatchRegcol) {
-          ph.threads = std::max(ph.threads, tp->a.W * tp->a.tpt);
-          ph.smem = std::max(ph.smem, tp->smem);
+        if (kind >= 0) {
+          cls = batch_class(tp->smem, kind == kBatchRegcol);
+          auto &L = ph.cls[cls];
+          L.threads = std::max(L.threads, kind == kBatchRegcol ? 128 : tp->a.W * tp->a.tpt);
+          L.smem = std::max(L.smem, kind == kBatchRegcol ? (size_t)0 : tp->smem);
         }
       }
-      ph.passes.push_back({(int)gi, (int)pi, kind});
+      ph.passes.push_back({(int)gi, (int)pi, kind, cls});
     }
   }
-  for (auto &ph : bp->phases)
-    if (ph.threads == 0) ph.threads = 128;  // register-column items only
   return bp;
 }
 
