@@ -1033,9 +1033,14 @@ namespace {
 // per SM instead of the one a 227 KB item allows; the classes of a phase run
 // concurrently on their own streams.  Class 4 holds register-column items.
 constexpr int kBatchClasses = 5;
-static int batch_class(size_t smem, bool regcol) {
+// Passes wider than kBatchWidth threads, or with tiles above 113 KB, share
+// class 3 (one 512-thread CTA per SM); the others run kBatchWidth-thread CTAs,
+// two or more per SM.
+constexpr int kBatchWidth = 256;
+static int batch_class(size_t smem, int threads, bool regcol) {
   if (regcol) return 4;
   const size_t s = smem + kBatchSmemHeader;
+  if (threads > kBatchWidth) return 3;
   return s <= 32 * 1024 ? 0 : s <= 76 * 1024 ? 1 : s <= 113 * 1024 ? 2 : 3;
 }
 
@@ -1377,6 +1382,26 @@ std::unique_ptr<BatchProgram> lower_batch_t(const std::vector<BatchGroup> &group
     }
     bp->groups.push_back(std::move(grp));
   }
+  // Retile ping-pong passes for the shared launches: as many transforms per
+  // tile as fill kBatchWidth threads within ~110 KB of shared memory (a
+  // standalone plan of a small batch keeps its tiles narrow to spread them
+  // over the SMs; in a batch the other groups do that).
+  for (auto &g : bp->groups)
+    for (auto &ps : g.prog->passes) {
+      auto *tp = dynamic_cast<TilePass<T> *>(ps.get());
+      if (!tp || !tp->a.pp || tp->a.regcol || tp->a.tpt > kBatchWidth) continue;
+      TileArgs<T> &a = tp->a;
+      const size_t per = tp->smem / (size_t)a.W;
+      int64_t W = std::min<int64_t>({(int64_t)(kBatchWidth / a.tpt), (int64_t)a.G,
+                                     (int64_t)std::max<size_t>(1, 110 * 1024 / per)});
+      W = std::max<int64_t>(W, a.W);
+      if (W * std::llabs(a.ig) + a.core.L * std::llabs(a.ii) >= (1ll << 31) ||
+          W * std::llabs(a.og) + a.core.L * std::llabs(a.ok) >= (1ll << 31))
+        continue;
+      a.W = (int)W;
+      a.wdiv = make_fastdiv((uint32_t)W);
+      tp->smem = per * (size_t)W;
+    }
   size_t nph = 0;
   for (const auto &g : bp->groups) nph = std::max(nph, g.prog->passes.size());
   bp->phases.resize(nph);
@@ -1396,7 +1421,7 @@ std::unique_ptr<BatchProgram> lower_batch_t(const std::vector<BatchGroup> &group
         }
         if (kind >= 0 && kind != kBatchRegcol && tp->smem + kBatchSmemHeader > 232448) kind = -1;
         if (kind >= 0) {
-          cls = batch_class(tp->smem, kind == kBatchRegcol);
+          cls = batch_class(tp->smem, tp->a.W * tp->a.tpt, kind == kBatchRegcol);
           auto &L = ph.cls[cls];
           L.threads = std::max(L.threads, kind == kBatchRegcol ? 128 : tp->a.W * tp->a.tpt);
           L.smem = std::max(L.smem, kind == kBatchRegcol ? (size_t)0 : tp->smem);
