@@ -17,7 +17,7 @@ import os
 from pathlib import Path
 
 __all__ = [
-    "FlagFFTError", "Plan", "plan1d", "plan2d", "plan3d", "plan_many", "plan_batch", "planner_tree", "library_path",
+    "FlagFFTError", "Plan", "plan1d", "plan2d", "plan3d", "plan_many", "plan_batch", "Server", "planner_tree", "library_path",
     "C2C", "Z2Z", "R2C", "D2Z", "C2R", "Z2D", "FORWARD", "INVERSE", "STATUS",
 ]
 
@@ -72,6 +72,13 @@ def _load():
         "flagfftB200PlanJson": (cp, [H]),
         "flagfftB200LaunchCount": (i, [H, i]),
         "flagfftB200PlanBatch": (i, [PH, i, ip, ip, i]),
+        "flagfftB200ServerCreate": (i, [PH, ctypes.c_longlong, i]),
+        "flagfftB200ServerPrepare": (i, [H, i, i, i]),
+        "flagfftB200ServerSubmit": (i, [H, i, i, i, i, vp, vp, ctypes.POINTER(ctypes.c_longlong)]),
+        "flagfftB200ServerWait": (i, [H, ctypes.c_longlong, ctypes.POINTER(ctypes.c_double)]),
+        "flagfftB200ServerStats": (i, [H, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong),
+                                       ctypes.POINTER(ctypes.c_longlong)]),
+        "flagfftB200ServerDestroy": (i, [H]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name)
@@ -249,6 +256,48 @@ def plan_batch(lengths, counts, ftype: int = C2C) -> Plan:
                                        ftype), "flagfftB200PlanBatch")
     total = sum(l * c for l, c in zip(lengths, counts))
     return Plan(h.value, ftype, (total,), 1)
+
+
+class Server:
+    """Request server (flagfftB200ServerCreate): continuous batching of
+    transforms of mixed type, length and batch on device buffers."""
+
+    def __init__(self, hbm_budget_bytes: int = 40 << 30, max_ticks: int = 4):
+        h = ctypes.c_void_p(0)
+        _check(_lib().flagfftB200ServerCreate(ctypes.byref(h), hbm_budget_bytes, max_ticks), "flagfftB200ServerCreate")
+        self._h = h
+
+    def prepare(self, ftype: int, n: int, direction: int = FORWARD) -> None:
+        _check(_lib().flagfftB200ServerPrepare(self._h, ftype, n, direction), "flagfftB200ServerPrepare")
+
+    def submit(self, ftype: int, n: int, batch: int, idata, odata, direction: int = FORWARD) -> int:
+        t = ctypes.c_longlong(0)
+        _check(_lib().flagfftB200ServerSubmit(self._h, ftype, n, batch, direction, ctypes.c_void_p(_ptr(idata)),
+                                              ctypes.c_void_p(_ptr(odata)), ctypes.byref(t)), "flagfftB200ServerSubmit")
+        return t.value
+
+    def wait(self, ticket: int) -> float:
+        """Blocks until the request finished; returns its latency in ms."""
+        ms = ctypes.c_double(0)
+        _check(_lib().flagfftB200ServerWait(self._h, ticket, ctypes.byref(ms)), "flagfftB200ServerWait")
+        return ms.value
+
+    def stats(self) -> dict:
+        c, t, u = ctypes.c_longlong(), ctypes.c_longlong(), ctypes.c_longlong()
+        _check(_lib().flagfftB200ServerStats(self._h, ctypes.byref(c), ctypes.byref(t), ctypes.byref(u)),
+               "flagfftB200ServerStats")
+        return {"completed": c.value, "ticks": t.value, "bytes_in_use": u.value}
+
+    def close(self) -> None:
+        if self._h:
+            _lib().flagfftB200ServerDestroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
 
 
 def planner_tree(n: int, is_double: bool = False, smem_bytes: int = 0) -> dict:

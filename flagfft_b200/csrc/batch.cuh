@@ -135,6 +135,22 @@ __global__ void __launch_bounds__(tile::TileBounds<T>::kMaxThreads)
 
 }  // namespace batch
 
+// Shared-memory classes of the persistent launches of a phase: items are
+// grouped by the shared memory their tiles need, so small items get many CTAs
+// per SM instead of the one a 227 KB item allows; the classes of a phase run
+// concurrently on their own streams.  Class 4 holds register-column items.
+constexpr int kBatchClasses = 5;
+// Passes wider than kBatchWidth threads, or with tiles above 113 KB, share
+// class 3 (one 512-thread CTA per SM); the others run kBatchWidth-thread CTAs,
+// two or more per SM.
+constexpr int kBatchWidth = 256;
+inline int batch_class(size_t smem, int threads, bool regcol) {
+  if (regcol) return 4;
+  const size_t s = smem + kBatchSmemHeader;
+  if (threads > kBatchWidth) return 3;
+  return s <= 32 * 1024 ? 0 : s <= 76 * 1024 ? 1 : s <= 113 * 1024 ? 2 : 3;
+}
+
 // Launch of one phase: `ctas` persistent CTAs of `threads` threads with
 // `smem` bytes of dynamic shared memory for the items' tiles (the launch adds
 // kBatchSmemHeader) over `nitems` items; *next must be 0.

@@ -32,6 +32,7 @@
 #include <stdexcept>
 
 #include "batch.cuh"
+#include "exec_internal.hpp"
 #include "tables.hpp"
 
 namespace ffb {
@@ -140,104 +141,6 @@ int64_t max_onchip_length(bool is_double) {
 }
 
 namespace {
-
-const char *buf_name(Buf b) {
-  switch (b) {
-    case Buf::In: return "in";
-    case Buf::Out: return "out";
-    case Buf::Scratch0: return "ws0";
-    case Buf::Scratch1: return "ws1";
-  }
-  return "?";
-}
-
-const char *kind_name(CoreKind k) {
-  switch (k) {
-    case CoreKind::Dit: return "stockham-dit";
-    case CoreKind::Bluestein: return "bluestein-fused";
-    case CoreKind::Rader: return "rader-fused";
-    case CoreKind::Conv: return "convolution-rows";
-  }
-  return "?";
-}
-
-const char *io_name(IoKind k) {
-  switch (k) {
-    case IoKind::C2C: return "c2c";
-    case IoKind::R2C: return "r2c-halfpack";
-    case IoKind::C2R: return "c2r-halfpack";
-    case IoKind::R2CFull: return "r2c-full";
-    case IoKind::C2RFull: return "c2r-full";
-    case IoKind::PackC2C: return "real-pairs-in";
-    case IoKind::C2CUnpack: return "real-pairs-out";
-  }
-  return "?";
-}
-
-template <typename T>
-struct TilePass final : PassBase {
-  TileArgs<T> a{};
-  CoreKind kind = CoreKind::Dit;
-  IoKind io = IoKind::C2C;
-  size_t smem = 0;
-  Buf src = Buf::In, dst = Buf::Out;
-  std::string note;
-
-  static void *pick(Buf b, const void *in, void *out, void *s0, void *s1) {
-    switch (b) {
-      case Buf::In: return const_cast<void *>(in);
-      case Buf::Out: return out;
-      case Buf::Scratch0: return s0;
-      case Buf::Scratch1: return s1;
-    }
-    return nullptr;
-  }
-
-  cudaError_t run(const void *in, void *out, void *s0, void *s1, cudaStream_t st) const override {
-    TileArgs<T> b = a;
-    b.in = pick(src, in, out, s0, s1);
-    b.out = pick(dst, in, out, s0, s1);
-    return launch_tile<T>(b, kind, io, smem, st);
-  }
-
-  std::string describe() const override {
-    std::ostringstream o;
-    o << (a.regcol ? "register-columns" : kind_name(kind)) << "/" << io_name(io) << " "
-      << (sizeof(T) == 4 ? "f32" : "f64") << " L=" << a.core.L
-      << " radices=[";
-    for (int s = 0; s < a.core.nst; ++s) o << (s ? "," : "") << a.core.radix[s];
-    o << "] n=" << a.n << " transforms=" << a.nbatch << "x" << a.G << " per_cta=" << a.W
-      << " threads=" << a.W * a.tpt << " smem=" << smem << " " << buf_name(src) << "->" << buf_name(dst);
-    if (a.post_twiddle) o << " +twiddle";
-    if (!note.empty()) o << " (" << note << ")";
-    return o.str();
-  }
-};
-
-// Elementwise real-transform post (Z -> half spectrum) or pre (half spectrum
-// -> Z) processing between the passes of a multi-pass R2C / C2R.
-template <typename T>
-struct RealPass final : PassBase {
-  bool post;
-  Buf src, dst;
-  long long batch, sdist, ddist;
-  int L;
-  const cpx<T> *rtw;
-  RealPass(bool post_, Buf s, Buf d, long long b, long long sd, long long dd, int64_t L_, const cpx<T> *r)
-      : post(post_), src(s), dst(d), batch(b), sdist(sd), ddist(dd), L((int)L_), rtw(r) {}
-  cudaError_t run(const void *in, void *out, void *s0, void *s1, cudaStream_t st) const override {
-    auto *sp = reinterpret_cast<const cpx<T> *>(TilePass<T>::pick(src, in, out, s0, s1));
-    auto *dp = reinterpret_cast<cpx<T> *>(TilePass<T>::pick(dst, in, out, s0, s1));
-    return post ? launch_real_post<T>(sp, dp, batch, sdist, ddist, L, rtw, st)
-                : launch_real_pre<T>(sp, dp, batch, sdist, ddist, L, rtw, st);
-  }
-  std::string describe() const override {
-    std::ostringstream o;
-    o << (post ? "real-post" : "real-pre") << " " << (sizeof(T) == 4 ? "f32" : "f64") << " L=" << L
-      << " transforms=" << batch << " " << buf_name(src) << "->" << buf_name(dst);
-    return o.str();
-  }
-};
 
 // What one CTA-resident transform needs.
 struct CoreSpec {
@@ -1027,22 +930,6 @@ std::unique_ptr<Program> lower_2d(const NodePtr &root, Planner &planner, bool is
 // Batch programs
 // ---------------------------------------------------------------------------
 namespace {
-
-// Shared-memory classes of the persistent launches of a phase: items are
-// grouped by the shared memory their tiles need, so small items get many CTAs
-// per SM instead of the one a 227 KB item allows; the classes of a phase run
-// concurrently on their own streams.  Class 4 holds register-column items.
-constexpr int kBatchClasses = 5;
-// Passes wider than kBatchWidth threads, or with tiles above 113 KB, share
-// class 3 (one 512-thread CTA per SM); the others run kBatchWidth-thread CTAs,
-// two or more per SM.
-constexpr int kBatchWidth = 256;
-static int batch_class(size_t smem, int threads, bool regcol) {
-  if (regcol) return 4;
-  const size_t s = smem + kBatchSmemHeader;
-  if (threads > kBatchWidth) return 3;
-  return s <= 32 * 1024 ? 0 : s <= 76 * 1024 ? 1 : s <= 113 * 1024 ? 2 : 3;
-}
 
 template <typename T>
 struct BatchProgramT final : BatchProgram {

@@ -60,6 +60,35 @@ FLAGFFT_API int flagfftB200LaunchCount(flagfftHandle plan, int direction);
 FLAGFFT_API flagfftResult flagfftB200PlanBatch(flagfftHandle *plan, int ngroups, const int *lengths, const int *counts,
                                               flagfftType type);
 
+/* Request server: continuous batching of transforms of mixed type, length
+ * and batch count.  No counterpart in the reference.
+ *
+ * A server owns a scheduler thread.  Submit queues a request (batch
+ * transforms of length n of any flagfftType, direction for C2C / Z2Z; input
+ * and output are device buffers laid out as flagfftPlan1d(n, type, batch)
+ * would read and write them) and returns at once with a ticket.  The
+ * scheduler admits queued requests in arrival order whenever one of
+ * `max_ticks` tick slots is free and the HBM budget allows (a request is
+ * charged its input, output and workspace bytes; workspaces come from the
+ * stream-ordered memory pool and return to it), and runs each tick's requests
+ * together as persistent work-queue launches on the slot's stream, so ticks
+ * overlap on the device.  A request's result does not depend on which
+ * requests share its tick.  Programs and tables of every (type, n,
+ * direction) seen stay resident; Prepare builds one ahead of the first
+ * request.  Wait blocks until the request finished and gives its latency
+ * from Submit to completion as seen by the scheduler (the caller's buffers
+ * may then be reused).  Submit from any thread; a request larger than the
+ * budget returns FLAGFFT_INVALID_SIZE. */
+typedef struct flagfftB200Server_st *flagfftB200Server;
+FLAGFFT_API flagfftResult flagfftB200ServerCreate(flagfftB200Server *srv, long long hbm_budget_bytes, int max_ticks);
+FLAGFFT_API flagfftResult flagfftB200ServerPrepare(flagfftB200Server srv, flagfftType type, int n, int direction);
+FLAGFFT_API flagfftResult flagfftB200ServerSubmit(flagfftB200Server srv, flagfftType type, int n, int batch,
+                                                 int direction, const void *idata, void *odata, long long *ticket);
+FLAGFFT_API flagfftResult flagfftB200ServerWait(flagfftB200Server srv, long long ticket, double *latency_ms);
+FLAGFFT_API flagfftResult flagfftB200ServerStats(flagfftB200Server srv, long long *completed, long long *ticks,
+                                                long long *bytes_in_use);
+FLAGFFT_API flagfftResult flagfftB200ServerDestroy(flagfftB200Server srv);
+
 /* Batched complex64 FFT of power-of-two length n (8192 <= n <= 2^24) that
  * allocates no memory.  No counterpart in the reference.
  *
