@@ -874,6 +874,24 @@ std::unique_ptr<Program> lower_t(const NodePtr &root, Planner &planner, Transfor
     }
     return prog;
   }
+  if (even && idist % 2 == 0 && odist % 2 == 0) {
+    // Any other even n: the complex transform of length n/2 over the rows
+    // reinterpreted as complex (whatever lowering that length takes), then
+    // the Hermitian post-processing in place on the output (R2C); or the
+    // pre-processing into a workspace, then the complex transform into the
+    // output rows reinterpreted as complex (C2R).
+    if (batch > 65535) throw std::runtime_error("multi-pass batch above 65535");
+    const cpx<T> *rtw = bld.table_rtw(n);
+    if (t == Transform::R2C) {
+      lower_c2c<T>(bld, *prog, core_node, false, L, batch, idist / 2, odist, Buf::In, Buf::Out);
+      prog->passes.push_back(std::make_unique<RealPass<T>>(true, Buf::Out, Buf::Out, batch, odist, odist, L, rtw));
+    } else {
+      prog->scratch1 = std::make_shared<DevMem>((size_t)(batch * L) * sizeof(cpx<T>));
+      prog->passes.push_back(std::make_unique<RealPass<T>>(false, Buf::In, Buf::Scratch1, batch, idist, L, L, rtw));
+      lower_c2c<T>(bld, *prog, core_node, true, L, batch, L, odist / 2, Buf::Scratch1, Buf::Out);
+    }
+    return prog;
+  }
   throw std::runtime_error("real transform length has no lowering on this engine");
 }
 

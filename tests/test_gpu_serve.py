@@ -73,11 +73,11 @@ def test_server_mix_matches_oracle_and_alone(ffb, torch_cuda):
 
 def test_server_budget_and_arguments(ffb, torch_cuda):
     torch = torch_cuda
-    x = torch.zeros(4096, dtype=torch.complex64, device="cuda")
+    x = torch.zeros(8192, dtype=torch.complex64, device="cuda")
     y = torch.empty_like(x)
     with ffb.Server(hbm_budget_bytes=1 << 16, max_ticks=1) as srv:
         with pytest.raises(ffb.FlagFFTError) as e:
-            srv.submit(ffb.C2C, 4096, 1, x, y)  # 64 KiB of I/O: above a 64 KiB budget with nothing else
+            srv.submit(ffb.C2C, 8192, 1, x, y)  # 128 KiB of input + output: above a 64 KiB budget
         assert e.value.code == 8
         with pytest.raises(ffb.FlagFFTError) as e:
             srv.submit(ffb.C2C, 0, 1, x, y)
