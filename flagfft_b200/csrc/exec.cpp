@@ -849,8 +849,9 @@ std::unique_ptr<Program> lower_t(const NodePtr &root, Planner &planner, Transfor
     return prog;
   }
   CoreSpec sa, sb;
+  // (the pack / unpack rides on a Dit core: pass A of R2C, pass B of C2R)
   if (even && core_node->kind == NodeKind::FourStep && bld.core_for(core_node->row, sa) &&
-      bld.core_for(core_node->col, sb)) {
+      bld.core_for(core_node->col, sb) && (t == Transform::R2C ? sa.kind : sb.kind) == CoreKind::Dit) {
     if (batch > 65535) throw std::runtime_error("multi-pass batch above 65535");
     const int64_t n1 = core_node->n1, n2 = core_node->n2;
     const cpx<T> *rtw = bld.table_rtw(n);
@@ -874,7 +875,7 @@ std::unique_ptr<Program> lower_t(const NodePtr &root, Planner &planner, Transfor
     }
     return prog;
   }
-  if (even && idist % 2 == 0 && odist % 2 == 0) {
+  if (even && (t == Transform::R2C ? idist % 2 == 0 : odist % 2 == 0)) {
     // Any other even n: the complex transform of length n/2 over the rows
     // reinterpreted as complex (whatever lowering that length takes), then
     // the Hermitian post-processing in place on the output (R2C); or the
@@ -892,7 +893,27 @@ std::unique_ptr<Program> lower_t(const NodePtr &root, Planner &planner, Transfor
     }
     return prog;
   }
-  throw std::runtime_error("real transform length has no lowering on this engine");
+  {
+    // Any length: widen to complex, the n-point complex transform of any
+    // lowering, then the half spectrum (R2C); or the Hermitian expansion,
+    // the inverse complex transform and the real part (C2R).
+    if (batch > 65535) throw std::runtime_error("multi-pass batch above 65535");
+    auto ws = std::make_shared<DevMem>((size_t)(batch * n) * sizeof(cpx<T>));
+    prog->scratch1 = ws;
+    // (the complex transform runs in place on scratch1: every lowering reads
+    // a tile whole before writing it, and a multi-pass one goes through its
+    // own workspace, scratch0)
+    if (t == Transform::R2C) {
+      prog->passes.push_back(std::make_unique<ConvertPass<T>>(0, Buf::In, Buf::Scratch1, batch, idist, n, n));
+      lower_c2c<T>(bld, *prog, root, false, n, batch, n, n, Buf::Scratch1, Buf::Scratch1);
+      prog->passes.push_back(std::make_unique<ConvertPass<T>>(1, Buf::Scratch1, Buf::Out, batch, n, odist, n));
+    } else {
+      prog->passes.push_back(std::make_unique<ConvertPass<T>>(2, Buf::In, Buf::Scratch1, batch, idist, n, n));
+      lower_c2c<T>(bld, *prog, root, true, n, batch, n, n, Buf::Scratch1, Buf::Scratch1);
+      prog->passes.push_back(std::make_unique<ConvertPass<T>>(3, Buf::Scratch1, Buf::Out, batch, n, odist, n));
+    }
+    return prog;
+  }
 }
 
 template <typename T>

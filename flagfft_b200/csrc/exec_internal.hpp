@@ -107,4 +107,26 @@ struct RealPass final : PassBase {
   }
 };
 
+// Elementwise widen / take / expand around a full complex transform of a
+// real signal (launch_real_convert).
+template <typename T>
+struct ConvertPass final : PassBase {
+  int mode;
+  Buf src, dst;
+  long long batch, sdist, ddist, n;
+  ConvertPass(int m, Buf s, Buf d, long long b, long long sd, long long dd, long long n_)
+      : mode(m), src(s), dst(d), batch(b), sdist(sd), ddist(dd), n(n_) {}
+  cudaError_t run(const void *in, void *out, void *s0, void *s1, cudaStream_t st) const override {
+    return launch_real_convert<T>(mode, TilePass<T>::pick(src, in, out, s0, s1),
+                                  TilePass<T>::pick(dst, in, out, s0, s1), batch, sdist, ddist, n, st);
+  }
+  std::string describe() const override {
+    static const char *names[4] = {"real-widen", "half-take", "hermitian-expand", "real-take"};
+    std::ostringstream o;
+    o << names[mode & 3] << " " << (sizeof(T) == 4 ? "f32" : "f64") << " n=" << n << " transforms=" << batch << " "
+      << buf_name(src) << "->" << buf_name(dst);
+    return o.str();
+  }
+};
+
 }  // namespace ffb

@@ -99,6 +99,56 @@ cudaError_t launch_real_pre(const cpx<T> *x, cpx<T> *z, long long batch, long lo
 #endif
 }
 
+namespace {
+template <typename T>
+FFB_HD void real_convert_one(int mode, const void *src, void *dst, long long sdist, long long ddist, long long n,
+                             long long b, long long k) {
+  if (mode == 0) {
+    const T *x = reinterpret_cast<const T *>(src) + b * sdist;
+    reinterpret_cast<cpx<T> *>(dst)[b * ddist + k] = mk(x[k], (T)0);
+  } else if (mode == 1) {
+    reinterpret_cast<cpx<T> *>(dst)[b * ddist + k] = reinterpret_cast<const cpx<T> *>(src)[b * sdist + k];
+  } else if (mode == 2) {
+    const cpx<T> *X = reinterpret_cast<const cpx<T> *>(src) + b * sdist;
+    cpx<T> v = k <= n / 2 ? X[k] : conjg(X[n - k]);
+    if (k == 0 || (n % 2 == 0 && k == n / 2)) v.y = (T)0;
+    reinterpret_cast<cpx<T> *>(dst)[b * ddist + k] = v;
+  } else {
+    reinterpret_cast<T *>(dst)[b * ddist + k] = reinterpret_cast<const cpx<T> *>(src)[b * sdist + k].x;
+  }
+}
+
+template <typename T>
+__global__ void k_real_convert(int mode, const void *src, void *dst, long long batch, long long sdist,
+                               long long ddist, long long n, long long count) {
+  const long long b = blockIdx.y;
+  for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < count; k += (long long)gridDim.x * blockDim.x)
+    real_convert_one<T>(mode, src, dst, sdist, ddist, n, b, k);
+}
+}  // namespace
+
+template <typename T>
+cudaError_t launch_real_convert(int mode, const void *src, void *dst, long long batch, long long sdist,
+                                long long ddist, long long n, cudaStream_t s) {
+  const long long count = mode == 1 ? n / 2 + 1 : n;
+#ifndef FFB_HOST_EMULATION
+  const int threads = 256;
+  const int blocks = (int)std::min<long long>((count + threads - 1) / threads, 2048);
+  k_real_convert<T><<<dim3(blocks, (unsigned)batch), threads, 0, s>>>(mode, src, dst, batch, sdist, ddist, n, count);
+  return cudaGetLastError();
+#else
+  (void)s;
+  for (long long b = 0; b < batch; ++b)
+    for (long long k = 0; k < count; ++k) real_convert_one<T>(mode, src, dst, sdist, ddist, n, b, k);
+  return cudaSuccess;
+#endif
+}
+
+template cudaError_t launch_real_convert<float>(int, const void *, void *, long long, long long, long long, long long,
+                                                cudaStream_t);
+template cudaError_t launch_real_convert<double>(int, const void *, void *, long long, long long, long long, long long,
+                                                 cudaStream_t);
+
 template cudaError_t launch_real_post<float>(const cpx<float> *, cpx<float> *, long long, long long, long long, int,
                                              const cpx<float> *, cudaStream_t);
 template cudaError_t launch_real_post<double>(const cpx<double> *, cpx<double> *, long long, long long, long long,

@@ -85,6 +85,17 @@ struct TileArgs {
 //         (in place allowed: z and x may alias with zdist == xdist)
 //   pre:  Z_k = (X_k + conj X_{L-k}) + i W_n^-k (X_k - conj X_{L-k}), k < L,
 //         Im X_0 and Im X_L ignored
+// Elementwise conversions around a full-length complex transform of a real
+// signal (any n, batch rows):
+//   mode 0 widen:  z[k] = x[k] + 0i, k < n           (x real, row dist xd; z complex, zd)
+//   mode 1 half:   y[k] = z[k], k <= n/2             (complex -> complex)
+//   mode 2 expand: z[k] = X[k] (k <= n/2), conj X[n-k] (k > n/2), Im X[0] and, for
+//                  even n, Im X[n/2] taken as 0       (complex half -> complex full)
+//   mode 3 real:   y[k] = Re z[k], k < n            (complex -> real)
+template <typename T>
+cudaError_t launch_real_convert(int mode, const void *src, void *dst, long long batch, long long sdist,
+                                long long ddist, long long n, cudaStream_t stream);
+
 template <typename T>
 cudaError_t launch_real_post(const cpx<T> *z, cpx<T> *x, long long batch, long long zdist, long long xdist, int L,
                              const cpx<T> *rtw, cudaStream_t stream);

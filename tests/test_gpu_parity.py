@@ -87,8 +87,10 @@ def test_input_scales(ffb, torch_cuda, plans, scale):
 
 @pytest.mark.parametrize("double", [False, True], ids=["R2C_C2R", "D2Z_Z2D"])
 # 40022 / 65534: n/2 = 20011 (prime) and 32767 = 7 * 31 * 151 run as a complex
-# transform of n/2 points of any lowering plus the Hermitian post / pre pass
-@pytest.mark.parametrize("n", [2, 3, 15, 16, 64, 100, 101, 134, 256, 2018, 4096, 8192, 16384, 1701, 9000, 40022, 65534])
+# transform of n/2 points of any lowering plus the Hermitian post / pre pass;
+# 201 = 3 * 67 and 40027 (prime, odd) widen to a full complex transform
+@pytest.mark.parametrize("n", [2, 3, 15, 16, 64, 100, 101, 134, 256, 2018, 4096, 8192, 16384, 1701, 9000, 40022, 65534,
+                               201, 40027])
 def test_real_vs_oracle(ffb, torch_cuda, n, double):
     torch = torch_cuda
     batch = 4
