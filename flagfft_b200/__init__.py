@@ -17,7 +17,7 @@ import os
 from pathlib import Path
 
 __all__ = [
-    "FlagFFTError", "Plan", "plan1d", "plan2d", "plan3d", "plan_many", "plan_batch", "Server", "planner_tree", "library_path",
+    "FlagFFTError", "Plan", "plan1d", "plan2d", "plan3d", "plan_many", "plan_batch", "Server", "tune", "tune_candidates", "planner_tree", "library_path",
     "C2C", "Z2Z", "R2C", "D2Z", "C2R", "Z2D", "FORWARD", "INVERSE", "STATUS",
 ]
 
@@ -79,6 +79,8 @@ def _load():
         "flagfftB200ServerStats": (i, [H, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong),
                                        ctypes.POINTER(ctypes.c_longlong)]),
         "flagfftB200ServerDestroy": (i, [H]),
+        "flagfftB200Tune": (i, [i, i, i, i, cp, cp, i, ctypes.POINTER(ctypes.c_double)]),
+        "flagfftB200TuneCandidates": (i, [i, i, cp, i]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name)
@@ -298,6 +300,26 @@ class Server:
 
     def __exit__(self, *exc):
         self.close()
+
+
+def tune(n: int, ftype: int = C2C, batch: int = 1, direction: int = FORWARD, db_path: str | None = None) -> dict:
+    """Autotune one request shape (flagfftB200Tune) and store the fastest tree
+    in the tune database; returns the report (every candidate's time)."""
+    buf = ctypes.create_string_buffer(1 << 20)
+    ms = ctypes.c_double(0)
+    _check(_lib().flagfftB200Tune(n, ftype, batch, direction, db_path.encode() if db_path else None, buf, len(buf),
+                                  ctypes.byref(ms)), "flagfftB200Tune")
+    return json.loads(buf.value.decode())
+
+
+def tune_candidates(n: int, is_double: bool = False) -> list:
+    """The autotuner's candidate trees for a length (host only)."""
+    need = _lib().flagfftB200TuneCandidates(n, int(is_double), None, 0)
+    if need < 0:
+        raise FlagFFTError(4, f"no candidates for length {n}")
+    buf = ctypes.create_string_buffer(need + 1)
+    _lib().flagfftB200TuneCandidates(n, int(is_double), buf, need + 1)
+    return json.loads(buf.value.decode())
 
 
 def planner_tree(n: int, is_double: bool = False, smem_bytes: int = 0) -> dict:

@@ -3,10 +3,12 @@
 // (src/exec/c_api_plan.cpp, src/exec/c_api_exec.cpp, src/exec/c_api_internal.cpp).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <memory>
+#include <optional>
 #include <mutex>
 #include <sstream>
 #include <string>
@@ -411,6 +413,129 @@ extern "C" int flagfftB200PlannerTree(int n, int is_double, long long smem_bytes
   } catch (const std::exception &) {
     return -1;
   }
+}
+
+extern "C" int flagfftB200TuneCandidates(int n, int is_double, char *buf, int buflen) {
+  if (n <= 0) return -1;
+  try {
+    Planner pl(is_double != 0, 232448);
+    std::string s = "[";
+    const auto c = pl.tune_candidates(n, 12);
+    for (size_t i = 0; i < c.size(); ++i) s += (i ? ", " : "") + c[i]->to_json();
+    s += "]";
+    if (buf && buflen > 0) {
+      size_t k = std::min<size_t>(s.size(), (size_t)buflen - 1);
+      std::memcpy(buf, s.data(), k);
+      buf[k] = 0;
+    }
+    return (int)s.size();
+  } catch (const std::exception &) {
+    return -1;
+  }
+}
+
+extern "C" flagfftResult flagfftB200Tune(int n, flagfftType type, int batch, int direction, const char *db_path,
+                                        char *report, int buflen, double *best_ms) {
+  if (n <= 0) return FLAGFFT_INVALID_SIZE;
+  if (batch <= 0) return FLAGFFT_INVALID_VALUE;
+  if (type != FLAGFFT_C2C && type != FLAGFFT_Z2Z) return FLAGFFT_INVALID_TYPE;
+  if (direction != FLAGFFT_FORWARD && direction != FLAGFFT_INVERSE) return FLAGFFT_INVALID_VALUE;
+  PlanDesc d;
+  d.rank = 1;
+  d.n = {n};
+  d.batch = batch;
+  d.type = type;
+  type_info(type, d);
+  flagfftResult dr = ensure_device(d);
+  if (dr != FLAGFFT_SUCCESS) return dr;
+#ifdef FFB_HOST_EMULATION
+  (void)db_path;
+  (void)report;
+  (void)buflen;
+  (void)best_ms;
+  return FLAGFFT_NOT_SUPPORTED;
+#else
+  try {
+    Planner pl(d.is_double, d.smem_optin);
+    const auto cands = pl.tune_candidates(n, 12);
+    const size_t bytes = (size_t)batch * (size_t)n * (d.is_double ? 16 : 8);
+    DevMem in(bytes), out(bytes);
+    cudaMemset(in.ptr, 0x3c, bytes);  // timing does not depend on the values
+    cudaStream_t st = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    Layout lay;
+    lay.batch = batch;
+    lay.idist = n;
+    lay.odist = n;
+    const bool inverse = direction == FLAGFFT_INVERSE;
+    std::string rows;
+    double best = 1e30, def_ms = -1;
+    NodePtr best_node;
+    for (size_t i = 0; i < cands.size(); ++i) {
+      double ms = -1;
+      try {
+        auto prog = lower(cands[i], pl, d.is_double, Transform::C2C, inverse, n, lay, false);
+        for (int w = 0; w < 2; ++w) prog->run(in.ptr, out.ptr, st);
+        std::vector<double> t;
+        for (int r = 0; r < 3; ++r) {
+          cudaEventRecord(e0, st);
+          for (int k = 0; k < 10; ++k) prog->run(in.ptr, out.ptr, st);
+          cudaEventRecord(e1, st);
+          cudaEventSynchronize(e1);
+          float el = 0;
+          cudaEventElapsedTime(&el, e0, e1);
+          t.push_back(el / 10.0);
+        }
+        std::sort(t.begin(), t.end());
+        ms = t[1];
+        if (cudaGetLastError() != cudaSuccess) ms = -1;
+      } catch (const std::exception &) {
+        ms = -1;
+      }
+      if (i == 0) def_ms = ms;
+      if (ms > 0 && ms < best) {
+        best = ms;
+        best_node = cands[i];
+      }
+      rows += std::string(rows.empty() ? "" : ", ") + "{\"key\": \"" + cands[i]->key_repr() +
+              "\", \"ms\": " + std::to_string(ms) + "}";
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaStreamDestroy(st);
+    if (!best_node) return FLAGFFT_EXEC_FAILED;
+    bool stored = false;
+    const auto path = db_path ? std::optional<std::string>(db_path) : tune_db_path();
+    if (path) {
+      TuneKey k;
+      k.device_arch = d.arch;
+      k.fft_length = n;
+      k.batch = batch;
+      k.dtype = d.is_double ? "complex128" : "complex64";
+      k.direction = inverse ? "inverse" : "forward";
+      stored = tune_store(k, "{\"root\": " + best_node->to_json() + "}", best, "flagfft-b200-autotune", *path);
+    }
+    if (best_ms) *best_ms = best;
+    const std::string rep = "{\"n\": " + std::to_string(n) + ", \"batch\": " + std::to_string(batch) +
+                            ", \"best_ms\": " + std::to_string(best) + ", \"default_ms\": " +
+                            std::to_string(def_ms) + ", \"stored\": " + (stored ? "true" : "false") +
+                            ", \"best\": " + best_node->to_json() + ", \"candidates\": [" + rows + "]}";
+    if (report && buflen > 0) {
+      size_t c = std::min<size_t>(rep.size(), (size_t)buflen - 1);
+      std::memcpy(report, rep.data(), c);
+      report[c] = 0;
+    }
+    return FLAGFFT_SUCCESS;
+  } catch (const std::bad_alloc &) {
+    return FLAGFFT_ALLOC_FAILED;
+  } catch (const std::exception &e) {
+    std::fprintf(stderr, "[flagfft] tune failed: %s\n", e.what());
+    return FLAGFFT_SETUP_FAILED;
+  }
+#endif
 }
 
 extern "C" const char *flagfftB200PlanJson(flagfftHandle h) {

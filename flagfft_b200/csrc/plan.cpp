@@ -550,6 +550,57 @@ double Planner::cost_for(int64_t n) {
   return v;
 }
 
+std::vector<NodePtr> Planner::tune_candidates(int64_t n, int limit) {
+  std::vector<NodePtr> out;
+  std::vector<std::string> seen;
+  auto add = [&](const NodePtr &node) {
+    if (!node || (int)out.size() >= limit || !raw_supported(node)) return;
+    const std::string k = node->key_repr();
+    if (std::find(seen.begin(), seen.end(), k) != seen.end()) return;
+    seen.push_back(k);
+    out.push_back(node);
+  };
+  NodePtr def = build_raw_root(*this, n, nullptr, nullptr);
+  add(def);
+  // leaf radix orders (descending, ascending) of the default factor multiset
+  int64_t rem = 1;
+  auto g = greedy(n, &rem);
+  if (rem == 1 && !g.empty() && n <= kLeafMaxN) {
+    std::vector<int64_t> f = leaf_factors(n);
+    std::vector<int64_t> asc = f, desc = f;
+    std::sort(asc.begin(), asc.end());
+    std::sort(desc.rbegin(), desc.rend());
+    for (const auto &o : {desc, asc, g})
+      if (use_leaf(n, o)) add(leaf_plan(n, o));
+  }
+  // four-step splits, most balanced first, children from the default planner
+  std::vector<std::pair<double, int64_t>> pairs;
+  for (int64_t n1 : divisors(n)) {
+    if (n1 <= 1 || n1 >= n) continue;
+    pairs.push_back({std::abs(std::log((double)n1) - std::log((double)(n / n1))), n1});
+  }
+  std::sort(pairs.begin(), pairs.end());
+  int splits = 0;
+  for (const auto &pr : pairs) {
+    if (splits >= 4) break;
+    try {
+      add(make_four_step_node(n, pr.second, n / pr.second, auto_node(pr.second), auto_node(n / pr.second)));
+      ++splits;
+    } catch (const std::exception &) {
+    }
+  }
+  // convolution routes for primes and lengths without a leaf
+  if (n > kDirectDftMaxN && (is_prime_length(n) || rem != 1)) {
+    const int64_t m = next_conv_length(2 * n - 1);
+    add(make_bluestein_node(n, m, auto_node(m)));
+    if (is_prime_length(n)) {
+      const int64_t root = find_primitive_root(n);
+      add(make_rader_node(n, root, rader_index_table(n, root), auto_node(n - 1)));
+    }
+  }
+  return out;
+}
+
 NodePtr build_raw_root(Planner &planner, int64_t n, const NodePtr &tuned_fwd, const NodePtr &tuned_inv) {
   NodePtr root = (tuned_fwd && raw_supported(tuned_fwd)) ? tuned_fwd : planner.build(n);
   if (!raw_supported(root)) root = (tuned_inv && raw_supported(tuned_inv)) ? tuned_inv : planner.build(n);

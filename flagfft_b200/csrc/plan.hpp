@@ -79,6 +79,11 @@ class Planner {
 
   NodePtr build(int64_t n);
   double cost_for(int64_t n);
+  // Alternative raw-supported trees for the autotuner, the default tree
+  // first: other orders of the leaf radices, balanced four-step splits with
+  // the default child trees, and Bluestein / Rader for primes; at most
+  // `limit`, distinct by key.
+  std::vector<NodePtr> tune_candidates(int64_t n, int limit);
   int64_t choose_lanes(int64_t n, const std::vector<int64_t> &factors) const;
   int64_t choose_num_warps(int64_t lanes) const;
 

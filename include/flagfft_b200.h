@@ -60,6 +60,24 @@ FLAGFFT_API int flagfftB200LaunchCount(flagfftHandle plan, int direction);
 FLAGFFT_API flagfftResult flagfftB200PlanBatch(flagfftHandle *plan, int ngroups, const int *lengths, const int *counts,
                                               flagfftType type);
 
+/* Autotuner: times the planner's alternative trees for a C2C / Z2Z request
+ * (batch transforms of length n, one direction) on the current device, and
+ * writes the fastest into the tune database as a valid rank-0 row of the
+ * reference's table `tuned_measurements` (db_path, or the path plan creation
+ * reads: $FLAGFFT_TUNE_DB, else <executable dir>/.flagfft/tuned_plans.sqlite),
+ * so later plans of that length, batch bucket, dtype and direction use it.
+ * The reference declares this step (flagfft-cli tune) but writes nothing
+ * (src/cli_tools/tune/tune.cpp:7-9); its lookup side is
+ * src/utils/plan_json.cpp:163-207.  Candidates: the default tree, other
+ * orders of its leaf radices, the four most balanced four-step splits, and
+ * Bluestein / Rader for primes.  `report` (buflen bytes) receives JSON with
+ * every candidate's time; *best_ms the fastest time per Exec. */
+FLAGFFT_API flagfftResult flagfftB200Tune(int n, flagfftType type, int batch, int direction, const char *db_path,
+                                         char *report, int buflen, double *best_ms);
+/* The autotuner's candidate trees for a length, as a JSON array (host only).
+ * Returns the full length, or -1. */
+FLAGFFT_API int flagfftB200TuneCandidates(int n, int is_double, char *buf, int buflen);
+
 /* Request server: continuous batching of transforms of mixed type, length
  * and batch count.  No counterpart in the reference.
  *

@@ -97,3 +97,14 @@ def test_batch_plan_argument_checks(ffb):
     assert L.flagfftB200PlanBatch(C.byref(h), 1, ints(16), ints(1), ffb.R2C) == 3
     assert L.flagfftB200PlanBatch(C.byref(h), 2, ints(16, 0), ints(1, 1), ffb.C2C) == 8
     assert L.flagfftB200PlanBatch(C.byref(h), 2, ints(16, 32), ints(1, 0), ffb.Z2Z) == 4
+
+
+def test_tune_candidates_host_only(ffb):
+    """The autotuner's candidates: the default tree first, distinct, every
+    one a tree of the requested length."""
+    for n, dbl in ((4096, False), (1009, False), (30030, True), (67, False)):
+        cands = ffb.tune_candidates(n, dbl)
+        assert cands and cands[0] == ffb.planner_tree(n, dbl)
+        keys = [repr(c) for c in cands]
+        assert len(set(keys)) == len(keys)
+        assert all(c["length"] == n for c in cands)
