@@ -545,4 +545,87 @@ FFB_HD void run_stockham_smem(const Core &c, cpx<T> *src, cpx<T> *oth, int tid, 
   }
 }
 
+// Stage runner of a ping-pong pass: the runtime radix sequence of a Core.
+template <typename T>
+struct GenericStages {
+  template <bool INV, class Sync>
+  FFB_HD void run(const Core &c, cpx<T> *src, cpx<T> *oth, int tid, int nthr, const cpx<T> *__restrict__ tw,
+                  Sync sync) const {
+    run_stockham_smem<T, INV>(c, src, oth, tid, nthr, tw, sync);
+  }
+};
+
+// ---------------------------------------------------------------------------
+// Stockham stages with the radix sequence fixed at compile time (radix-16
+// chains of power-of-two lengths).  With L, Ns and R constants, j mod Ns is a
+// mask, the twiddle rows sit at constant strides, and the padded positions
+// p + p/16 of a butterfly's R reads (and R writes) are one base plus constant
+// offsets whenever the stride between them is a multiple of 16 (or the
+// butterfly's outputs are R consecutive positions inside one 16-block): two
+// address computations per butterfly instead of 2R.
+// ---------------------------------------------------------------------------
+template <typename T, bool INV, int L, int Ns, int R>
+FFB_HD void fixed_stage(const cpx<T> *src, cpx<T> *dst, int tid, int nthr, const cpx<T> *__restrict__ tw) {
+  constexpr int nb = L / R;
+  for (int j = tid; j < nb; j += nthr) {
+    const int k = Ns == 1 ? 0 : j % Ns;
+    cpx<T> v[R];
+    if constexpr (nb % 16 == 0) {
+      const cpx<T> *rp = src + pp_pos(j);
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[r] = rp[r * (nb + nb / 16)];
+    } else {
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[r] = src[pp_pos(j + r * nb)];
+    }
+    if constexpr (Ns > 1) {
+      const cpx<T> *row = tw + k;  // row r-1 of the stage block at (r-1) * Ns
+#pragma unroll
+      for (int r = 1; r < R; ++r) v[r] = cmul(v[r], ldg_c(row + (r - 1) * Ns));
+    }
+    dft_fixed<R, INV, T>(v);
+    const int base = (j - k) * R + k;
+    if constexpr (Ns % 16 == 0) {
+      cpx<T> *wp = dst + pp_pos(base);
+#pragma unroll
+      for (int q = 0; q < R; ++q) wp[q * (Ns + Ns / 16)] = v[q];
+    } else if constexpr (Ns == 1 && 16 % R == 0) {
+      cpx<T> *wp = dst + pp_pos(base);  // R consecutive positions inside one 16-block
+#pragma unroll
+      for (int q = 0; q < R; ++q) wp[q] = v[q];
+    } else {
+#pragma unroll
+      for (int q = 0; q < R; ++q) dst[pp_pos(base + q * Ns)] = v[q];
+    }
+  }
+}
+
+// Stages Ns, Ns*R0, ... of a length-L transform: stage reads `src`, writes
+// `oth`, then the two swap; `twoff` is the stage's block in the core's table.
+template <typename T, bool INV, int L, int Ns, int TwOff, int... Rs>
+struct FixedStages {
+  template <class Sync>
+  static FFB_HD void run(cpx<T> *, cpx<T> *, int, int, const cpx<T> *__restrict__, Sync) {}
+};
+template <typename T, bool INV, int L, int Ns, int TwOff, int R, int... Rest>
+struct FixedStages<T, INV, L, Ns, TwOff, R, Rest...> {
+  template <class Sync>
+  static FFB_HD void run(cpx<T> *src, cpx<T> *oth, int tid, int nthr, const cpx<T> *__restrict__ tw, Sync sync) {
+    fixed_stage<T, INV, L, Ns, R>(src, oth, tid, nthr, tw + TwOff);
+    sync();
+    FixedStages<T, INV, L, Ns * R, TwOff + (R - 1) * Ns, Rest...>::run(oth, src, tid, nthr, tw, sync);
+  }
+};
+
+// Stage runner for one compile-time radix sequence (the Core it runs must
+// have exactly these radices).
+template <typename T, int L, int... Rs>
+struct FixedStagesRunner {
+  template <bool INV, class Sync>
+  FFB_HD void run(const Core &, cpx<T> *src, cpx<T> *oth, int tid, int nthr, const cpx<T> *__restrict__ tw,
+                  Sync sync) const {
+    FixedStages<T, INV, L, 1, 0, Rs...>::run(src, oth, tid, nthr, tw, sync);
+  }
+};
+
 }  // namespace ffb

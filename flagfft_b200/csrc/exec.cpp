@@ -462,12 +462,18 @@ class Builder {
     // the in-place DIT / DIF path otherwise.
     const size_t pp_per = (2 * (size_t)pp_size((int)L) + 3) * sizeof(cpx<T>);
     a.pp = (io == IoKind::C2C && L > 1 && pp_per <= limit) ? 1 : 0;
+    // ping-pong cores run their radices largest first (any order is the same
+    // DFT; this one matches the compile-time sequences), and a convolution's
+    // inverse core the same order; the in-place pair needs DIF then DIT with
+    // the radices reversed
+    std::vector<int> radices = spec.radices;
+    if (a.pp) std::sort(radices.rbegin(), radices.rend());
     if (spec.kind == CoreKind::Dit) {
-      a.core = make_dit_core(L, spec.radices);
+      a.core = make_dit_core(L, radices);
     } else {
-      a.core = a.pp ? make_dit_core(L, spec.radices) : make_dif_core(L, spec.radices);
-      std::vector<int> rev(spec.radices.rbegin(), spec.radices.rend());
-      a.core2 = make_dit_core(L, rev);
+      a.core = a.pp ? make_dit_core(L, radices) : make_dif_core(L, radices);
+      std::vector<int> rev(radices.rbegin(), radices.rend());
+      a.core2 = make_dit_core(L, a.pp ? radices : rev);
       if (spec.kind != CoreKind::Conv) fill_convolution(a, spec, inverse);  // Conv: caller supplies the kernel
     }
     // one-codelet transforms lying side by side in memory on both sides run

@@ -14,6 +14,8 @@ template <typename T, int K>
 cudaError_t launch_group(const TileArgs<T> &a, int io, size_t smem, cudaStream_t s);
 template <typename T, int K, bool INV>
 cudaError_t launch_pp(const TileArgs<T> &a, size_t smem, cudaStream_t s);
+template <typename T, int KIND, bool INV>
+cudaError_t launch_pp_fixed_any(const TileArgs<T> &a, size_t smem, cudaStream_t s);
 template <typename T, int KIND, int IO>
 cudaError_t launch_one(const TileArgs<T> &a, size_t smem, cudaStream_t s);
 }  // namespace tile
@@ -163,6 +165,14 @@ cudaError_t launch_tile(const TileArgs<T> &a, CoreKind kind, IoKind io, size_t s
   const int k = (int)kind, o = (int)io;
   if (a.regcol) return launch_regcol<T>(a, s);
   if (a.pp && o == 0) {
+    // compile-time radix sequences first (cudaErrorNotSupported: no kernel for this core)
+    if (k == 0 || k == 1 || k == 3) {
+      const cudaError_t e = k == 0 ? (a.inv ? tile::launch_pp_fixed_any<T, 0, true>(a, smem, s)
+                                            : tile::launch_pp_fixed_any<T, 0, false>(a, smem, s))
+                            : k == 1 ? tile::launch_pp_fixed_any<T, 1, false>(a, smem, s)
+                                     : tile::launch_pp_fixed_any<T, 3, false>(a, smem, s);
+      if (e != cudaErrorNotSupported) return e;
+    }
     switch (k) {
       case 0: return a.inv ? tile::launch_pp<T, 0, true>(a, smem, s) : tile::launch_pp<T, 0, false>(a, smem, s);
       case 1: return tile::launch_pp<T, 1, false>(a, smem, s);

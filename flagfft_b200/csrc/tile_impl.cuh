@@ -377,9 +377,12 @@ FFB_HD int pp_slot_len(int L) {
 }
 
 // INV: direction of a Dit core (KIND 0); convolutions (KIND 1-3) run their
-// forward core and inverse core2 whatever INV is.
-template <typename T, int KIND, bool INV, class X>
-FFB_HD void tile_body_pp(const TileArgs<T> &a, long long bx, long long by, cpx<T> *sm, const X &x) {
+// forward core and inverse core2 whatever INV is.  Stages: the stage runner
+// (GenericStages, or FixedStagesRunner for a compile-time radix sequence
+// that core and core2 both have).
+template <typename T, int KIND, bool INV, class X, class Stages = GenericStages<T>>
+FFB_HD void tile_body_pp(const TileArgs<T> &a, long long bx, long long by, cpx<T> *sm, const X &x,
+                         const Stages &stages = Stages{}) {
   const int L = a.core.L;
   const int Lq = pp_size(L);
   const int slot_len = pp_slot_len<T>(L);
@@ -435,7 +438,7 @@ FFB_HD void tile_body_pp(const TileArgs<T> &a, long long bx, long long by, cpx<T
     x.per_slot(W, [&](int slot, int tid, int tpt) FFB_INL {
       cpx<T> *const b0 = sm + slot * slot_len, *const b1 = b0 + Lq;
       const int S = a.core.nst;
-      run_stockham_smem<T, KIND == 0 && INV>(a.core, b0, b1, tid, tpt, a.tw, sync);
+      stages.template run<KIND == 0 && INV>(a.core, b0, b1, tid, tpt, a.tw, sync);
       if constexpr (KIND != 0) {
         // kernel product on the forward result (natural order), then the inverse
         const int wc = slot < wlive ? slot : wlive - 1;
@@ -450,7 +453,7 @@ FFB_HD void tile_body_pp(const TileArgs<T> &a, long long bx, long long by, cpx<T
           r[pp_pos(p)] = cmul(v, ldg_c(kern + p));
         }
         sync();
-        run_stockham_smem<T, true>(a.core2, r, (S & 1) ? b0 : b1, tid, tpt, a.tw2, sync);
+        stages.template run<true>(a.core2, r, (S & 1) ? b0 : b1, tid, tpt, a.tw2, sync);
       }
     });
   }
@@ -521,6 +524,79 @@ __global__ void __launch_bounds__(TileBounds<T>::kMaxThreads) k_tile_pp(const __
   extern __shared__ __align__(16) unsigned char smraw[];
   DevX x{a.tpt, a.wfast};
   tile_body_pp<T, KIND, INV>(a, (long long)blockIdx.x, (long long)blockIdx.y, reinterpret_cast<cpx<T> *>(smraw), x);
+}
+
+template <typename T, int KIND, bool INV, int L, int... Rs>
+__global__ void __launch_bounds__(TileBounds<T>::kMaxThreads) k_tile_pp_fixed(const __grid_constant__ TileArgs<T> a) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  DevX x{a.tpt, a.wfast};
+  tile_body_pp<T, KIND, INV>(a, (long long)blockIdx.x, (long long)blockIdx.y, reinterpret_cast<cpx<T> *>(smraw), x,
+                             FixedStagesRunner<T, L, Rs...>{});
+}
+
+// True when `c` is exactly the radix sequence Rs... of length L.
+template <int L, int... Rs>
+FFB_HD bool core_is(const Core &c) {
+  constexpr int n = sizeof...(Rs);
+  const int r[n] = {Rs...};
+  if (c.L != L || c.nst != n) return false;
+  for (int s = 0; s < n; ++s)
+    if (c.radix[s] != r[s]) return false;
+  return true;
+}
+
+#ifndef FFB_HOST_EMULATION
+template <typename T, int KIND, bool INV, int L, int... Rs>
+cudaError_t launch_pp_fixed(const TileArgs<T> &a, size_t smem, cudaStream_t s) {
+  static bool configured = false;
+  if (!configured) {
+    cudaError_t e = cudaFuncSetAttribute(k_tile_pp_fixed<T, KIND, INV, L, Rs...>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, 232448);
+    if (e != cudaSuccess) return e;
+    configured = true;
+  }
+  dim3 grid((unsigned)((a.G + a.W - 1) / a.W), (unsigned)a.nbatch, 1);
+  dim3 block((unsigned)(a.W * a.tpt), 1, 1);
+  k_tile_pp_fixed<T, KIND, INV, L, Rs...><<<grid, block, smem, s>>>(a);
+  return cudaGetLastError();
+}
+#else
+template <typename T, int KIND, bool INV, int L, int... Rs>
+cudaError_t launch_pp_fixed(const TileArgs<T> &a, size_t smem, cudaStream_t) {
+  std::vector<unsigned char> buf(smem + 64);
+  cpx<T> *sm = reinterpret_cast<cpx<T> *>(buf.data());
+  const long long tiles = (a.G + a.W - 1) / a.W;
+  HostX x;
+  for (long long by = 0; by < a.nbatch; ++by)
+    for (long long bx = 0; bx < tiles; ++bx) {
+      std::memset(buf.data(), 0xff, buf.size());
+      tile_body_pp<T, KIND, INV>(a, bx, by, sm, x, FixedStagesRunner<T, L, Rs...>{});
+    }
+  return cudaSuccess;
+}
+#endif
+
+// The compile-time radix sequences with their own kernels: radix-16 chains
+// of the power-of-two lengths 128..8192 (one smaller radix last).
+#define FFB_FIXED_SEQUENCES(X)        \
+  X(128, 16, 8)                       \
+  X(256, 16, 16)                      \
+  X(512, 16, 16, 2)                   \
+  X(1024, 16, 16, 4)                  \
+  X(2048, 16, 16, 8)                  \
+  X(4096, 16, 16, 16)                 \
+  X(8192, 16, 16, 16, 2)
+
+// Launches the fixed-sequence kernel matching the pass's core (and core2 for
+// convolutions); cudaErrorNotSupported when none matches.
+template <typename T, int KIND, bool INV>
+cudaError_t launch_pp_fixed_any(const TileArgs<T> &a, size_t smem, cudaStream_t s) {
+#define FFB_TRY(L, ...)                                                                              \
+  if (core_is<L, __VA_ARGS__>(a.core) && (KIND == 0 || core_is<L, __VA_ARGS__>(a.core2)))           \
+    return launch_pp_fixed<T, KIND, INV, L, __VA_ARGS__>(a, smem, s);
+  FFB_FIXED_SEQUENCES(FFB_TRY)
+#undef FFB_TRY
+  return cudaErrorNotSupported;
 }
 
 #ifndef FFB_HOST_EMULATION
