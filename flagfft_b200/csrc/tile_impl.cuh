@@ -577,8 +577,10 @@ cudaError_t launch_pp_fixed(const TileArgs<T> &a, size_t smem, cudaStream_t) {
 #endif
 
 // The compile-time radix sequences with their own kernels: radix-16 chains
-// of the power-of-two lengths 128..8192 (one smaller radix last).
+// of the power-of-two lengths 128..8192 (one smaller radix last), and the
+// mixed-radix 1701 = 9 * 9 * 7 * 3.
 #define FFB_FIXED_SEQUENCES(X)        \
+  X(1701, 9, 9, 7, 3)                 \
   X(128, 16, 8)                       \
   X(256, 16, 16)                      \
   X(512, 16, 16, 2)                   \
