@@ -469,8 +469,8 @@ FFB_HD void run_dif(cpx<T> *buf, const Core &c, int tid, int nthr,
 
 // Shared-memory position of element p in a ping-pong buffer: one pad element
 // per 16 spreads the stride-R writes of the early stages over the banks.
-FFB_HD int pp_pos(int p) { return p + (p >> 4); }
-FFB_HD int pp_size(int L) { return ((L + (L >> 4) + 1) + 1) & ~1; }
+FFB_HD constexpr int pp_pos(int p) { return p + (p >> 4); }
+FFB_HD constexpr int pp_size(int L) { return ((L + (L >> 4) + 1) + 1) & ~1; }
 
 template <int R, bool INV, typename T, class Src, class Dst>
 FFB_HD void stockham_stage_r(const Core &c, int s, int tid, int nthr, const cpx<T> *__restrict__ tw,

@@ -20,6 +20,12 @@ template <typename T, int KIND, int IO>
 cudaError_t launch_one(const TileArgs<T> &a, size_t smem, cudaStream_t s);
 }  // namespace tile
 
+namespace rows {
+// defined in k_*_rows*.cu
+template <typename T, int KIND, bool INV>
+cudaError_t launch_rows_any(const TileArgs<T> &a, size_t smem, cudaStream_t s);
+}  // namespace rows
+
 namespace {
 
 // One thread per pair (k, L-k), k = 0..L/2: reads both Z values, writes both
@@ -165,7 +171,15 @@ cudaError_t launch_tile(const TileArgs<T> &a, CoreKind kind, IoKind io, size_t s
   const int k = (int)kind, o = (int)io;
   if (a.regcol) return launch_regcol<T>(a, s);
   if (a.pp && o == 0) {
-    // compile-time radix sequences first (cudaErrorNotSupported: no kernel for this core)
+    // compile-time radix sequences first: contiguous rows, then any layout
+    // (cudaErrorNotSupported: no kernel for this pass)
+    if (k == 0 || k == 1 || k == 3) {
+      const cudaError_t e = k == 0 ? (a.inv ? rows::launch_rows_any<T, 0, true>(a, smem, s)
+                                            : rows::launch_rows_any<T, 0, false>(a, smem, s))
+                            : k == 1 ? rows::launch_rows_any<T, 1, false>(a, smem, s)
+                                     : rows::launch_rows_any<T, 3, false>(a, smem, s);
+      if (e != cudaErrorNotSupported) return e;
+    }
     if (k == 0 || k == 1 || k == 3) {
       const cudaError_t e = k == 0 ? (a.inv ? tile::launch_pp_fixed_any<T, 0, true>(a, smem, s)
                                             : tile::launch_pp_fixed_any<T, 0, false>(a, smem, s))

@@ -1,0 +1,395 @@
+// Row passes with the whole shape fixed at compile time.
+//
+// A ping-pong pass whose transforms are contiguous rows (element i of
+// transform g at g * ig + i, output k at g * og + k) and whose core is one of
+// the compile-time radix sequences runs here, with the threads per transform
+// (TPT) a constant too.  Against the general tile body this
+//   * reads the first Stockham stage's butterfly inputs straight from global
+//     memory (butterfly j of the first stage takes elements j + r * L/R0, so
+//     consecutive threads read consecutive addresses), skipping the load
+//     phase's shared-memory round trip and barrier;
+//   * writes the last stage's outputs straight to global memory (the last
+//     stage's butterfly j writes elements j + q * L/R_last, coalesced the
+//     same way), skipping the store phase;
+//   * in a convolution, multiplies the forward transform's last-stage outputs
+//     by the kernel spectrum in registers before they reach shared memory;
+//   * has every loop bound and shared-memory offset compile-time, so a
+//     thread's R reads and R writes of a stage are one address each plus
+//     constant offsets.
+// A length-L transform with S stages thus makes S - 1 shared-memory round
+// trips (2S - 1 for a convolution) instead of S + 1 (2S + 2).
+#pragma once
+
+#include "tile_impl.cuh"
+
+namespace ffb {
+namespace rows {
+
+// Compile-time radix sequence: radix, span (product of the earlier radices)
+// and twiddle-block offset of stage s, laid out as the host builds a Dit
+// core's per-stage table (stage s block: R_s - 1 rows of span_s entries).
+template <int... Rs>
+struct Seq {
+  static constexpr int n = sizeof...(Rs);
+  static FFB_HD constexpr int r(int s) {
+    constexpr int a[] = {Rs...};
+    return a[s];
+  }
+  static FFB_HD constexpr int span(int s) {
+    int p = 1;
+    for (int i = 0; i < s; ++i) p *= r(i);
+    return p;
+  }
+  static FFB_HD constexpr int twoff(int s) {
+    int o = 0;
+    for (int i = 0; i < s; ++i) o += (r(i) - 1) * span(i);
+    return o;
+  }
+  static FFB_HD constexpr int rmax() {
+    int m = 0;
+    for (int i = 0; i < n; ++i) m = r(i) > m ? r(i) : m;
+    return m;
+  }
+};
+
+// Threads per transform of a length-L core whose largest radix is rmax: one
+// butterfly of the largest radix per thread, rounded up to a power of two
+// below 32 and to a multiple of 32 above (the executor's rule).
+FFB_HD constexpr int tpt_of(int L, int rmax) {
+  const int t = (L + rmax - 1) / rmax;
+  if (t <= 32) {
+    int p = 1;
+    while (p < t) p <<= 1;
+    return p;
+  }
+  return (t + 31) / 32 * 32;
+}
+
+// Thread policy: DevT runs a phase's body once as this CUDA thread; HostT
+// (host emulation of the index arithmetic) runs it for every thread in turn.
+struct DevT {
+  template <class F>
+  FFB_HD void each(int, F &&f) const {
+#ifdef __CUDA_ARCH__
+    f((int)threadIdx.x);
+#else
+    (void)f;
+#endif
+  }
+  FFB_HD void sync() const {
+#ifdef __CUDA_ARCH__
+    __syncthreads();
+#endif
+  }
+};
+struct HostT {
+  template <class F>
+  FFB_HD void each(int nthr, F &&f) const {
+    for (int t = 0; t < nthr; ++t) f(t);
+  }
+  FFB_HD void sync() const {}
+};
+
+// Ping-pong buffer access: get reads elements j + r * S (r < R), put writes
+// elements base + q * S.
+template <typename T>
+struct SmemIO {
+  cpx<T> *b;
+  template <int S, int R>
+  FFB_HD void get(int j, cpx<T> (&x)[R]) const {
+    if constexpr (S % 16 == 0) {
+      const cpx<T> *p = b + pp_pos(j);
+#pragma unroll
+      for (int r = 0; r < R; ++r) x[r] = p[r * (S + S / 16)];
+    } else {
+#pragma unroll
+      for (int r = 0; r < R; ++r) x[r] = b[pp_pos(j + r * S)];
+    }
+  }
+  template <int S, int R>
+  FFB_HD void put(int base, const cpx<T> (&x)[R]) const {
+    if constexpr (S % 16 == 0) {
+      cpx<T> *p = b + pp_pos(base);
+#pragma unroll
+      for (int q = 0; q < R; ++q) p[q * (S + S / 16)] = x[q];
+    } else if constexpr (S == 1 && 16 % R == 0) {
+      cpx<T> *p = b + pp_pos(base);  // base is a multiple of R: R positions inside one 16-block
+#pragma unroll
+      for (int q = 0; q < R; ++q) p[q] = x[q];
+    } else {
+#pragma unroll
+      for (int q = 0; q < R; ++q) b[pp_pos(base + q * S)] = x[q];
+    }
+  }
+};
+
+// Last forward stage of a convolution: output k (natural order) times the
+// kernel spectrum entry k, into the ping-pong buffer.
+template <typename T>
+struct SmemKernIO {
+  cpx<T> *b;
+  const cpx<T> *kern;
+  template <int S, int R>
+  FFB_HD void put(int base, const cpx<T> (&x)[R]) const {
+    cpx<T> y[R];
+#pragma unroll
+    for (int q = 0; q < R; ++q) y[q] = cmul(x[q], ldg_c(kern + base + q * S));
+    SmemIO<T>{b}.template put<S, R>(base, y);
+  }
+};
+
+// Four-step post-twiddle W_N^{g k} (conjugated for the inverse) from the two
+// split tables, m = g * k < N.
+template <typename T>
+FFB_HD cpx<T> post_twiddle(const TileArgs<T> &a, cpx<T> v, long long g, int k) {
+  const uint32_t m = (uint32_t)(g * (long long)k);
+  const uint32_t hi = fdiv(m, a.ptw_div);
+  const uint32_t lo = m - hi * a.ptw_div.d;
+  cpx<T> t = cmul(ldg_c(a.ptw_hi + hi), ldg_c(a.ptw_lo + lo));
+  if (a.inv) t.y = -t.y;
+  return cmul(v, t);
+}
+
+// First stage's reader: element i of the row in global memory, with the
+// pass kind's load-side factor (KIND 1: chirp, zero past n; KIND 0 with
+// chirp_mode 1: chirp at j = i * cj_e + g * cj_g, zero past n).
+template <typename T, int KIND>
+struct GlobalIn {
+  const TileArgs<T> *a;
+  const cpx<T> *row;
+  long long g;
+  template <int S, int R>
+  FFB_HD void get(int j, cpx<T> (&x)[R]) const {
+    if constexpr (KIND == 1) {
+      const int n = a->n;
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const int i = j + r * S;
+        x[r] = i < n ? cmul(ldg_c(row + i), ldg_c(a->chirp + i)) : mk((T)0, (T)0);
+      }
+    } else if constexpr (KIND == 0) {
+      if (a->chirp_mode == 1) {
+        const long long n = a->n;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const int i = j + r * S;
+          const long long c = (long long)i * a->cj_e + g * a->cj_g;
+          x[r] = c < n ? cmul(ldg_c(row + i), ldg_c(a->chirp + c)) : mk((T)0, (T)0);
+        }
+      } else {
+#pragma unroll
+        for (int r = 0; r < R; ++r) x[r] = ldg_c(row + j + r * S);
+      }
+    } else {
+#pragma unroll
+      for (int r = 0; r < R; ++r) x[r] = ldg_c(row + j + r * S);
+    }
+  }
+};
+
+// Last stage's writer: output k of the row to global memory, with the pass
+// kind's store-side factor (KIND 1: chirp, only k < n; KIND 0 with
+// chirp_mode 2: chirp at j = k * cj_e + g * cj_g, only j < n; otherwise the
+// optional four-step post-twiddle).  Nothing is written for a dead row.
+template <typename T, int KIND>
+struct GlobalOut {
+  const TileArgs<T> *a;
+  cpx<T> *row;
+  long long g;
+  bool live;
+  template <int S, int R>
+  FFB_HD void put(int base, const cpx<T> (&x)[R]) const {
+    if (!live) return;
+    const bool ptw = a->post_twiddle != 0;
+    if constexpr (KIND == 1) {
+      const int n = a->n;
+#pragma unroll
+      for (int q = 0; q < R; ++q) {
+        const int k = base + q * S;
+        if (k < n) {
+          cpx<T> v = cmul(x[q], ldg_c(a->chirp + k));
+          row[k] = ptw ? post_twiddle(*a, v, g, k) : v;
+        }
+      }
+    } else {
+      if (KIND == 0 && a->chirp_mode == 2) {
+        const long long n = a->n;
+#pragma unroll
+        for (int q = 0; q < R; ++q) {
+          const int k = base + q * S;
+          const long long c = (long long)k * a->cj_e + g * a->cj_g;
+          if (c < n) row[k] = cmul(x[q], ldg_c(a->chirp + c));
+        }
+      } else if (ptw) {
+#pragma unroll
+        for (int q = 0; q < R; ++q) row[base + q * S] = post_twiddle(*a, x[q], g, base + q * S);
+      } else {
+#pragma unroll
+        for (int q = 0; q < R; ++q) row[base + q * S] = x[q];
+      }
+    }
+  }
+};
+
+// Stockham stage with span Ns and radix R of a length-L transform for the
+// butterflies of one thread (j = t, t + TPT, ... < L/R): inputs j + r L/R
+// from rd, twiddles W_{Ns R}^{r (j mod Ns)} from the stage block, outputs
+// (j - j mod Ns) R + j mod Ns + q Ns to wr.
+template <typename T, bool INV, int L, int TPT, int Ns, int R, class Rd, class Wr>
+FFB_HD void row_stage(int t, const cpx<T> *__restrict__ blk, const Rd &rd, const Wr &wr) {
+  constexpr int nb = L / R;
+  constexpr int V = (nb + TPT - 1) / TPT;
+#pragma unroll
+  for (int v = 0; v < V; ++v) {
+    const int j = t + v * TPT;
+    if (nb % TPT == 0 || j < nb) {
+      const int k = Ns == 1 ? 0 : j % Ns;
+      cpx<T> x[R];
+      rd.template get<nb, R>(j, x);
+      if constexpr (Ns > 1) {
+        const cpx<T> *row = blk + k;
+#pragma unroll
+        for (int r = 1; r < R; ++r) x[r] = cmul(x[r], ldg_c(row + (r - 1) * Ns));
+      }
+      dft_fixed<R, INV, T>(x);
+      wr.template put<Ns, R>((j - k) * R + k, x);
+    }
+  }
+}
+
+// Stages S.. of sequence Q.  Stage s reads ping-pong buffer (P + s - 1) & 1
+// and writes (P + s) & 1 of its row's slot; stage 0 reads through
+// first(w, t, in_buf) instead, the last stage writes through
+// last(w, t, out_buf).  A barrier separates consecutive stages; none follows
+// the last.
+template <typename T, bool INV, int L, int TPT, class Q, int P, int S, class X, class First, class Last>
+FFB_HD void run_chain(const X &x, int nthr, const cpx<T> *__restrict__ tw, cpx<T> *sm, const First &first,
+                      const Last &last) {
+  if constexpr (S < Q::n) {
+    constexpr int R = Q::r(S), Ns = Q::span(S), TwOff = Q::twoff(S);
+    constexpr int Lq = pp_size(L), slot = 2 * Lq + 3;
+    x.each(nthr, [&](int tid) FFB_INL {
+      const int w = tid / TPT, t = tid - w * TPT;
+      cpx<T> *const b0 = sm + w * slot;
+      cpx<T> *const bin = ((P + S - 1) & 1) ? b0 + Lq : b0;
+      cpx<T> *const bout = ((P + S) & 1) ? b0 + Lq : b0;
+      if constexpr (S == 0 && S == Q::n - 1) {
+        row_stage<T, INV, L, TPT, Ns, R>(t, tw + TwOff, first(w, bin), last(w, bout));
+      } else if constexpr (S == 0) {
+        row_stage<T, INV, L, TPT, Ns, R>(t, tw + TwOff, first(w, bin), SmemIO<T>{bout});
+      } else if constexpr (S == Q::n - 1) {
+        row_stage<T, INV, L, TPT, Ns, R>(t, tw + TwOff, SmemIO<T>{bin}, last(w, bout));
+      } else {
+        row_stage<T, INV, L, TPT, Ns, R>(t, tw + TwOff, SmemIO<T>{bin}, SmemIO<T>{bout});
+      }
+    });
+    if constexpr (S + 1 < Q::n) {
+      x.sync();
+      run_chain<T, INV, L, TPT, Q, P, S + 1>(x, nthr, tw, sm, first, last);
+    }
+  }
+}
+
+// One CTA tile of W rows (W = blockDim / TPT): KIND 0 a Dit transform in
+// direction INV, KIND 1 the fused Bluestein chain, KIND 3 a convolution row
+// (forward core, kernel product, inverse core2).
+template <typename T, int KIND, bool INV, int L, int TPT, class X, int... Rs>
+FFB_HD void rows_body(const TileArgs<T> &a, long long bx, long long by, cpx<T> *sm, const X &x) {
+  using Q = Seq<Rs...>;
+  const int W = a.W;
+  const int nthr = W * TPT;
+  const long long g0 = bx * W;
+  const int wlive = (int)((a.G - g0) < W ? (a.G - g0) : W);
+  const cpx<T> *in = reinterpret_cast<const cpx<T> *>(a.in) + by * a.ib + g0 * a.ig;
+  cpx<T> *out = reinterpret_cast<cpx<T> *>(a.out) + by * a.ob + g0 * a.og;
+  const TileArgs<T> *ap = &a;
+  // dead rows of the last tile compute on the last live row's data and store nothing
+  auto first = [&](int w, cpx<T> *) FFB_INL {
+    const int wc = w < wlive ? w : wlive - 1;
+    return GlobalIn<T, KIND>{ap, in + wc * a.ig, g0 + wc};
+  };
+  auto last = [&](int w, cpx<T> *) FFB_INL {
+    return GlobalOut<T, KIND>{ap, out + w * a.og, g0 + w, w < wlive};
+  };
+  if constexpr (KIND == 0) {
+    run_chain<T, INV, L, TPT, Q, 0, 0>(x, nthr, a.tw, sm, first, last);
+  } else {
+    auto kern_last = [&](int w, cpx<T> *bout) FFB_INL {
+      const cpx<T> *kern = a.kern;
+      if constexpr (KIND == 3) {
+        const int wc = w < wlive ? w : wlive - 1;
+        kern += (g0 + wc) * a.kern_stride;
+      }
+      return SmemKernIO<T>{bout, kern};
+    };
+    auto smem_first = [&](int, cpx<T> *bin) FFB_INL { return SmemIO<T>{bin}; };
+    run_chain<T, false, L, TPT, Q, 0, 0>(x, nthr, a.tw, sm, first, kern_last);
+    x.sync();
+    run_chain<T, true, L, TPT, Q, Q::n, 0>(x, nthr, a.tw2, sm, smem_first, last);
+  }
+}
+
+template <typename T, int KIND, bool INV, int L, int... Rs>
+__global__ void __launch_bounds__(tile::TileBounds<T>::kMaxThreads) k_rows(const __grid_constant__ TileArgs<T> a) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  constexpr int TPT = tpt_of(L, Seq<Rs...>::rmax());
+  rows_body<T, KIND, INV, L, TPT, DevT, Rs...>(a, (long long)blockIdx.x, (long long)blockIdx.y,
+                                               reinterpret_cast<cpx<T> *>(smraw), DevT{});
+}
+
+// True when the pass can run as rows of this sequence: contiguous rows on
+// both sides, the executor's threads per transform, and (convolutions) the
+// same sequence for the inverse core.
+template <typename T, int KIND, int L, int... Rs>
+FFB_HD bool rows_fit(const TileArgs<T> &a) {
+  constexpr int TPT = tpt_of(L, Seq<Rs...>::rmax());
+  return a.pp && !a.wfast && a.ii == 1 && a.ok == 1 && a.tpt == TPT &&
+         a.W * TPT <= tile::TileBounds<T>::kMaxThreads && tile::core_is<L, Rs...>(a.core) &&
+         (KIND == 0 || tile::core_is<L, Rs...>(a.core2));
+}
+
+#ifndef FFB_HOST_EMULATION
+template <typename T, int KIND, bool INV, int L, int... Rs>
+cudaError_t launch_rows(const TileArgs<T> &a, size_t smem, cudaStream_t s) {
+  static bool configured = false;
+  if (!configured) {
+    cudaError_t e =
+        cudaFuncSetAttribute(k_rows<T, KIND, INV, L, Rs...>, cudaFuncAttributeMaxDynamicSharedMemorySize, 232448);
+    if (e != cudaSuccess) return e;
+    configured = true;
+  }
+  constexpr int TPT = tpt_of(L, Seq<Rs...>::rmax());
+  dim3 grid((unsigned)((a.G + a.W - 1) / a.W), (unsigned)a.nbatch, 1);
+  dim3 block((unsigned)(a.W * TPT), 1, 1);
+  k_rows<T, KIND, INV, L, Rs...><<<grid, block, smem, s>>>(a);
+  return cudaGetLastError();
+}
+#else
+template <typename T, int KIND, bool INV, int L, int... Rs>
+cudaError_t launch_rows(const TileArgs<T> &a, size_t smem, cudaStream_t) {
+  constexpr int TPT = tpt_of(L, Seq<Rs...>::rmax());
+  std::vector<unsigned char> buf(smem + 64);
+  cpx<T> *sm = reinterpret_cast<cpx<T> *>(buf.data());
+  const long long tiles = (a.G + a.W - 1) / a.W;
+  for (long long by = 0; by < a.nbatch; ++by)
+    for (long long bx = 0; bx < tiles; ++bx) {
+      std::memset(buf.data(), 0xff, buf.size());
+      rows_body<T, KIND, INV, L, TPT, HostT, Rs...>(a, bx, by, sm, HostT{});
+    }
+  return cudaSuccess;
+}
+#endif
+
+// Launches the row kernel of the pass's sequence; cudaErrorNotSupported when
+// the pass is not rows of a compile-time sequence.
+template <typename T, int KIND, bool INV>
+cudaError_t launch_rows_any(const TileArgs<T> &a, size_t smem, cudaStream_t s) {
+#define FFB_TRY_ROWS(L, ...) \
+  if (rows_fit<T, KIND, L, __VA_ARGS__>(a)) return launch_rows<T, KIND, INV, L, __VA_ARGS__>(a, smem, s);
+  FFB_FIXED_SEQUENCES(FFB_TRY_ROWS)
+#undef FFB_TRY_ROWS
+  return cudaErrorNotSupported;
+}
+
+}  // namespace rows
+}  // namespace ffb
