@@ -237,21 +237,40 @@ double chain_cost(int64_t m, std::vector<int> *radices, std::unordered_map<int64
   return cost;
 }
 
+// The compile-time radix sequence of length L (FFB_FIXED_SEQUENCES), if it
+// has one: such a length runs on a row kernel with every index constant.
+bool fixed_sequence(int64_t L, std::vector<int> *r) {
+#define FFB_SEQ(len, ...)        \
+  if (L == (len)) {              \
+    if (r) *r = {__VA_ARGS__};   \
+    return true;                 \
+  }
+  FFB_FIXED_SEQUENCES(FFB_SEQ)
+#undef FFB_SEQ
+  return false;
+}
+
+// Cost weight of a length with a compile-time sequence against the chain
+// cost model (its row kernel ran 1.4-2x faster than the runtime-sequence
+// kernel at 1701, 2048 and 4096 on B200).
+constexpr double kFixedWeight = 0.6;
+
 // On-chip convolution length for a length-n Bluestein: the M in
-// [2n - 1, maxL] with the least M x chain cost; 0 if none fits.
+// [2n - 1, maxL] with the least M x chain cost (weighted for compile-time
+// sequences); 0 if none fits.
 int64_t choose_conv_length(int64_t n, int64_t maxL, std::vector<int> *radices) {
   std::unordered_map<int64_t, std::pair<double, int>> memo;
   int64_t best_m = 0;
   double best = 1e30;
   const int64_t lo = 2 * n - 1, hi = std::min<int64_t>(maxL, 2 * lo + 64);
   for (int64_t m = lo; m <= hi; ++m) {
-    const double c = (double)m * chain_cost(m, nullptr, memo);
+    const double c = (double)m * chain_cost(m, nullptr, memo) * (fixed_sequence(m, nullptr) ? kFixedWeight : 1.0);
     if (c < best) {
       best = c;
       best_m = m;
     }
   }
-  if (best_m) chain_cost(best_m, radices, memo);
+  if (best_m && !fixed_sequence(best_m, radices)) chain_cost(best_m, radices, memo);
   return best_m;
 }
 
@@ -267,7 +286,8 @@ int64_t choose_split_conv(int64_t n, int64_t maxL, int64_t *n1_out, std::vector<
   for (int64_t m = lo; m <= hi; ++m)
     for (int n1 : kCols) {
       if (m % n1 || m / n1 > maxL) continue;
-      const double c = (double)m * chain_cost(m / n1, nullptr, memo);
+      const double c =
+          (double)m * chain_cost(m / n1, nullptr, memo) * (fixed_sequence(m / n1, nullptr) ? kFixedWeight : 1.0);
       if (c < best) {
         best = c;
         best_m = m;
@@ -276,7 +296,7 @@ int64_t choose_split_conv(int64_t n, int64_t maxL, int64_t *n1_out, std::vector<
     }
   if (best_m) {
     *n1_out = best_n1;
-    chain_cost(best_m / best_n1, row_radices, memo);
+    if (!fixed_sequence(best_m / best_n1, row_radices)) chain_cost(best_m / best_n1, row_radices, memo);
   }
   return best_m;
 }
@@ -388,13 +408,15 @@ class Builder {
     }
     auto r = flatten(node);
     if (!r.empty() && node->length <= maxL) {
+      fixed_sequence(node->length, &r);  // the same DFT on the compile-time sequence
       spec = {CoreKind::Dit, node->length, node->length, r, node};
       return true;
     }
     // a tree whose nodes do not flatten into one radix chain (a four-step
     // over Bluestein / Rader children): the executor's own chain when the
     // length has one and fits
-    if (node->kind == NodeKind::FourStep && node->length <= maxL && radix_chain(node->length, &r)) {
+    if (node->kind == NodeKind::FourStep && node->length <= maxL &&
+        (fixed_sequence(node->length, &r) || radix_chain(node->length, &r))) {
       spec = {CoreKind::Dit, node->length, node->length, r, node};
       return true;
     }

@@ -5,6 +5,7 @@
 #include <cstring>
 
 #include "kernels.cuh"
+#include "rows.cuh"
 
 namespace ffb {
 
@@ -203,6 +204,20 @@ cudaError_t launch_tile(const TileArgs<T> &a, CoreKind kind, IoKind io, size_t s
   return cudaErrorInvalidValue;
 }
 
+template <typename T>
+size_t tile_smem(const TileArgs<T> &a, CoreKind kind, IoKind io, size_t smem) {
+  const int k = (int)kind;
+  if (a.regcol) return 0;
+  if (a.pp && io == IoKind::C2C && (k == 0 || k == 1 || k == 3)) {
+    const size_t r = k == 0 ? rows::rows_smem_any<T, 0>(a) : k == 1 ? rows::rows_smem_any<T, 1>(a)
+                                                                     : rows::rows_smem_any<T, 3>(a);
+    if (r) return r;
+  }
+  return smem;
+}
+
+template size_t tile_smem<float>(const TileArgs<float> &, CoreKind, IoKind, size_t);
+template size_t tile_smem<double>(const TileArgs<double> &, CoreKind, IoKind, size_t);
 template cudaError_t launch_tile<float>(const TileArgs<float> &, CoreKind, IoKind, size_t, cudaStream_t);
 template cudaError_t launch_tile<double>(const TileArgs<double> &, CoreKind, IoKind, size_t, cudaStream_t);
 

@@ -32,6 +32,20 @@ enum class IoKind : int {
 // Transform g of outer batch b reads element i at  in + b*ib + g*ig + i*ii
 // and writes element k at                          out + b*ob + g*og + k*ok
 // (units: elements of the pass's input / output type).
+// The compile-time radix sequences with their own kernels: radix-16 chains
+// of the power-of-two lengths 128..8192 (one smaller radix last), and the
+// mixed-radix 1701 = 9 * 9 * 7 * 3.  The executor runs a length that has one
+// on it (and prefers such lengths for convolutions).
+#define FFB_FIXED_SEQUENCES(X)        \
+  X(1701, 9, 9, 7, 3)                 \
+  X(128, 16, 8)                       \
+  X(256, 16, 16)                      \
+  X(512, 16, 16, 2)                   \
+  X(1024, 16, 16, 4)                  \
+  X(2048, 16, 16, 8)                  \
+  X(4096, 16, 16, 16)                 \
+  X(8192, 16, 16, 16, 2)
+
 template <typename T>
 struct TileArgs {
   const void *in;
@@ -105,6 +119,10 @@ cudaError_t launch_real_pre(const cpx<T> *x, cpx<T> *z, long long batch, long lo
 
 template <typename T>
 cudaError_t launch_tile(const TileArgs<T> &a, CoreKind kind, IoKind io, size_t smem_bytes, cudaStream_t stream);
+// Dynamic shared memory the launch of a tile pass uses (the row kernels of
+// the compile-time sequences take less than the pass's general figure).
+template <typename T>
+size_t tile_smem(const TileArgs<T> &a, CoreKind kind, IoKind io, size_t smem_bytes);
 
 // Register column pass (TileArgs::regcol); defined in regcol.cu.
 template <typename T>

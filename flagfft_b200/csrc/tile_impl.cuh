@@ -576,19 +576,6 @@ cudaError_t launch_pp_fixed(const TileArgs<T> &a, size_t smem, cudaStream_t) {
 }
 #endif
 
-// The compile-time radix sequences with their own kernels: radix-16 chains
-// of the power-of-two lengths 128..8192 (one smaller radix last), and the
-// mixed-radix 1701 = 9 * 9 * 7 * 3.
-#define FFB_FIXED_SEQUENCES(X)        \
-  X(1701, 9, 9, 7, 3)                 \
-  X(128, 16, 8)                       \
-  X(256, 16, 16)                      \
-  X(512, 16, 16, 2)                   \
-  X(1024, 16, 16, 4)                  \
-  X(2048, 16, 16, 8)                  \
-  X(4096, 16, 16, 16)                 \
-  X(8192, 16, 16, 16, 2)
-
 // Launches the fixed-sequence kernel matching the pass's core (and core2 for
 // convolutions); cudaErrorNotSupported when none matches.
 template <typename T, int KIND, bool INV>
