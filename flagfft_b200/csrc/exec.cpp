@@ -642,25 +642,8 @@ class Builder {
     });
   }
 
-  // Four-step post-twiddle W_N^m: one table of all N roots up to
-  // kFullTwiddleMax (one load per element), else hi[m / split] * lo[m % split]
-  // with split ~ sqrt(N).
-  static constexpr int64_t kFullTwiddleMax = 1 << 16;
+  // Four-step post-twiddle W_N^m = hi[m / split] * lo[m % split].
   void set_post_twiddle(TileArgs<T> &a, int64_t N) {
-    if (N <= kFullTwiddleMax) {
-      a.post_twiddle = 1;
-      a.ptw_lo = cached<cpx<T>>("ptwfull|" + std::to_string(N), [&]() {
-        std::vector<cpx<T>> w((size_t)N);
-        for (int64_t m = 0; m < N; ++m) {
-          cld r = unit_root(m, N, -1);
-          w[(size_t)m] = mk((T)r.real(), (T)r.imag());
-        }
-        return w;
-      });
-      a.ptw_hi = nullptr;
-      a.ptw_div = make_fastdiv((uint32_t)N);
-      return;
-    }
     const int64_t split = (int64_t)std::ceil(std::sqrt((double)N));
     const int64_t nhi = (N + split - 1) / split;
     a.post_twiddle = 1;

@@ -69,8 +69,7 @@ struct TileArgs {
   const int *perm_out;  // Rader: q -> g^q mod p
   const cpx<T> *rtw;    // real-transform twiddles W_n^k, k <= n/2 (IoKind R2C / C2R)
   // optional post-twiddle of a four-step column pass: output k of transform g
-  // is multiplied by W_N^{g*k} = hi[m / split] * lo[m % split], m = g*k < N;
-  // ptw_hi null: lo holds all N roots (four_step_twiddle)
+  // is multiplied by W_N^{g*k} = hi[m / split] * lo[m % split], m = g*k < N
   int post_twiddle;
   const cpx<T> *ptw_lo;
   const cpx<T> *ptw_hi;
@@ -93,14 +92,6 @@ struct TileArgs {
   // C2C, transforms contiguous in memory on both sides: ig == og == 1).
   int regcol;
 };
-
-// W_N^m (forward sign) of a pass's four-step twiddle tables.
-template <typename T>
-FFB_HD cpx<T> four_step_twiddle(const TileArgs<T> &a, uint32_t m) {
-  if (!a.ptw_hi) return ldg_c(a.ptw_lo + m);
-  const uint32_t hi = fdiv(m, a.ptw_div);
-  return cmul(ldg_c(a.ptw_hi + hi), ldg_c(a.ptw_lo + (m - hi * a.ptw_div.d)));
-}
 
 // Real-transform pre/post processing between the passes of a multi-pass
 // R2C / C2R (L = n/2 complex points per transform, rtw[k] = W_n^k, k <= L):

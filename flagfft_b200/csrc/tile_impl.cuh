@@ -226,7 +226,9 @@ FFB_HD void tile_body(const TileArgs<T> &a, long long bx, long long by, cpx<T> *
   auto post_twiddle = [&](cpx<T> v, long long g, int k) FFB_INL -> cpx<T> {
     if (!a.post_twiddle) return v;
     const uint32_t m = (uint32_t)(g * (long long)k);
-    cpx<T> t = four_step_twiddle(a, m);
+    const uint32_t hi = fdiv(m, a.ptw_div);
+    const uint32_t lo = m - hi * a.ptw_div.d;
+    cpx<T> t = cmul(ldg_c(a.ptw_hi + hi), ldg_c(a.ptw_lo + lo));
     if (a.inv) t.y = -t.y;
     return cmul(v, t);
   };
@@ -462,7 +464,9 @@ FFB_HD void tile_body_pp(const TileArgs<T> &a, long long bx, long long by, cpx<T
   auto post_twiddle = [&](cpx<T> v, long long g, int k) FFB_INL -> cpx<T> {
     if (!a.post_twiddle) return v;
     const uint32_t m = (uint32_t)(g * (long long)k);
-    cpx<T> t = four_step_twiddle(a, m);
+    const uint32_t hi = fdiv(m, a.ptw_div);
+    const uint32_t lo = m - hi * a.ptw_div.d;
+    cpx<T> t = cmul(ldg_c(a.ptw_hi + hi), ldg_c(a.ptw_lo + lo));
     if (a.inv) t.y = -t.y;
     return cmul(v, t);
   };
