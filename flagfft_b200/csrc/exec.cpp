@@ -274,10 +274,12 @@ int64_t choose_conv_length(int64_t n, int64_t maxL, std::vector<int> *radices) {
   return best_m;
 }
 
-// Three-pass convolution M = n1 * n2: n1 one codelet (the register-column
-// passes), n2 on chip (the convolution rows).  Minimises M x chain cost of n2
-// (the column passes cost about the same for every n1).
-int64_t choose_split_conv(int64_t n, int64_t maxL, int64_t *n1_out, std::vector<int> *row_radices) {
+// Four-step convolution M = n1 * n2: n1 one codelet (the column passes), n2
+// on chip (the convolution rows).  Minimises M x chain cost of n2 (the column
+// passes cost about the same for every n1), weighted for compile-time row
+// sequences and, when `one_pass`, for the shapes the one-pass kernel runs.
+constexpr double kOnePassWeight = 0.35;
+int64_t choose_split_conv(int64_t n, int64_t maxL, bool one_pass, int64_t *n1_out, std::vector<int> *row_radices) {
   std::unordered_map<int64_t, std::pair<double, int>> memo;
   static const int kCols[] = {16, 15, 13, 12, 11, 10, 9, 8};
   int64_t best_m = 0, best_n1 = 0;
@@ -286,8 +288,10 @@ int64_t choose_split_conv(int64_t n, int64_t maxL, int64_t *n1_out, std::vector<
   for (int64_t m = lo; m <= hi; ++m)
     for (int n1 : kCols) {
       if (m % n1 || m / n1 > maxL) continue;
-      const double c =
-          (double)m * chain_cost(m / n1, nullptr, memo) * (fixed_sequence(m / n1, nullptr) ? kFixedWeight : 1.0);
+      const bool fixed = fixed_sequence(m / n1, nullptr);
+      const double c = (double)m * chain_cost(m / n1, nullptr, memo) *
+                       (one_pass && fixed && blue4_shape(n1, (int)(m / n1)) ? kOnePassWeight
+                                                                             : fixed ? kFixedWeight : 1.0);
       if (c < best) {
         best = c;
         best_m = m;
@@ -806,7 +810,29 @@ void lower_c2c(Builder<T> &bld, Program &prog, const NodePtr &root, bool inverse
     // fused (src/exec/raw_nodes.cpp:153-204 runs the same chain as 7 launches).
     int64_t n1 = 0;
     std::vector<int> row_radices;
-    const int64_t M = choose_split_conv(n, max_onchip_length(sizeof(T) == 8), &n1, &row_radices);
+    const bool one_pass_ok = sizeof(T) == 4;
+    const int64_t M = choose_split_conv(n, max_onchip_length(sizeof(T) == 8), one_pass_ok, &n1, &row_radices);
+    std::vector<int> seq;
+    if (M && one_pass_ok && blue4_shape((int)n1, (int)(M / n1)) && fixed_sequence(M / n1, &seq) &&
+        seq == row_radices) {
+      // the whole chain in one CTA per transform: n1 rows of n2 points in
+      // shared memory (blue4.cuh)
+      const int64_t n2 = M / n1;
+      CoreSpec sc{CoreKind::Conv, n2, n2, row_radices, nullptr};
+      auto *p = bld.add_pass(sc, IoKind::C2C, true, batch, 1, idist, 0, 1, odist, 0, 1, src, dst, n);
+      TileArgs<T> &a = p->a;
+      a.blue_cols = (int)n1;
+      a.G = 1;
+      a.W = 1;
+      a.n = (int)n;
+      a.chirp = bld.table_chirp(n, inverse);
+      a.kern = bld.table_bluestein_rows(n, row_radices, n1, n2, inverse, true);
+      a.kern_stride = n2;
+      bld.set_post_twiddle(a, M);
+      p->smem = blue4_smem((int)n1, (int)n2, sizeof(cpx<T>));
+      p->note = "bluestein one pass: " + std::to_string(n1) + " x " + std::to_string(n2) + " four-step in one CTA";
+      return;
+    }
     if (M) {
       const int64_t n2 = M / n1;
       const CoreSpec sa{CoreKind::Dit, n1, n1, {(int)n1}, nullptr};
@@ -1343,7 +1369,7 @@ std::unique_ptr<BatchProgram> lower_batch_t(const std::vector<BatchGroup> &group
   for (auto &g : bp->groups)
     for (auto &ps : g.prog->passes) {
       auto *tp = dynamic_cast<TilePass<T> *>(ps.get());
-      if (!tp || !tp->a.pp || tp->a.regcol || tp->a.tpt > kBatchWidth) continue;
+      if (!tp || !tp->a.pp || tp->a.regcol || tp->a.blue_cols || tp->a.tpt > kBatchWidth) continue;
       TileArgs<T> &a = tp->a;
       const size_t per = tp->smem / (size_t)a.W;
       int64_t W = std::min<int64_t>({(int64_t)(kBatchWidth / a.tpt), (int64_t)a.G,
@@ -1367,7 +1393,7 @@ std::unique_ptr<BatchProgram> lower_batch_t(const std::vector<BatchGroup> &group
       if (auto *tp = dynamic_cast<const TilePass<T> *>(g.prog->passes[pi].get())) {
         if (tp->a.regcol) {
           kind = kBatchRegcol;
-        } else if (tp->a.pp && tp->io == IoKind::C2C) {
+        } else if (tp->a.pp && !tp->a.blue_cols && tp->io == IoKind::C2C) {
           kind = tp->kind == CoreKind::Dit         ? kBatchPpDit
                  : tp->kind == CoreKind::Bluestein ? kBatchPpBluestein
                  : tp->kind == CoreKind::Rader     ? kBatchPpRader

@@ -70,12 +70,13 @@ struct TilePass final : PassBase {
 
   std::string describe() const override {
     std::ostringstream o;
-    o << (a.regcol ? "register-columns" : kind_name(kind)) << "/" << io_name(io) << " "
+    o << (a.regcol ? "register-columns" : a.blue_cols ? "bluestein-four-step" : kind_name(kind)) << "/" << io_name(io)
+      << " "
       << (sizeof(T) == 4 ? "f32" : "f64") << " L=" << a.core.L
       << " radices=[";
     for (int s = 0; s < a.core.nst; ++s) o << (s ? "," : "") << a.core.radix[s];
     o << "] n=" << a.n << " transforms=" << a.nbatch << "x" << a.G << " per_cta=" << a.W
-      << " threads=" << a.W * a.tpt << " smem=" << tile_smem<T>(a, kind, io, smem) << " " << buf_name(src) << "->"
+      << " threads=" << (a.blue_cols ? blue4_threads(a.blue_cols, a.core.L) : a.W * a.tpt) << " smem=" << tile_smem<T>(a, kind, io, smem) << " " << buf_name(src) << "->"
       << buf_name(dst);
     if (a.post_twiddle) o << " +twiddle";
     if (!note.empty()) o << " (" << note << ")";

@@ -46,6 +46,22 @@ enum class IoKind : int {
   X(4096, 16, 16, 16)                 \
   X(8192, 16, 16, 16, 2)
 
+// Shapes (N1 rows of an L2-point compile-time sequence) of the one-pass
+// four-step Bluestein kernel (blue4.cuh), single precision: the N1 padded
+// rows fit one CTA's shared memory.
+#define FFB_BLUE4_SHAPES(X)                                                                              \
+  X(8, 2048, 16, 16, 8) X(9, 2048, 16, 16, 8) X(10, 2048, 16, 16, 8) X(11, 2048, 16, 16, 8)              \
+  X(12, 2048, 16, 16, 8) X(13, 2048, 16, 16, 8) X(13, 1024, 16, 16, 4) X(15, 1024, 16, 16, 4)            \
+  X(16, 1024, 16, 16, 4)
+
+inline bool blue4_shape(int n1, int L2) {
+#define FFB_B4_HAS(N1, L2_, ...) \
+  if (n1 == (N1) && L2 == (L2_)) return true;
+  FFB_BLUE4_SHAPES(FFB_B4_HAS)
+#undef FFB_B4_HAS
+  return false;
+}
+
 template <typename T>
 struct TileArgs {
   const void *in;
@@ -91,6 +107,9 @@ struct TileArgs {
   // one codelet in registers, no shared memory (Dit core with one stage,
   // C2C, transforms contiguous in memory on both sides: ig == og == 1).
   int regcol;
+  // > 0: one-pass four-step Bluestein (blue4.cuh) with this many columns
+  // (rows of the core's sequence); one CTA per transform.
+  int blue_cols;
 };
 
 // Real-transform pre/post processing between the passes of a multi-pass
@@ -123,6 +142,14 @@ cudaError_t launch_tile(const TileArgs<T> &a, CoreKind kind, IoKind io, size_t s
 // the compile-time sequences take less than the pass's general figure).
 template <typename T>
 size_t tile_smem(const TileArgs<T> &a, CoreKind kind, IoKind io, size_t smem_bytes);
+
+// One-pass four-step Bluestein (TileArgs::blue_cols); defined in
+// k_f32_blue4.cu (single precision only).
+template <typename T>
+cudaError_t launch_blue4(const TileArgs<T> &a, cudaStream_t stream);
+// Its dynamic shared memory and threads per CTA.
+size_t blue4_smem(int n1, int L2, size_t elem_bytes);
+int blue4_threads(int n1, int L2);
 
 // Register column pass (TileArgs::regcol); defined in regcol.cu.
 template <typename T>

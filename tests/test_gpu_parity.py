@@ -22,6 +22,9 @@ EXTRA = [2, 3, 5, 7, 11, 13, 17, 19, 6, 10, 12, 15, 1701, 2023, 10007, 20020, 65
 # twiddle applied in their stores), and a Rader prime whose p - 1 has a prime
 # factor above 19 (2099: p - 1 = 2 x 1049, run through a Bluestein core)
 COMPOSITE = [11573, 19549, 32980, 61423, 2099]
+# single-precision Bluestein lengths whose n1 x n2 four-step convolution runs
+# in one CTA per transform, one per shape (9..13 x 2048, 13 / 15 / 16 x 1024)
+ONE_PASS = [8213, 9221, 10243, 11279, 12301, 6491, 6659, 7688]
 
 
 def _ref_plan(plans, n, double):
@@ -74,6 +77,24 @@ def test_c2c_z2z_vs_oracle(ffb, torch_cuda, plans, n, double):
         ref = O.c2c(x.astype(np.complex128), direction, plan)
         est = None if double or n > 20020 else O.error_stats(O.c2c(x, direction, plan, precision="f32"), ref)
         _check(O.error_stats(got, ref), ftype, n, est)
+
+
+@pytest.mark.parametrize("n", ONE_PASS)
+def test_bluestein_one_pass_vs_oracle(ffb, torch_cuda, plans, n):
+    torch = torch_cuda
+    batch = 3
+    plan_ours = ffb.plan1d(n, ffb.C2C, batch)
+    try:
+        assert "bluestein-four-step" in plan_ours.description()
+    finally:
+        plan_ours.destroy()
+    x = O.random_complex(n * batch, O.accuracy_seed(O.C2C, n, batch), False).reshape(batch, n)
+    plan = _ref_plan(plans, n, False)
+    for direction in (-1, 1):
+        got = _run_c2c(ffb, torch, x, direction, False)
+        ref = O.c2c(x.astype(np.complex128), direction, plan)
+        est = O.error_stats(O.c2c(x, direction, plan, precision="f32"), ref)
+        _check(O.error_stats(got, ref), O.C2C, n, est)
 
 
 @pytest.mark.parametrize("scale", [2.0 ** -20, 1.0, 2.0 ** 20])
