@@ -743,6 +743,10 @@ class Builder {
 // HBM round trip more, but smaller, more numerous CTAs); "inplace" keeps
 // every transform that fits one CTA in one pass.
 thread_local int t_policy_override = -1;  // set while lowering batch groups
+// Set while lowering batch groups: the one-pass four-step Bluestein (its own
+// launch per group) gives way to the three-pass chain, whose passes join the
+// persistent launches.
+thread_local bool t_no_one_pass = false;
 
 static int onchip_policy() {
   if (t_policy_override >= 0) return t_policy_override;
@@ -810,7 +814,7 @@ void lower_c2c(Builder<T> &bld, Program &prog, const NodePtr &root, bool inverse
     // fused (src/exec/raw_nodes.cpp:153-204 runs the same chain as 7 launches).
     int64_t n1 = 0;
     std::vector<int> row_radices;
-    const bool one_pass_ok = sizeof(T) == 4;
+    const bool one_pass_ok = sizeof(T) == 4 && !t_no_one_pass;
     const int64_t M = choose_split_conv(n, max_onchip_length(sizeof(T) == 8), one_pass_ok, &n1, &row_radices);
     std::vector<int> seq;
     if (M && one_pass_ok && blue4_shape((int)n1, (int)(M / n1)) && fixed_sequence(M / n1, &seq) &&
@@ -1343,7 +1347,14 @@ std::unique_ptr<BatchProgram> lower_batch_t(const std::vector<BatchGroup> &group
     lay.batch = g.count;
     lay.idist = g.n;
     lay.odist = g.n;
-    grp.prog = lower_t<T>(root, planner, Transform::C2C, inverse, g.n, lay, false);
+    t_no_one_pass = true;
+    try {
+      grp.prog = lower_t<T>(root, planner, Transform::C2C, inverse, g.n, lay, false);
+    } catch (...) {
+      t_no_one_pass = false;
+      throw;
+    }
+    t_no_one_pass = false;
     // in-place passes cannot join a persistent launch: prefer a multi-pass lowering
     bool in_place = false;
     for (const auto &ps : grp.prog->passes) {
@@ -1352,13 +1363,16 @@ std::unique_ptr<BatchProgram> lower_batch_t(const std::vector<BatchGroup> &group
     }
     if (in_place) {
       t_policy_override = 2;
+      t_no_one_pass = true;
       try {
         grp.prog = lower_t<T>(root, planner, Transform::C2C, inverse, g.n, lay, false);
       } catch (...) {
         t_policy_override = -1;
+        t_no_one_pass = false;
         throw;
       }
       t_policy_override = -1;
+      t_no_one_pass = false;
     }
     bp->groups.push_back(std::move(grp));
   }
