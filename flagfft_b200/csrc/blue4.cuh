@@ -15,7 +15,8 @@
 // M-point workspace for the three-pass chain (src/exec/raw_nodes.cpp:153-204
 // runs the same chain as separate launches).  Row stages hold their values in
 // registers across a barrier between reads and writes; the rows are done in
-// two groups so that only half of the convolution is in registers at a time.
+// two groups so that only half of the convolution is in registers at a time
+// (row_pipe).
 #pragma once
 
 #include "rows.cuh"
@@ -37,7 +38,7 @@ FFB_HD cpx<T> split_twiddle(const TileArgs<T> &a, uint32_t m) {
 }
 
 // Shape of the kernel for N1 rows of sequence Rs...: TPT threads per row,
-// rows processed in groups of NR (two groups), NT threads in all.
+// rows processed in two groups of NR, NT threads in all.
 template <int N1, int L2, int... Rs>
 struct Shape {
   static constexpr int TPT = tpt_of(L2, Seq<Rs...>::rmax());
@@ -47,36 +48,57 @@ struct Shape {
   static constexpr int slot = slot_len<L2>();
 };
 
-// Stage S.. of the row FFTs of all N1 rows in direction INV; KERN: the last
-// stage multiplies by the kernel spectrum row before its writes.
-template <typename T, bool INV, bool KERN, int N1, int L2, class Q, int S, class Sh, class X>
-FFB_HD void row_chain(const X &x, const cpx<T> *__restrict__ tw, cpx<T> *sm, const cpx<T> *kern,
-                      long long kstride) {
-  if constexpr (S < Q::n) {
-    constexpr int R = Q::r(S), Ns = Q::span(S), TwOff = Q::twoff(S);
-    constexpr bool last = S == Q::n - 1;
-#pragma unroll 1
-    for (int grp = 0; grp < Sh::NG; ++grp) {
-      auto rd = [&](int tid) FFB_INL {
-        const int wr_ = grp * Sh::NR + tid / Sh::TPT, t = tid % Sh::TPT;
-        const int w = wr_ < N1 ? wr_ : N1 - 1;  // threads past the last row read a live row, write nothing
-        return rows::stage_read<T, INV, L2, Sh::TPT, Ns, R>(t, tw + TwOff, SmemIO<T>{sm + w * Sh::slot});
-      };
-      auto wr = [&](int tid, const rows::StageRegs<T, L2, Sh::TPT, R> &st) FFB_INL {
-        const int w = grp * Sh::NR + tid / Sh::TPT, t = tid % Sh::TPT;
-        if (w >= N1) return;
-        if constexpr (KERN && last) {
-          rows::stage_write<T, L2, Sh::TPT, Ns, R>(t, st, SmemKernIO<T>{sm + w * Sh::slot, kern + w * kstride});
-        } else {
-          rows::stage_write<T, L2, Sh::TPT, Ns, R>(t, st, SmemIO<T>{sm + w * Sh::slot});
-        }
-      };
-      // reads of this group, barrier, writes of this group (the next group's
-      // reads touch other rows, so they follow without a barrier)
-      x.each2(Sh::NT, rd, wr);
+// The row convolution as one pipeline of 2 x nst stages (nst forward, then
+// nst inverse; the last forward stage multiplies by the kernel spectrum row)
+// over two groups of rows.  Step k reads group k % 2 of stage k / 2; between
+// two barriers a thread writes what it read in the previous step and reads
+// the next group:  R(0,0) | W(0,0) R(0,1) | W(0,1) R(1,0) | ... | W(last,1).
+// A write and the read after it touch different row groups, and every read
+// of a group follows a barrier after that group's previous writes, so a
+// stage costs two barriers and a thread holds one group's values at a time.
+template <typename T, int N1, int L2, class Q, class Sh, int S>
+struct RowStage {
+  static constexpr int nst = Q::n;
+  static constexpr bool inv = S >= nst;
+  static constexpr int qs = inv ? S - nst : S;
+  static constexpr int R = Q::r(qs), Ns = Q::span(qs), TwOff = Q::twoff(qs);
+  using Regs = rows::StageRegs<T, L2, Sh::TPT, R>;
+
+  static FFB_HD Regs read(const TileArgs<T> &a, cpx<T> *sm, int grp, int tid) {
+    const int wr_ = grp * Sh::NR + tid / Sh::TPT, t = tid % Sh::TPT;
+    const int w = wr_ < N1 ? wr_ : N1 - 1;  // threads past the last row read a live row, write nothing
+    return rows::stage_read<T, inv, L2, Sh::TPT, Ns, R>(t, (inv ? a.tw2 : a.tw) + TwOff, SmemIO<T>{sm + w * Sh::slot});
+  }
+  static FFB_HD void write(const TileArgs<T> &a, cpx<T> *sm, int grp, int tid, const Regs &st) {
+    const int w = grp * Sh::NR + tid / Sh::TPT, t = tid % Sh::TPT;
+    if (w >= N1) return;
+    if constexpr (S == nst - 1) {
+      rows::stage_write<T, L2, Sh::TPT, Ns, R>(t, st, SmemKernIO<T>{sm + w * Sh::slot, a.kern + w * a.kern_stride});
+    } else {
+      rows::stage_write<T, L2, Sh::TPT, Ns, R>(t, st, SmemIO<T>{sm + w * Sh::slot});
     }
-    x.sync();
-    row_chain<T, INV, KERN, N1, L2, Q, S + 1, Sh>(x, tw, sm, kern, kstride);
+  }
+};
+
+// (host emulation instantiates it with per-thread state vectors)
+#pragma nv_exec_check_disable
+template <typename T, int N1, int L2, class Q, class Sh, int K, class X, class St>
+FFB_HD void row_pipe(const X &x, const TileArgs<T> &a, cpx<T> *sm, const St &st) {
+  static_assert(Sh::NG == 2, "the pipeline runs two row groups");
+  constexpr int P = K - 1;  // the step whose reads st holds
+  using Prev = RowStage<T, N1, L2, Q, Sh, P / 2>;
+  if constexpr (K == 4 * Q::n) {
+    x.last(Sh::NT, [&](int tid, const typename Prev::Regs &s) FFB_INL { Prev::write(a, sm, P % 2, tid, s); }, st);
+  } else {
+    using Cur = RowStage<T, N1, L2, Q, Sh, K / 2>;
+    auto nxt = x.step(
+        Sh::NT,
+        [&](int tid, const typename Prev::Regs &s) FFB_INL {
+          Prev::write(a, sm, P % 2, tid, s);
+          return Cur::read(a, sm, K % 2, tid);
+        },
+        st);
+    row_pipe<T, N1, L2, Q, Sh, K + 1>(x, a, sm, nxt);
   }
 }
 
@@ -84,6 +106,7 @@ FFB_HD void row_chain(const X &x, const cpx<T> *__restrict__ tw, cpx<T> *sm, con
 // core2 the row sequence with tables tw / tw2, kern the N1 x L2 kernel
 // spectrum rows (kern_stride = L2), chirp the n-point chirp, ptw_* the split
 // W_M tables, n the logical length, ib / ob the transform distances.
+#pragma nv_exec_check_disable
 template <typename T, int N1, int L2, class X, int... Rs>
 FFB_HD void blue4_body(const TileArgs<T> &a, long long by, cpx<T> *sm, const X &x) {
   using Q = Seq<Rs...>;
@@ -115,8 +138,12 @@ FFB_HD void blue4_body(const TileArgs<T> &a, long long by, cpx<T> *sm, const X &
   x.sync();
 
   // 2. row FFTs, kernel product, inverse row FFTs
-  row_chain<T, false, true, N1, L2, Q, 0, Sh>(x, a.tw, sm, a.kern, a.kern_stride);
-  row_chain<T, true, false, N1, L2, Q, 0, Sh>(x, a.tw2, sm, nullptr, 0);
+  {
+    using First = RowStage<T, N1, L2, Q, Sh, 0>;
+    auto st = x.first(Sh::NT, [&](int tid) FFB_INL { return First::read(a, sm, 0, tid); });
+    row_pipe<T, N1, L2, Q, Sh, 1>(x, a, sm, st);
+  }
+  x.sync();
 
   // 3. W_M^{-k1 j2}, inverse column DFT over k1, chirp, y_j for j < n
   x.each(Sh::NT, [&](int tid) FFB_INL {

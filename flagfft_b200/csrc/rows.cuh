@@ -84,6 +84,36 @@ struct DevT {
     __syncthreads();
 #endif
   }
+  // A barrier-separated pipeline of per-thread steps: first() starts it,
+  // step() crosses a barrier and maps this thread's state to the next,
+  // last() crosses a barrier and consumes it.
+  template <class F>
+  FFB_HD auto first(int, F &&f) const {
+#ifdef __CUDA_ARCH__
+    return f((int)threadIdx.x);
+#else
+    return f(0);
+#endif
+  }
+  template <class F, class S>
+  FFB_HD auto step(int, F &&f, const S &st) const {
+#ifdef __CUDA_ARCH__
+    __syncthreads();
+    return f((int)threadIdx.x, st);
+#else
+    return f(0, st);
+#endif
+  }
+  template <class F, class S>
+  FFB_HD void last(int, F &&f, const S &st) const {
+#ifdef __CUDA_ARCH__
+    __syncthreads();
+    f((int)threadIdx.x, st);
+#else
+    (void)f;
+    (void)st;
+#endif
+  }
   // rd's result stays in this thread's registers across the barrier
   template <class FR, class FW>
   FFB_HD void each2(int, FR &&rd, FW &&wr) const {
@@ -103,6 +133,31 @@ struct HostT {
     for (int t = 0; t < nthr; ++t) f(t);
   }
   FFB_HD void sync() const {}
+  // the pipeline with one state per thread, every step over all threads
+  template <class F>
+  FFB_HD auto first(int nthr, F &&f) const {
+    std::vector<decltype(f(0))> out;
+#ifndef __CUDA_ARCH__
+    out.reserve((size_t)nthr);
+    for (int t = 0; t < nthr; ++t) out.push_back(f(t));
+#endif
+    return out;
+  }
+  template <class F, class S>
+  FFB_HD auto step(int nthr, F &&f, const std::vector<S> &st) const {
+    std::vector<decltype(f(0, st[0]))> out;
+#ifndef __CUDA_ARCH__
+    out.reserve((size_t)nthr);
+    for (int t = 0; t < nthr; ++t) out.push_back(f(t, st[(size_t)t]));
+#endif
+    return out;
+  }
+  template <class F, class S>
+  FFB_HD void last(int nthr, F &&f, const std::vector<S> &st) const {
+#ifndef __CUDA_ARCH__
+    for (int t = 0; t < nthr; ++t) f(t, st[(size_t)t]);
+#endif
+  }
   template <class FR, class FW>
   FFB_HD void each2(int nthr, FR &&rd, FW &&wr) const {
 #ifndef __CUDA_ARCH__
