@@ -30,6 +30,12 @@ using rows::SmemKernIO;
 using rows::slot_len;
 using rows::tpt_of;
 
+// W_M^m (forward sign) from the pass's two split four-step tables, m < M.
+template <typename T>
+FFB_HD cpx<T> split_twiddle(const TileArgs<T> &a, uint32_t m) {
+  const uint32_t hi = fdiv(m, a.ptw_div);
+  return cmul(ldg_c(a.ptw_hi + hi), ldg_c(a.ptw_lo + (m - hi * a.ptw_div.d)));
+}
 
 // Shape of the kernel for N1 rows of sequence Rs...: TPT threads per row,
 // rows processed in two groups of NR, NT threads in all.
@@ -98,9 +104,8 @@ FFB_HD void row_pipe(const X &x, const TileArgs<T> &a, cpx<T> *sm, const St &st)
 
 // One transform (batch index by) of the one-pass chain.  TileArgs: core /
 // core2 the row sequence with tables tw / tw2, kern the N1 x L2 kernel
-// spectrum rows (kern_stride = L2), chirp the n-point chirp, the W_M
-// twiddles of column j2, row k1 (four_step_twiddle with g = j2), n the
-// logical length, ib / ob the transform distances.
+// spectrum rows (kern_stride = L2), chirp the n-point chirp, ptw_* the split
+// W_M tables, n the logical length, ib / ob the transform distances.
 #pragma nv_exec_check_disable
 template <typename T, int N1, int L2, class X, int... Rs>
 FFB_HD void blue4_body(const TileArgs<T> &a, long long by, cpx<T> *sm, const X &x) {
@@ -123,7 +128,7 @@ FFB_HD void blue4_body(const TileArgs<T> &a, long long by, cpx<T> *sm, const X &
       dft_fixed<N1, false, T>(v);
       if (j2) {
 #pragma unroll
-        for (int k1 = 1; k1 < N1; ++k1) v[k1] = cmul(v[k1], four_step_twiddle(a, j2, k1));
+        for (int k1 = 1; k1 < N1; ++k1) v[k1] = cmul(v[k1], split_twiddle(a, (uint32_t)(k1 * j2)));
       }
       const int p = pp_pos(j2);
 #pragma unroll
@@ -150,7 +155,7 @@ FFB_HD void blue4_body(const TileArgs<T> &a, long long by, cpx<T> *sm, const X &
       for (int k1 = 0; k1 < N1; ++k1) v[k1] = sm[k1 * Sh::slot + p];
       if (j2) {
 #pragma unroll
-        for (int k1 = 1; k1 < N1; ++k1) v[k1] = cmul(v[k1], conjg(four_step_twiddle(a, j2, k1)));
+        for (int k1 = 1; k1 < N1; ++k1) v[k1] = cmul(v[k1], conjg(split_twiddle(a, (uint32_t)(k1 * j2))));
       }
       dft_fixed<N1, true, T>(v);
 #pragma unroll

@@ -646,25 +646,6 @@ class Builder {
     });
   }
 
-  // Four-step post-twiddles of N = n1 x n2 as the matrix W_N^{a b} (a < n1,
-  // b < n2): one coalesced load per element; g_row says whether a pass's
-  // transform index is a (1) or b (0).
-  void set_post_twiddle_matrix(TileArgs<T> &a, int64_t n1, int64_t n2, bool g_row) {
-    const int64_t N = n1 * n2;
-    a.post_twiddle = 1;
-    a.ptw_mat = cached<cpx<T>>("ptwmat|" + std::to_string(n1) + "x" + std::to_string(n2), [&]() {
-      std::vector<cpx<T>> h((size_t)N);
-      for (int64_t r = 0; r < n1; ++r)
-        for (int64_t c = 0; c < n2; ++c) {
-          cld w = unit_root(r * c, N, -1);
-          h[(size_t)(r * n2 + c)] = mk((T)w.real(), (T)w.imag());
-        }
-      return h;
-    });
-    a.ptw_n2 = n2;
-    a.ptw_g_row = g_row ? 1 : 0;
-  }
-
   // Four-step post-twiddle W_N^m = hi[m / split] * lo[m % split].
   void set_post_twiddle(TileArgs<T> &a, int64_t N) {
     const int64_t split = (int64_t)std::ceil(std::sqrt((double)N));
@@ -761,10 +742,6 @@ class Builder {
 // chain; "multipass" splits every tree that has a multi-pass lowering (one
 // HBM round trip more, but smaller, more numerous CTAs); "inplace" keeps
 // every transform that fits one CTA in one pass.
-// Largest four-step N whose post-twiddles are one n1 x n2 matrix (2 MB at
-// f32) rather than two sqrt(N) split tables.
-constexpr int64_t kTwiddleMatrixMax = 1 << 18;
-
 thread_local int t_policy_override = -1;  // set while lowering batch groups
 // Set while lowering batch groups: the one-pass four-step Bluestein (its own
 // launch per group) gives way to the three-pass chain, whose passes join the
@@ -821,10 +798,7 @@ void lower_c2c(Builder<T> &bld, Program &prog, const NodePtr &root, bool inverse
       prog.scratch0 = std::make_shared<DevMem>((size_t)(batch * n) * sizeof(cpx<T>));
       // pass A: columns j2 (stride n2) of length n1, x W_n^{j2 k1}, rows Y[j2][k1]
       auto *pa = bld.add_pass(sa, IoKind::C2C, inverse, batch, n2, idist, 1, n2, n, n1, 1, src, Buf::Scratch0, n1);
-      if (n <= kTwiddleMatrixMax)
-        bld.set_post_twiddle_matrix(pa->a, n1, n2, false);
-      else
-        bld.set_post_twiddle(pa->a, n);
+      bld.set_post_twiddle(pa->a, n);
       // pass B: for each k1, length n2 over Y[j2][k1] -> X[k1 + n1 k2]
       bld.add_pass(sb, IoKind::C2C, inverse, batch, n1, n, 1, n1, odist, 1, n1, Buf::Scratch0, dst, n2);
       return;
@@ -858,7 +832,7 @@ void lower_c2c(Builder<T> &bld, Program &prog, const NodePtr &root, bool inverse
       a.chirp = bld.table_chirp(n, inverse);
       a.kern = bld.table_bluestein_rows(n, row_radices, n1, n2, inverse, true);
       a.kern_stride = n2;
-      bld.set_post_twiddle_matrix(a, n1, n2, false);
+      bld.set_post_twiddle(a, M);
       p->smem = blue4_smem((int)n1, (int)n2, sizeof(cpx<T>));
       p->note = "bluestein one pass: " + std::to_string(n1) + " x " + std::to_string(n2) + " four-step in one CTA";
       return;
@@ -875,7 +849,7 @@ void lower_c2c(Builder<T> &bld, Program &prog, const NodePtr &root, bool inverse
       pa->a.chirp = chirp;
       pa->a.cj_e = n2;
       pa->a.cj_g = 1;
-      bld.set_post_twiddle_matrix(pa->a, n1, n2, false);
+      bld.set_post_twiddle(pa->a, M);
       pa->note = "bluestein 1/3: chirp + column FFT";
       // B: per k1: FFT over j2, x B[k1 + n1 k2] / M, inverse FFT over k2, x W_M^{-j2 k1}
       CoreSpec sc = sb;
@@ -883,7 +857,7 @@ void lower_c2c(Builder<T> &bld, Program &prog, const NodePtr &root, bool inverse
       auto *pb = bld.add_pass(sc, IoKind::C2C, true, batch, n1, M, n2, 1, M, n2, 1, Buf::Scratch0, Buf::Scratch0, n2);
       pb->a.kern = bld.table_bluestein_rows(n, sb.radices, n1, n2, inverse, pb->a.pp != 0);
       pb->a.kern_stride = n2;
-      bld.set_post_twiddle_matrix(pb->a, n1, n2, true);
+      bld.set_post_twiddle(pb->a, M);
       pb->note = "bluestein 2/3: row convolution";
       // C: inverse FFT over k1 -> j1, y_j = conv_j c_j for j = j1 n2 + j2 < n
       auto *pc = bld.add_pass(sa, IoKind::C2C, true, batch, n2, M, 1, n2, odist, 1, n2, Buf::Scratch0, dst, n);

@@ -90,13 +90,6 @@ struct TileArgs {
   const cpx<T> *ptw_lo;
   const cpx<T> *ptw_hi;
   FastDiv ptw_div;
-  // instead of the split tables, for a four-step N = n1 x n2 small enough:
-  // the matrix ptw_mat[a * n2 + b] = W_N^{a b} (a < n1, b < n2), with the
-  // transform index g the row a (ptw_g_row = 1) or the column b (0), so that
-  // consecutive transforms or elements read consecutive entries
-  const cpx<T> *ptw_mat;
-  long long ptw_n2;
-  int ptw_g_row;
   FastDiv ldiv;  // / core.L
   FastDiv wdiv;  // / W
   FastDiv ndiv;  // / n
@@ -118,15 +111,6 @@ struct TileArgs {
   // (rows of the core's sequence); one CTA per transform.
   int blue_cols;
 };
-
-// Four-step twiddle W_N^{g k} (forward sign) of output k of transform g.
-template <typename T>
-FFB_HD cpx<T> four_step_twiddle(const TileArgs<T> &a, long long g, int k) {
-  if (a.ptw_mat) return ldg_c(a.ptw_mat + (a.ptw_g_row ? g * a.ptw_n2 + k : (long long)k * a.ptw_n2 + g));
-  const uint32_t m = (uint32_t)(g * (long long)k);
-  const uint32_t hi = fdiv(m, a.ptw_div);
-  return cmul(ldg_c(a.ptw_hi + hi), ldg_c(a.ptw_lo + (m - hi * a.ptw_div.d)));
-}
 
 // Real-transform pre/post processing between the passes of a multi-pass
 // R2C / C2R (L = n/2 complex points per transform, rtw[k] = W_n^k, k <= L):

@@ -29,10 +29,12 @@ FFB_HD void regcol_transform(const TileArgs<T> &a, long long by, long long g) {
       if (j < a.n) out[k * a.ok] = cmul(v[k], ldg_c(a.chirp + j));
     }
   } else if (a.post_twiddle) {
-    // output k of transform g times W_N^{g k}
+    // output k of transform g times W_N^{g k} = hi[m / split] * lo[m % split]
 #pragma unroll
     for (int k = 0; k < R; ++k) {
-      cpx<T> t = four_step_twiddle(a, g, k);
+      const uint32_t m = (uint32_t)(g * k);
+      const uint32_t hi = fdiv(m, a.ptw_div);
+      cpx<T> t = cmul(ldg_c(a.ptw_hi + hi), ldg_c(a.ptw_lo + (m - hi * a.ptw_div.d)));
       if constexpr (INV) t.y = -t.y;
       out[k * a.ok] = cmul(v[k], t);
     }

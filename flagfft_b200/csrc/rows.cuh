@@ -242,10 +242,14 @@ struct SmemKernIO {
   }
 };
 
-// Four-step post-twiddle W_N^{g k} (conjugated for the inverse), g k < N.
+// Four-step post-twiddle W_N^{g k} (conjugated for the inverse) from the two
+// split tables, m = g * k < N.
 template <typename T>
 FFB_HD cpx<T> post_twiddle(const TileArgs<T> &a, cpx<T> v, long long g, int k) {
-  cpx<T> t = four_step_twiddle(a, g, k);
+  const uint32_t m = (uint32_t)(g * (long long)k);
+  const uint32_t hi = fdiv(m, a.ptw_div);
+  const uint32_t lo = m - hi * a.ptw_div.d;
+  cpx<T> t = cmul(ldg_c(a.ptw_hi + hi), ldg_c(a.ptw_lo + lo));
   if (a.inv) t.y = -t.y;
   return cmul(v, t);
 }

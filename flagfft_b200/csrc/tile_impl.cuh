@@ -225,7 +225,10 @@ FFB_HD void tile_body(const TileArgs<T> &a, long long bx, long long by, cpx<T> *
   // (forward sign; conjugated for the inverse), g*k < N < 2^31.
   auto post_twiddle = [&](cpx<T> v, long long g, int k) FFB_INL -> cpx<T> {
     if (!a.post_twiddle) return v;
-    cpx<T> t = four_step_twiddle(a, g, k);
+    const uint32_t m = (uint32_t)(g * (long long)k);
+    const uint32_t hi = fdiv(m, a.ptw_div);
+    const uint32_t lo = m - hi * a.ptw_div.d;
+    cpx<T> t = cmul(ldg_c(a.ptw_hi + hi), ldg_c(a.ptw_lo + lo));
     if (a.inv) t.y = -t.y;
     return cmul(v, t);
   };
@@ -460,7 +463,10 @@ FFB_HD void tile_body_pp(const TileArgs<T> &a, long long bx, long long by, cpx<T
   const int res_off = (S_total & 1) ? Lq : 0;
   auto post_twiddle = [&](cpx<T> v, long long g, int k) FFB_INL -> cpx<T> {
     if (!a.post_twiddle) return v;
-    cpx<T> t = four_step_twiddle(a, g, k);
+    const uint32_t m = (uint32_t)(g * (long long)k);
+    const uint32_t hi = fdiv(m, a.ptw_div);
+    const uint32_t lo = m - hi * a.ptw_div.d;
+    cpx<T> t = cmul(ldg_c(a.ptw_hi + hi), ldg_c(a.ptw_lo + lo));
     if (a.inv) t.y = -t.y;
     return cmul(v, t);
   };
