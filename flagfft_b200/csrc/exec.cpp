@@ -487,7 +487,14 @@ class Builder {
     // Stockham ping-pong when two buffers of the transform fit (C2C passes);
     // the in-place DIT / DIF path otherwise.
     const size_t pp_per = (2 * (size_t)pp_size((int)L) + 3) * sizeof(cpx<T>);
-    a.pp = (io == IoKind::C2C && L > 1 && pp_per <= limit) ? 1 : 0;
+    // a contiguous-row pass of a compile-time sequence runs on a row kernel,
+    // which keeps one buffer per row (rows.cuh): it needs half of pp_per
+    std::vector<int> seq, sorted_r = spec.radices;
+    std::sort(sorted_r.rbegin(), sorted_r.rend());
+    const size_t rows_per = ((size_t)pp_size((int)L) + 1) * sizeof(cpx<T>);
+    const bool rows_only = io == IoKind::C2C && L > 1 && pp_per > limit && rows_per <= limit && ii == 1 &&
+                           ok == 1 && ii <= ig && fixed_sequence(L, &seq) && seq == sorted_r;
+    a.pp = (io == IoKind::C2C && L > 1 && (pp_per <= limit || rows_only)) ? 1 : 0;
     // ping-pong cores run their radices largest first (any order is the same
     // DFT; this one matches the compile-time sequences), and a convolution's
     // inverse core the same order; the in-place pair needs DIF then DIT with
@@ -531,7 +538,9 @@ class Builder {
     const bool strided = ii > ig;
     a.wfast = strided ? 1 : 0;
     int tpt = choose_tpt(L, spec.radices);
-    const size_t per = a.pp ? pp_per : tile_smem_per_transform<T>((int)L) + Swz<T>::G * sizeof(cpx<T>);
+    const size_t per = rows_only ? rows_per
+                       : a.pp    ? pp_per
+                                 : tile_smem_per_transform<T>((int)L) + Swz<T>::G * sizeof(cpx<T>);
     // Transforms per CTA: about 256 threads' worth, within a shared-memory
     // budget that leaves room for a second CTA per SM, and no more than keeps
     // ~2 CTAs per SM busy; column tiles take at least 8 transforms so each

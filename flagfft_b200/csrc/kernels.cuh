@@ -33,7 +33,7 @@ enum class IoKind : int {
 // and writes element k at                          out + b*ob + g*og + k*ok
 // (units: elements of the pass's input / output type).
 // The compile-time radix sequences with their own kernels: radix-16 chains
-// of the power-of-two lengths 128..8192 (one smaller radix last), and the
+// of the power-of-two lengths 128..16384 (one smaller radix last), and the
 // mixed-radix 1701 = 9 * 9 * 7 * 3.  The executor runs a length that has one
 // on it (and prefers such lengths for convolutions).
 #define FFB_FIXED_SEQUENCES(X)        \
@@ -44,7 +44,8 @@ enum class IoKind : int {
   X(1024, 16, 16, 4)                  \
   X(2048, 16, 16, 8)                  \
   X(4096, 16, 16, 16)                 \
-  X(8192, 16, 16, 16, 2)
+  X(8192, 16, 16, 16, 2)              \
+  X(16384, 16, 16, 16, 4)
 
 // Shapes (N1 rows of an L2-point compile-time sequence) of the one-pass
 // four-step Bluestein kernel (blue4.cuh), single precision: the N1 padded

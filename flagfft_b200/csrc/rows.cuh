@@ -68,6 +68,14 @@ FFB_HD constexpr int tpt_of(int L, int rmax) {
   return (t + 31) / 32 * 32;
 }
 
+// Threads per row of a row kernel: tpt_of, at most the precision's CTA
+// limit (L = 16384 runs 512 threads, two radix-16 butterflies each).
+template <typename T, int L, int... Rs>
+FFB_HD constexpr int rows_tpt() {
+  return tpt_of(L, Seq<Rs...>::rmax()) < tile::TileBounds<T>::kMaxThreads ? tpt_of(L, Seq<Rs...>::rmax())
+                                                                           : tile::TileBounds<T>::kMaxThreads;
+}
+
 // Thread policy: DevT runs a phase's body once as this CUDA thread; HostT
 // (host emulation of the index arithmetic) runs it for every thread in turn.
 struct DevT {
@@ -474,7 +482,7 @@ FFB_HD void rows_body(const TileArgs<T> &a, long long bx, long long by, cpx<T> *
 template <typename T, int KIND, bool INV, int L, int... Rs>
 __global__ void __launch_bounds__(tile::TileBounds<T>::kMaxThreads) k_rows(const __grid_constant__ TileArgs<T> a) {
   extern __shared__ __align__(16) unsigned char smraw[];
-  constexpr int TPT = tpt_of(L, Seq<Rs...>::rmax());
+  constexpr int TPT = rows_tpt<T, L, Rs...>();
   rows_body<T, KIND, INV, L, TPT, DevT, Rs...>(a, (long long)blockIdx.x, (long long)blockIdx.y,
                                                reinterpret_cast<cpx<T> *>(smraw), DevT{});
 }
@@ -484,7 +492,7 @@ __global__ void __launch_bounds__(tile::TileBounds<T>::kMaxThreads) k_rows(const
 // same sequence for the inverse core.
 template <typename T, int KIND, int L, int... Rs>
 FFB_HD bool rows_fit(const TileArgs<T> &a) {
-  constexpr int TPT = tpt_of(L, Seq<Rs...>::rmax());
+  constexpr int TPT = rows_tpt<T, L, Rs...>();
   return a.pp && !a.wfast && a.ii == 1 && a.ok == 1 && a.tpt == TPT &&
          a.W * TPT <= tile::TileBounds<T>::kMaxThreads && tile::core_is<L, Rs...>(a.core) &&
          (KIND == 0 || tile::core_is<L, Rs...>(a.core2));
@@ -506,7 +514,7 @@ cudaError_t launch_rows(const TileArgs<T> &a, cudaStream_t s) {
     if (e != cudaSuccess) return e;
     configured = true;
   }
-  constexpr int TPT = tpt_of(L, Seq<Rs...>::rmax());
+  constexpr int TPT = rows_tpt<T, L, Rs...>();
   dim3 grid((unsigned)((a.G + a.W - 1) / a.W), (unsigned)a.nbatch, 1);
   dim3 block((unsigned)(a.W * TPT), 1, 1);
   k_rows<T, KIND, INV, L, Rs...><<<grid, block, rows_smem<T, L>(a), s>>>(a);
@@ -515,7 +523,7 @@ cudaError_t launch_rows(const TileArgs<T> &a, cudaStream_t s) {
 #else
 template <typename T, int KIND, bool INV, int L, int... Rs>
 cudaError_t launch_rows(const TileArgs<T> &a, cudaStream_t) {
-  constexpr int TPT = tpt_of(L, Seq<Rs...>::rmax());
+  constexpr int TPT = rows_tpt<T, L, Rs...>();
   std::vector<unsigned char> buf(rows_smem<T, L>(a) + 64);
   cpx<T> *sm = reinterpret_cast<cpx<T> *>(buf.data());
   const long long tiles = (a.G + a.W - 1) / a.W;

@@ -248,13 +248,16 @@ FFB_HD void tile_body(const TileArgs<T> &a, long long bx, long long by, cpx<T> *
   };
 
   // ---------------------------------------------------------------- store
+  // output mapping: consecutive threads take consecutive transforms when a
+  // transform's outputs are strided (ok > og), else consecutive elements
+  const int ofast = a.ok > a.og ? 1 : 0;
   if constexpr (IO == 0) {
     if constexpr (KIND == 2) {
       // X[g^q] = x0 + conv[q] (scatter by q keeps the reads conflict-free);  X[0] = x0 + sum
       const int total = W * L;
       for (int e = t0; e < total; e += nt) {
         int w, q;
-        split_elem(e, W, L, a.wfast, a.wdiv, a.ldiv, w, q);
+        split_elem(e, W, L, ofast, a.wdiv, a.ldiv, w, q);
         const long long g = g0 + w;
         if (g < a.G) {
           const cpx<T> *bw = sm + w * Lp;
@@ -271,7 +274,7 @@ FFB_HD void tile_body(const TileArgs<T> &a, long long bx, long long by, cpx<T> *
       const int total = W * nout;
       auto produce = [&](int e) FFB_INL -> cpx<T> {
         int w, k;
-        split_elem(e, W, nout, a.wfast, a.wdiv, KIND == 1 ? a.ndiv : a.ldiv, w, k);
+        split_elem(e, W, nout, ofast, a.wdiv, KIND == 1 ? a.ndiv : a.ldiv, w, k);
         const long long g = g0 + w;
         const long long gc = g < a.G ? g : a.G - 1;
         cpx<T> v = out_elem(w, k);
@@ -285,7 +288,7 @@ FFB_HD void tile_body(const TileArgs<T> &a, long long bx, long long by, cpx<T> *
       };
       auto consume = [&](int e, cpx<T> v) FFB_INL {
         int w, k;
-        split_elem(e, W, nout, a.wfast, a.wdiv, KIND == 1 ? a.ndiv : a.ldiv, w, k);
+        split_elem(e, W, nout, ofast, a.wdiv, KIND == 1 ? a.ndiv : a.ldiv, w, k);
         const long long g = g0 + w;
         if (g >= a.G) return;
         if constexpr (KIND == 0) {
@@ -301,7 +304,7 @@ FFB_HD void tile_body(const TileArgs<T> &a, long long bx, long long by, cpx<T> *
     const int total = W * nbins;
     for (int e = t0; e < total; e += nt) {
       int w, k;
-      if (a.wfast) {
+      if (ofast) {
         k = e / W;
         w = e - k * W;
       } else {
@@ -322,7 +325,7 @@ FFB_HD void tile_body(const TileArgs<T> &a, long long bx, long long by, cpx<T> *
     const int total = W * cnt;
     for (int e = t0; e < total; e += nt) {
       int w, j;
-      split_elem(e, W, cnt, a.wfast, a.wdiv, IO == 2 ? a.hdiv : a.ldiv, w, j);
+      split_elem(e, W, cnt, ofast, a.wdiv, IO == 2 ? a.hdiv : a.ldiv, w, j);
       const long long g = g0 + w;
       if (g >= a.G) continue;
       cpx<T> z = out_elem(w, j);
@@ -333,7 +336,7 @@ FFB_HD void tile_body(const TileArgs<T> &a, long long bx, long long by, cpx<T> *
     const int total = W * L;
     for (int e = t0; e < total; e += nt) {
       int w, k;
-      split_elem(e, W, L, a.wfast, a.wdiv, a.ldiv, w, k);
+      split_elem(e, W, L, ofast, a.wdiv, a.ldiv, w, k);
       const long long g = g0 + w;
       if (g < a.G) st_cpx<T>(out, g * a.og + (long long)k * a.ok, post_twiddle(out_elem(w, k), g, k));
     }
@@ -342,7 +345,7 @@ FFB_HD void tile_body(const TileArgs<T> &a, long long bx, long long by, cpx<T> *
     const int total = W * nbins;
     for (int e = t0; e < total; e += nt) {
       int w, k;
-      if (a.wfast) {
+      if (ofast) {
         k = e / W;
         w = e - k * W;
       } else {
@@ -356,7 +359,7 @@ FFB_HD void tile_body(const TileArgs<T> &a, long long bx, long long by, cpx<T> *
     const int total = W * n;
     for (int e = t0; e < total; e += nt) {
       int w, k;
-      split_elem(e, W, n, a.wfast, a.wdiv, a.ndiv, w, k);
+      split_elem(e, W, n, ofast, a.wdiv, a.ndiv, w, k);
       const long long g = g0 + w;
       if (g < a.G) st_real<T>(out, g * a.og + (long long)k * a.ok, out_elem(w, k).x);
     }
@@ -472,12 +475,16 @@ FFB_HD void tile_body_pp(const TileArgs<T> &a, long long bx, long long by, cpx<T
   };
   const int nout = KIND == 1 ? n : L;
   const int total = W * nout;
+  // output mapping: consecutive threads take consecutive transforms when a
+  // transform's outputs are strided (ok > og), else consecutive elements, so
+  // both the loads and the stores of a column tile are coalesced
+  const int ofast = a.ok > a.og ? 1 : 0;
   // produce: the output value and its offset from `out`, or -1 when the
   // element is not written (a dead transform of the last tile, or a
   // chirp-on-store position past n)
   auto produce = [&](int e) FFB_INL -> ElemAt<T> {
     int w, k;
-    split_elem(e, W, nout, a.wfast, a.wdiv, KIND == 1 ? a.ndiv : a.ldiv, w, k);
+    split_elem(e, W, nout, ofast, a.wdiv, KIND == 1 ? a.ndiv : a.ldiv, w, k);
     const int wc = w < wlive ? w : wlive - 1;
     const int at = w < wlive ? w * og + k * ok : -1;
     const cpx<T> *bw = sm + w * slot_len;
