@@ -237,6 +237,11 @@ double chain_cost(int64_t m, std::vector<int> *radices, std::unordered_map<int64
   return cost;
 }
 
+// Set while lowering batch groups: the one-pass four-step Bluestein and the
+// strided tile kernels (their own launches) give way to lowerings whose
+// passes join the persistent launches.
+thread_local bool t_no_one_pass = false;
+
 // The compile-time radix sequence of length L (FFB_FIXED_SEQUENCES), if it
 // has one: such a length runs on a row kernel with every index constant.
 bool fixed_sequence(int64_t L, std::vector<int> *r) {
@@ -553,12 +558,27 @@ class Builder {
     if (strided) W = std::max<int64_t>(W, std::min<int64_t>({8, G, (int64_t)(limit / per)}));
     W = std::max<int64_t>(W, 1);
     if (W * tpt > kMaxThreads) tpt = std::max<int>(1, (int)(kMaxThreads / W));
+    size_t smem_tiles = 0;
+    {
+      // a strided pass of a compile-time sequence: the tile kernel, whose
+      // one buffer per transform fits twice the transforms of two buffers
+      int tw = 0, tthreads = 0;
+      size_t tsm = 0;
+      if (spec.kind == CoreKind::Dit && io == IoKind::C2C && a.pp && (ii > ig || ok > og) && !t_no_one_pass &&
+          fixed_sequence(L, &seq) && seq == sorted_r && tiles_shape<T>((int)L, &tw, &tthreads, &tsm) &&
+          std::min<int64_t>(tw, G) > W) {
+        a.tiles = 1;
+        W = tw;
+        tpt = tthreads;  // all threads of the CTA (the kernel splits them over the tile's transforms)
+        smem_tiles = tsm;
+      }
+    }
     a.W = (int)W;
     a.tpt = tpt;
     // offsets inside one CTA's tile are 32-bit in the kernels
     if (W * std::llabs(ig) + L * std::llabs(ii) >= (1ll << 31) || W * std::llabs(og) + L * std::llabs(ok) >= (1ll << 31))
       throw std::runtime_error("tile extent above 2^31 elements");
-    const size_t smem = per * (size_t)W;
+    const size_t smem = a.tiles ? smem_tiles : per * (size_t)W;
     a.ldiv = make_fastdiv((uint32_t)L);
     a.wdiv = make_fastdiv((uint32_t)W);
     a.ndiv = make_fastdiv((uint32_t)std::max<int64_t>(1, logical_n));
@@ -752,10 +772,6 @@ class Builder {
 // HBM round trip more, but smaller, more numerous CTAs); "inplace" keeps
 // every transform that fits one CTA in one pass.
 thread_local int t_policy_override = -1;  // set while lowering batch groups
-// Set while lowering batch groups: the one-pass four-step Bluestein (its own
-// launch per group) gives way to the three-pass chain, whose passes join the
-// persistent launches.
-thread_local bool t_no_one_pass = false;
 
 static int onchip_policy() {
   if (t_policy_override >= 0) return t_policy_override;
@@ -1392,7 +1408,7 @@ std::unique_ptr<BatchProgram> lower_batch_t(const std::vector<BatchGroup> &group
   for (auto &g : bp->groups)
     for (auto &ps : g.prog->passes) {
       auto *tp = dynamic_cast<TilePass<T> *>(ps.get());
-      if (!tp || !tp->a.pp || tp->a.regcol || tp->a.blue_cols || tp->a.tpt > kBatchWidth) continue;
+      if (!tp || !tp->a.pp || tp->a.regcol || tp->a.blue_cols || tp->a.tiles || tp->a.tpt > kBatchWidth) continue;
       TileArgs<T> &a = tp->a;
       const size_t per = tp->smem / (size_t)a.W;
       int64_t W = std::min<int64_t>({(int64_t)(kBatchWidth / a.tpt), (int64_t)a.G,
@@ -1416,7 +1432,7 @@ std::unique_ptr<BatchProgram> lower_batch_t(const std::vector<BatchGroup> &group
       if (auto *tp = dynamic_cast<const TilePass<T> *>(g.prog->passes[pi].get())) {
         if (tp->a.regcol) {
           kind = kBatchRegcol;
-        } else if (tp->a.pp && !tp->a.blue_cols && tp->io == IoKind::C2C) {
+        } else if (tp->a.pp && !tp->a.blue_cols && !tp->a.tiles && tp->io == IoKind::C2C) {
           kind = tp->kind == CoreKind::Dit         ? kBatchPpDit
                  : tp->kind == CoreKind::Bluestein ? kBatchPpBluestein
                  : tp->kind == CoreKind::Rader     ? kBatchPpRader

@@ -76,7 +76,8 @@ struct TilePass final : PassBase {
       << " radices=[";
     for (int s = 0; s < a.core.nst; ++s) o << (s ? "," : "") << a.core.radix[s];
     o << "] n=" << a.n << " transforms=" << a.nbatch << "x" << a.G << " per_cta=" << a.W
-      << " threads=" << (a.blue_cols ? blue4_threads(a.blue_cols, a.core.L) : a.W * a.tpt) << " smem=" << tile_smem<T>(a, kind, io, smem) << " " << buf_name(src) << "->"
+      << " threads=" << (a.blue_cols ? blue4_threads(a.blue_cols, a.core.L) : a.tiles ? a.tpt : a.W * a.tpt)
+      << (a.tiles ? " tiles" : "") << " smem=" << tile_smem<T>(a, kind, io, smem) << " " << buf_name(src) << "->"
       << buf_name(dst);
     if (a.post_twiddle) o << " +twiddle";
     if (!note.empty()) o << " (" << note << ")";

@@ -172,6 +172,7 @@ cudaError_t launch_tile(const TileArgs<T> &a, CoreKind kind, IoKind io, size_t s
   const int k = (int)kind, o = (int)io;
   if (a.regcol) return launch_regcol<T>(a, s);
   if (a.blue_cols) return launch_blue4<T>(a, s);
+  if (a.tiles) return launch_tiles<T>(a, s);
   if (a.pp && o == 0) {
     // compile-time radix sequences first: contiguous rows, then any layout
     // (cudaErrorNotSupported: no kernel for this pass)
@@ -210,6 +211,7 @@ size_t tile_smem(const TileArgs<T> &a, CoreKind kind, IoKind io, size_t smem) {
   const int k = (int)kind;
   if (a.regcol) return 0;
   if (a.blue_cols) return blue4_smem(a.blue_cols, a.core.L, sizeof(cpx<T>));
+  if (a.tiles) return smem;
   if (a.pp && io == IoKind::C2C && (k == 0 || k == 1 || k == 3)) {
     const size_t r = k == 0 ? rows::rows_smem_any<T, 0>(a) : k == 1 ? rows::rows_smem_any<T, 1>(a)
                                                                      : rows::rows_smem_any<T, 3>(a);

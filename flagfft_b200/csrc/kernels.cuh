@@ -111,6 +111,9 @@ struct TileArgs {
   // > 0: one-pass four-step Bluestein (blue4.cuh) with this many columns
   // (rows of the core's sequence); one CTA per transform.
   int blue_cols;
+  // 1: strided tile kernel of a compile-time sequence (tiles.cuh): W is its
+  // fixed tile width, one shared buffer per transform.
+  int tiles;
 };
 
 // Real-transform pre/post processing between the passes of a multi-pass
@@ -143,6 +146,14 @@ cudaError_t launch_tile(const TileArgs<T> &a, CoreKind kind, IoKind io, size_t s
 // the compile-time sequences take less than the pass's general figure).
 template <typename T>
 size_t tile_smem(const TileArgs<T> &a, CoreKind kind, IoKind io, size_t smem_bytes);
+
+// Strided tile kernels of the compile-time sequences (TileArgs::tiles);
+// defined in k_f32_tiles.cu / k_f64_tiles.cu.  tiles_shape gives the tile
+// width, threads and shared memory for a sequence length (false: none).
+template <typename T>
+cudaError_t launch_tiles(const TileArgs<T> &a, cudaStream_t stream);
+template <typename T>
+bool tiles_shape(int L, int *W, int *threads, size_t *smem);
 
 // One-pass four-step Bluestein (TileArgs::blue_cols); defined in
 // k_f32_blue4.cu (single precision only).

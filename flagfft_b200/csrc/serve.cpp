@@ -286,7 +286,7 @@ class Server {
         int kind = -1;
         if (a.regcol) {
           kind = kBatchRegcol;
-        } else if (a.pp && !a.blue_cols && tp->io == IoKind::C2C) {
+        } else if (a.pp && !a.blue_cols && !a.tiles && tp->io == IoKind::C2C) {
           kind = tp->kind == CoreKind::Dit         ? kBatchPpDit
                  : tp->kind == CoreKind::Bluestein ? kBatchPpBluestein
                  : tp->kind == CoreKind::Rader     ? kBatchPpRader
