@@ -27,16 +27,23 @@ using rows::SmemIO;
 using rows::slot_len;
 
 // Threads, rows per group and groups of the tile kernel of a length-L
-// sequence: NT = NR * TPT threads (NR as many rows as fit the precision's
-// thread limit), NG groups as many as fit shared memory (2..4), W = NR * NG.
+// sequence: NT = NR * TPT threads, NR rows per group (at most 8, within the
+// precision's thread limit), NG groups (2..4) so that W = NR * NG reaches the
+// transforms a 128-byte row segment holds (16 single, 8 double precision)
+// where shared memory allows.  A small W keeps several CTAs per SM, whose
+// global loads overlap.
 template <typename T, int L, int... Rs>
 struct Shape {
   static constexpr int TPT = rows::rows_tpt<T, L, Rs...>();
-  static constexpr int NR = tile::TileBounds<T>::kMaxThreads / TPT;
+  static constexpr int nr_max = tile::TileBounds<T>::kMaxThreads / TPT;
+  static constexpr int NR = nr_max < 8 ? nr_max : 8;
   static constexpr int NT = NR * TPT;
   static constexpr int slot = slot_len<L>();
   static constexpr int fit = (int)(232448 / ((size_t)NR * slot * sizeof(cpx<T>)));
-  static constexpr int NG = fit < 4 ? fit : 4;
+  static constexpr int target = sizeof(T) == 4 ? 16 : 8;
+  static constexpr int want = (target + NR - 1) / NR < 2 ? 2 : (target + NR - 1) / NR;
+  static constexpr int cap = fit < 4 ? fit : 4;
+  static constexpr int NG = want < cap ? want : cap;
   static constexpr int W = NR * NG;
 };
 
@@ -87,7 +94,7 @@ FFB_HD void tile_body(const TileArgs<T> &a, long long bx, long long by, cpx<T> *
   using Q = Seq<Rs...>;
   using Sh = Shape<T, L, Rs...>;
   constexpr int W = Sh::W, NT = Sh::NT, total = W * L;
-  constexpr int U = sizeof(T) == 4 ? 8 : 4;  // global accesses in flight per thread
+  constexpr int U = sizeof(T) == 4 ? 16 : 8;  // global accesses in flight per thread
   const long long g0 = bx * W;
   const int wlive = (int)((a.G - g0) < W ? (a.G - g0) : W);
   const cpx<T> *in = reinterpret_cast<const cpx<T> *>(a.in) + by * a.ib + g0 * a.ig;
