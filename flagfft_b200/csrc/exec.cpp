@@ -560,13 +560,14 @@ class Builder {
     if (W * tpt > kMaxThreads) tpt = std::max<int>(1, (int)(kMaxThreads / W));
     size_t smem_tiles = 0;
     {
-      // a strided pass of a compile-time sequence: the tile kernel, whose
-      // one buffer per transform fits twice the transforms of two buffers
+      // a strided pass of a compile-time sequence: the tile kernel (one
+      // buffer per transform, compile-time indexing), at least as wide as
+      // the general tile
       int tw = 0, tthreads = 0;
       size_t tsm = 0;
       if (spec.kind == CoreKind::Dit && io == IoKind::C2C && a.pp && (ii > ig || ok > og) && !t_no_one_pass &&
           fixed_sequence(L, &seq) && seq == sorted_r && tiles_shape<T>((int)L, &tw, &tthreads, &tsm) &&
-          std::min<int64_t>(tw, G) > W) {
+          std::min<int64_t>(tw, G) >= W) {
         a.tiles = 1;
         W = tw;
         tpt = tthreads;  // all threads of the CTA (the kernel splits them over the tile's transforms)
