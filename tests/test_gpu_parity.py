@@ -97,6 +97,43 @@ def test_bluestein_one_pass_vs_oracle(ffb, torch_cuda, plans, n):
         _check(O.error_stats(got, ref), O.C2C, n, est)
 
 
+@pytest.mark.parametrize("double", [False, True], ids=["C2C", "Z2Z"])
+@pytest.mark.parametrize("n,batch", [(131072, 1), (65536, 3), (32768, 2)])
+def test_four_step_tiles_vs_oracle(ffb, torch_cuda, plans, n, batch, double):
+    """Four-steps whose strided passes run on the tile kernels (partial last
+    tiles included)."""
+    torch = torch_cuda
+    ftype = O.Z2Z if double else O.C2C
+    x = O.random_complex(n * batch, O.accuracy_seed(ftype, n, batch), double).reshape(batch, n)
+    for direction in (-1, 1):
+        got = _run_c2c(ffb, torch, x, direction, double)
+        ref = O.c2c(x.astype(np.complex128), direction)
+        _check(O.error_stats(got, ref), ftype, n)
+
+
+@pytest.mark.parametrize("double", [False, True], ids=["C2C", "Z2Z"])
+@pytest.mark.parametrize("shape", [(2048, 40), (4096, 24), (1024, 50), (1701, 20)])
+def test_2d_column_tiles_vs_oracle(ffb, torch_cuda, shape, double):
+    """2-D transforms whose column pass runs on the tile kernels, with a
+    partial last tile of columns."""
+    torch = torch_cuda
+    n0, n1 = shape
+    x = O.random_complex(n0 * n1, 4321 + n0 + n1, double).reshape(1, n0, n1)
+    dev_in = torch.from_numpy(x).cuda()
+    dev_out = torch.empty_like(dev_in)
+    p = ffb.plan_many([n0, n1], None, 1, n0 * n1, None, 1, n0 * n1, ffb.Z2Z if double else ffb.C2C, 1)
+    try:
+        assert "tiles" in p.description()
+        for d in (-1, 1):
+            p.execute(dev_in, dev_out, d)
+            torch.cuda.synchronize()
+            ref = O.fft2(x.astype(np.complex128), "c2c", d)
+            _check(O.error_stats(dev_out.cpu().numpy().reshape(1, -1), ref.reshape(1, -1)),
+                   O.Z2Z if double else O.C2C, n0 * n1)
+    finally:
+        p.destroy()
+
+
 @pytest.mark.parametrize("scale", [2.0 ** -20, 1.0, 2.0 ** 20])
 def test_input_scales(ffb, torch_cuda, plans, scale):
     """ctest/flagfft_test.h:457: inputs scaled by 2^-20, 1, 2^20."""
