@@ -45,6 +45,11 @@ struct Shape {
   static constexpr int cap = fit < 4 ? fit : 4;
   static constexpr int NG = want < cap ? want : cap;
   static constexpr int W = NR * NG;
+  // CTAs per SM that shared memory allows (at most 8): the register budget
+  // the kernel is compiled for
+  static constexpr size_t smem = (size_t)W * slot * sizeof(cpx<T>);
+  static constexpr int per_sm = smem ? (int)(232448 / (smem + 1024)) : 1;
+  static constexpr int min_blocks = per_sm < 1 ? 1 : per_sm > 8 ? 8 : per_sm;
 };
 
 template <typename T, bool INV, int L, class Q, class Sh, int S>
@@ -94,16 +99,43 @@ FFB_HD void tile_body(const TileArgs<T> &a, long long bx, long long by, cpx<T> *
   using Q = Seq<Rs...>;
   using Sh = Shape<T, L, Rs...>;
   constexpr int W = Sh::W, NT = Sh::NT, total = W * L;
-  constexpr int U = sizeof(T) == 4 ? 16 : 8;  // global accesses in flight per thread
+  constexpr int U = sizeof(T) == 4 ? 8 : 4;  // global accesses in flight per thread
   const long long g0 = bx * W;
   const int wlive = (int)((a.G - g0) < W ? (a.G - g0) : W);
   const cpx<T> *in = reinterpret_cast<const cpx<T> *>(a.in) + by * a.ib + g0 * a.ig;
   cpx<T> *out = reinterpret_cast<cpx<T> *>(a.out) + by * a.ob + g0 * a.og;
   const long long n = a.n;
 
-  // load: element e of the tile -> (transform w, element i)
+  // load: element e of the tile -> (transform w, element i).  A strided input
+  // whose tile width divides the thread count keeps one transform per thread
+  // (w = tid % W) and steps its element by NT / W: one pointer increment per
+  // load.
   const bool in_fast = a.ii > a.ig;
-  x.each(NT, [&](int tid) FFB_INL {
+  bool loaded = false;
+  if constexpr (NT % W == 0) {
+    if (in_fast && a.chirp_mode == 0) {
+      x.each(NT, [&](int tid) FFB_INL {
+        constexpr int IS = NT / W, M = (L + IS - 1) / IS;
+        const int w = tid % W, i0 = tid / W;
+        const int wc = w < wlive ? w : wlive - 1;
+        const cpx<T> *src = in + wc * a.ig + (long long)i0 * a.ii;
+        const long long step = (long long)IS * a.ii;
+        cpx<T> *dst = sm + w * Sh::slot;
+#pragma unroll 1
+        for (int m0 = 0; m0 < M; m0 += U) {
+          cpx<T> v[U];
+#pragma unroll
+          for (int u = 0; u < U; ++u)
+            if (m0 + u < M && (L % IS == 0 || i0 + (m0 + u) * IS < L)) v[u] = rows::ld_stream(src + (m0 + u) * step);
+#pragma unroll
+          for (int u = 0; u < U; ++u)
+            if (m0 + u < M && (L % IS == 0 || i0 + (m0 + u) * IS < L)) dst[pp_pos(i0 + (m0 + u) * IS)] = v[u];
+        }
+      });
+      loaded = true;
+    }
+  }
+  if (!loaded) x.each(NT, [&](int tid) FFB_INL {
 #pragma unroll 1
     for (int c = tid; c < total; c += U * NT) {
       cpx<T> v[U];
@@ -140,8 +172,31 @@ FFB_HD void tile_body(const TileArgs<T> &a, long long bx, long long by, cpx<T> *
   }
   x.sync();
 
-  // store: element e of the tile -> (transform w, output k)
+  // store: element e of the tile -> (transform w, output k); a strided output
+  // keeps one transform per thread as the load does
   const bool out_fast = a.ok > a.og;
+  if constexpr (NT % W == 0) {
+    if (out_fast && a.chirp_mode == 0) {
+      x.each(NT, [&](int tid) FFB_INL {
+        constexpr int IS = NT / W, M = (L + IS - 1) / IS;
+        const int w = tid % W, k0 = tid / W;
+        if (w >= wlive) return;
+        const long long g = g0 + w;
+        cpx<T> *dst = out + w * a.og + (long long)k0 * a.ok;
+        const long long step = (long long)IS * a.ok;
+        const cpx<T> *src = sm + w * Sh::slot;
+        const bool ptw = a.post_twiddle != 0;
+#pragma unroll 4
+        for (int m = 0; m < M; ++m) {
+          const int k = k0 + m * IS;
+          if (L % IS != 0 && k >= L) break;
+          const cpx<T> v = src[pp_pos(k)];
+          dst[m * step] = ptw ? rows::post_twiddle(a, v, g, k) : v;
+        }
+      });
+      return;
+    }
+  }
   x.each(NT, [&](int tid) FFB_INL {
 #pragma unroll 1
     for (int c = tid; c < total; c += U * NT) {
@@ -168,7 +223,7 @@ FFB_HD void tile_body(const TileArgs<T> &a, long long bx, long long by, cpx<T> *
 }
 
 template <typename T, bool INV, int L, int... Rs>
-__global__ void __launch_bounds__(Shape<T, L, Rs...>::NT) k_tiles(const __grid_constant__ TileArgs<T> a) {
+__global__ void __launch_bounds__(Shape<T, L, Rs...>::NT, Shape<T, L, Rs...>::min_blocks) k_tiles(const __grid_constant__ TileArgs<T> a) {
   extern __shared__ __align__(16) unsigned char smraw[];
   tile_body<T, INV, L, rows::DevT, Rs...>(a, (long long)blockIdx.x, (long long)blockIdx.y,
                                           reinterpret_cast<cpx<T> *>(smraw), rows::DevT{});
