@@ -941,9 +941,14 @@ std::unique_ptr<Program> lower_t(const NodePtr &root, Planner &planner, Transfor
     const cpx<T> *rtw = bld.table_rtw(n);
     prog->scratch0 = std::make_shared<DevMem>((size_t)(batch * L) * sizeof(cpx<T>));
     if (t == Transform::R2C) {
-      // A: z_j = x_2j + i x_2j+1 (j = j1 n2 + j2), FFT over j1, x W_L^{j2 k1} -> Y[j2][k1]
-      auto *pa = bld.add_pass(sa, IoKind::PackC2C, false, batch, n2, idist, 2, 2 * n2, L, n1, 1, Buf::In,
-                              Buf::Scratch0, n1);
+      // A: z_j = x_2j + i x_2j+1 (j = j1 n2 + j2), FFT over j1, x W_L^{j2 k1} -> Y[j2][k1];
+      // with an even row distance the pairs are the rows read as complex
+      // elements, and the pass is a plain complex one (tile kernels apply)
+      auto *pa = idist % 2 == 0
+                     ? bld.add_pass(sa, IoKind::C2C, false, batch, n2, idist / 2, 1, n2, L, n1, 1, Buf::In,
+                                    Buf::Scratch0, n1)
+                     : bld.add_pass(sa, IoKind::PackC2C, false, batch, n2, idist, 2, 2 * n2, L, n1, 1, Buf::In,
+                                    Buf::Scratch0, n1);
       bld.set_post_twiddle(pa->a, L);
       // B: FFT over j2 -> Z[k1 + n1 k2] in the output rows
       bld.add_pass(sb, IoKind::C2C, false, batch, n1, L, 1, n1, odist, 1, n1, Buf::Scratch0, Buf::Out, n2);
@@ -954,8 +959,13 @@ std::unique_ptr<Program> lower_t(const NodePtr &root, Planner &planner, Transfor
           std::make_unique<RealPass<T>>(false, Buf::In, Buf::Scratch1, batch, idist, L, L, rtw));
       auto *pa = bld.add_pass(sa, IoKind::C2C, true, batch, n2, L, 1, n2, L, n1, 1, Buf::Scratch1, Buf::Scratch0, n1);
       bld.set_post_twiddle(pa->a, L);
-      // B: inverse FFT over j2, z_j -> x_2j, x_2j+1 (j = k1 + n1 k2)
-      bld.add_pass(sb, IoKind::C2CUnpack, true, batch, n1, L, 1, n1, odist, 2, 2 * n1, Buf::Scratch0, Buf::Out, n2);
+      // B: inverse FFT over j2, z_j -> x_2j, x_2j+1 (j = k1 + n1 k2): with an
+      // even row distance, complex elements of the output rows
+      if (odist % 2 == 0)
+        bld.add_pass(sb, IoKind::C2C, true, batch, n1, L, 1, n1, odist / 2, 1, n1, Buf::Scratch0, Buf::Out, n2);
+      else
+        bld.add_pass(sb, IoKind::C2CUnpack, true, batch, n1, L, 1, n1, odist, 2, 2 * n1, Buf::Scratch0, Buf::Out,
+                     n2);
     }
     return prog;
   }

@@ -148,7 +148,7 @@ def test_input_scales(ffb, torch_cuda, plans, scale):
 # transform of n/2 points of any lowering plus the Hermitian post / pre pass;
 # 201 = 3 * 67 and 40027 (prime, odd) widen to a full complex transform
 @pytest.mark.parametrize("n", [2, 3, 15, 16, 64, 100, 101, 134, 256, 2018, 4096, 8192, 16384, 1701, 9000, 40022, 65534,
-                               201, 40027])
+                               201, 40027, 131072, 262144])
 def test_real_vs_oracle(ffb, torch_cuda, n, double):
     torch = torch_cuda
     batch = 4
