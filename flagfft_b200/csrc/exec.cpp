@@ -500,6 +500,7 @@ class Builder {
     const bool rows_only = io == IoKind::C2C && L > 1 && pp_per > limit && rows_per <= limit && ii == 1 &&
                            ok == 1 && ii <= ig && fixed_sequence(L, &seq) && seq == sorted_r;
     a.pp = (io == IoKind::C2C && L > 1 && (pp_per <= limit || rows_only)) ? 1 : 0;
+    a.rows_only = (a.pp && pp_per > limit) ? 1 : 0;
     // ping-pong cores run their radices largest first (any order is the same
     // DFT; this one matches the compile-time sequences), and a convolution's
     // inverse core the same order; the in-place pair needs DIF then DIT with
@@ -1419,9 +1420,11 @@ std::unique_ptr<BatchProgram> lower_batch_t(const std::vector<BatchGroup> &group
   for (auto &g : bp->groups)
     for (auto &ps : g.prog->passes) {
       auto *tp = dynamic_cast<TilePass<T> *>(ps.get());
-      if (!tp || !tp->a.pp || tp->a.regcol || tp->a.blue_cols || tp->a.tiles || tp->a.tpt > kBatchWidth) continue;
+      if (!tp || !tp->a.pp || tp->a.regcol || tp->a.blue_cols || tp->a.tiles || tp->a.rows_only ||
+          tp->a.tpt > kBatchWidth)
+        continue;
       TileArgs<T> &a = tp->a;
-      const size_t per = tp->smem / (size_t)a.W;
+      const size_t per = pp_tile_smem(a) / (size_t)a.W;
       int64_t W = std::min<int64_t>({(int64_t)(kBatchWidth / a.tpt), (int64_t)a.G,
                                      (int64_t)std::max<size_t>(1, 110 * 1024 / per)});
       W = std::max<int64_t>(W, a.W);
@@ -1443,18 +1446,21 @@ std::unique_ptr<BatchProgram> lower_batch_t(const std::vector<BatchGroup> &group
       if (auto *tp = dynamic_cast<const TilePass<T> *>(g.prog->passes[pi].get())) {
         if (tp->a.regcol) {
           kind = kBatchRegcol;
-        } else if (tp->a.pp && !tp->a.blue_cols && !tp->a.tiles && tp->io == IoKind::C2C) {
+        } else if (tp->a.pp && !tp->a.blue_cols && !tp->a.tiles && !tp->a.rows_only && tp->io == IoKind::C2C) {
           kind = tp->kind == CoreKind::Dit         ? kBatchPpDit
                  : tp->kind == CoreKind::Bluestein ? kBatchPpBluestein
                  : tp->kind == CoreKind::Rader     ? kBatchPpRader
                                                    : kBatchPpConv;
         }
-        if (kind >= 0 && kind != kBatchRegcol && tp->smem + kBatchSmemHeader > 232448) kind = -1;
+        // a persistent item runs the general ping-pong body: size its shared
+        // memory from the tile itself
+        const size_t item_smem = kind >= 0 && kind != kBatchRegcol ? pp_tile_smem(tp->a) : 0;
+        if (kind >= 0 && kind != kBatchRegcol && item_smem + kBatchSmemHeader > 232448) kind = -1;
         if (kind >= 0) {
-          cls = batch_class(tp->smem, tp->a.W * tp->a.tpt, kind == kBatchRegcol);
+          cls = batch_class(item_smem, tp->a.W * tp->a.tpt, kind == kBatchRegcol);
           auto &L = ph.cls[cls];
           L.threads = std::max(L.threads, kind == kBatchRegcol ? 128 : tp->a.W * tp->a.tpt);
-          L.smem = std::max(L.smem, kind == kBatchRegcol ? (size_t)0 : tp->smem);
+          L.smem = std::max(L.smem, item_smem);
         }
       }
       ph.passes.push_back({(int)gi, (int)pi, kind, cls});

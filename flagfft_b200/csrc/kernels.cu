@@ -183,6 +183,7 @@ cudaError_t launch_tile(const TileArgs<T> &a, CoreKind kind, IoKind io, size_t s
                                      : rows::launch_rows_any<T, 3, false>(a, smem, s);
       if (e != cudaErrorNotSupported) return e;
     }
+    if (a.rows_only) return cudaErrorInvalidConfiguration;  // no general tile fits its shared memory
     if (k == 0 || k == 1 || k == 3) {
       const cudaError_t e = k == 0 ? (a.inv ? tile::launch_pp_fixed_any<T, 0, true>(a, smem, s)
                                             : tile::launch_pp_fixed_any<T, 0, false>(a, smem, s))

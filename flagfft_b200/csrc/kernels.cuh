@@ -114,7 +114,17 @@ struct TileArgs {
   // 1: strided tile kernel of a compile-time sequence (tiles.cuh): W is its
   // fixed tile width, one shared buffer per transform.
   int tiles;
+  // 1: a ping-pong pass only a row kernel can run (its one buffer per row
+  // fits shared memory, two do not); never a general ping-pong tile.
+  int rows_only;
 };
+
+// Shared memory the general ping-pong tile body needs for a pass's W
+// transforms (two buffers and three spare elements per transform).
+template <typename T>
+inline size_t pp_tile_smem(const TileArgs<T> &a) {
+  return (size_t)a.W * (2 * (size_t)pp_size(a.core.L) + 3) * sizeof(cpx<T>);
+}
 
 // Real-transform pre/post processing between the passes of a multi-pass
 // R2C / C2R (L = n/2 complex points per transform, rtw[k] = W_n^k, k <= L):

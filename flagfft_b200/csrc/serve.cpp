@@ -286,13 +286,13 @@ class Server {
         int kind = -1;
         if (a.regcol) {
           kind = kBatchRegcol;
-        } else if (a.pp && !a.blue_cols && !a.tiles && tp->io == IoKind::C2C) {
+        } else if (a.pp && !a.blue_cols && !a.tiles && !a.rows_only && tp->io == IoKind::C2C) {
           kind = tp->kind == CoreKind::Dit         ? kBatchPpDit
                  : tp->kind == CoreKind::Bluestein ? kBatchPpBluestein
                  : tp->kind == CoreKind::Rader     ? kBatchPpRader
                                                    : kBatchPpConv;
           // the request's own tile width (independent of the other requests)
-          const size_t per = tp->smem / (size_t)tp->a.W;
+          const size_t per = pp_tile_smem(tp->a) / (size_t)tp->a.W;
           if (a.tpt <= kBatchWidth) {
             int64_t W = std::min<int64_t>({(int64_t)(kBatchWidth / a.tpt), (int64_t)a.G,
                                            (int64_t)std::max<size_t>(1, 110 * 1024 / per)});

@@ -11,9 +11,10 @@ from oracle import oracle as O
 pytestmark = pytest.mark.gpu
 
 # single-pass (Stockham, fused Bluestein, fused Rader), two-pass four-step and
-# three-pass Bluestein lengths side by side
-LENGTHS = [16, 2, 13, 67, 1009, 1701, 4096, 10007, 20020, 65536, 12289]
-COUNTS = [5, 3, 4, 2, 3, 2, 2, 2, 1, 1, 1]
+# three-pass Bluestein lengths side by side, and 16384 (single precision: a
+# row-kernel pass that launches on its own beside the persistent launches)
+LENGTHS = [16, 2, 13, 67, 1009, 1701, 4096, 10007, 20020, 65536, 12289, 16384]
+COUNTS = [5, 3, 4, 2, 3, 2, 2, 2, 1, 1, 1, 2]
 
 
 def _check_groups(got, x, lengths, counts, direction, double):
