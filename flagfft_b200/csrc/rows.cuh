@@ -479,8 +479,8 @@ FFB_HD void rows_body(const TileArgs<T> &a, long long bx, long long by, cpx<T> *
   }
 }
 
-template <typename T, int KIND, bool INV, int L, int... Rs>
-__global__ void __launch_bounds__(tile::TileBounds<T>::kMaxThreads) k_rows(const __grid_constant__ TileArgs<T> a) {
+template <typename T, int KIND, bool INV, int MB, int L, int... Rs>
+__global__ void __launch_bounds__(tile::TileBounds<T>::kMaxThreads, MB) k_rows(const __grid_constant__ TileArgs<T> a) {
   extern __shared__ __align__(16) unsigned char smraw[];
   constexpr int TPT = rows_tpt<T, L, Rs...>();
   rows_body<T, KIND, INV, L, TPT, DevT, Rs...>(a, (long long)blockIdx.x, (long long)blockIdx.y,
@@ -505,20 +505,33 @@ size_t rows_smem(const TileArgs<T> &a) {
 }
 
 #ifndef FFB_HOST_EMULATION
-template <typename T, int KIND, bool INV, int L, int... Rs>
-cudaError_t launch_rows(const TileArgs<T> &a, cudaStream_t s) {
+template <typename T, int KIND, bool INV, int MB, int L, int... Rs>
+cudaError_t launch_rows_mb(const TileArgs<T> &a, cudaStream_t s) {
   static bool configured = false;
   if (!configured) {
-    cudaError_t e =
-        cudaFuncSetAttribute(k_rows<T, KIND, INV, L, Rs...>, cudaFuncAttributeMaxDynamicSharedMemorySize, 232448);
+    cudaError_t e = cudaFuncSetAttribute(k_rows<T, KIND, INV, MB, L, Rs...>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, 232448);
     if (e != cudaSuccess) return e;
     configured = true;
   }
   constexpr int TPT = rows_tpt<T, L, Rs...>();
   dim3 grid((unsigned)((a.G + a.W - 1) / a.W), (unsigned)a.nbatch, 1);
   dim3 block((unsigned)(a.W * TPT), 1, 1);
-  k_rows<T, KIND, INV, L, Rs...><<<grid, block, rows_smem<T, L>(a), s>>>(a);
+  k_rows<T, KIND, INV, MB, L, Rs...><<<grid, block, rows_smem<T, L>(a), s>>>(a);
   return cudaGetLastError();
+}
+// Double-precision transforms of up to 4096 points are compiled for two
+// CTAs per SM (at most 128 registers, no spills): without the bound the
+// compiler took 146-208 registers and left one 256-thread CTA per SM
+// (Z2Z 4096 x 8192: 274 us against 200 us with it).  The convolution kernels
+// ran slower with it, and 8192 points would spill.
+template <typename T, int KIND, int L>
+constexpr int rows_min_blocks() {
+  return sizeof(T) == 8 && KIND == 0 && L <= 4096 ? 2 : 1;
+}
+template <typename T, int KIND, bool INV, int L, int... Rs>
+cudaError_t launch_rows(const TileArgs<T> &a, cudaStream_t s) {
+  return launch_rows_mb<T, KIND, INV, rows_min_blocks<T, KIND, L>(), L, Rs...>(a, s);
 }
 #else
 template <typename T, int KIND, bool INV, int L, int... Rs>
