@@ -9,13 +9,7 @@ namespace ffb {
 #ifndef FFB_HOST_EMULATION
 template <typename T>
 static cudaError_t batch_configure() {
-  static bool done = false;
-  if (!done) {
-    cudaError_t e = cudaFuncSetAttribute(batch::k_batch<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 232448);
-    if (e != cudaSuccess) return e;
-    done = true;
-  }
-  return cudaSuccess;
+  return set_smem_limit_once<batch::k_batch<T>>(232448);
 }
 
 template <typename T>

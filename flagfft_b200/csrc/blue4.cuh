@@ -181,12 +181,9 @@ constexpr size_t smem_of() {
 #ifndef FFB_HOST_EMULATION
 template <typename T, int N1, int L2, int... Rs>
 cudaError_t launch(const TileArgs<T> &a, cudaStream_t s) {
-  static bool configured = false;
-  if (!configured) {
-    cudaError_t e = cudaFuncSetAttribute(k_blue4<T, N1, L2, Rs...>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem_of<T, N1, L2>());
+  {
+    cudaError_t e = set_smem_limit_once<k_blue4<T, N1, L2, Rs...>>((int)smem_of<T, N1, L2>());
     if (e != cudaSuccess) return e;
-    configured = true;
   }
   k_blue4<T, N1, L2, Rs...><<<dim3((unsigned)a.nbatch), dim3(Shape<N1, L2, Rs...>::NT), smem_of<T, N1, L2>(), s>>>(a);
   return cudaGetLastError();

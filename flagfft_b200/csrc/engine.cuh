@@ -27,6 +27,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "device_once.hpp"
+
 // Every engine function is host+device: the host build runs the same code
 // sequentially (one "thread", barriers as no-ops) to check index arithmetic
 // without a GPU.
@@ -38,6 +40,24 @@
 namespace ffb {
 
 #include "roots.inc"
+
+#ifndef FFB_HOST_EMULATION
+// Raises Kernel's dynamic shared-memory limit to `bytes` on the current
+// device, once per device (the attribute belongs to the device).  One flag
+// set per kernel instantiation: Kernel is a template argument, so kernels of
+// the same signature keep separate flags.
+template <auto Kernel>
+inline cudaError_t set_smem_limit_once(int bytes) {
+  static DeviceOnce once;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (once.done(dev)) return cudaSuccess;
+  e = cudaFuncSetAttribute(Kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess) once.mark(dev);
+  return e;
+}
+#endif
 
 template <typename T>
 struct alignas(2 * sizeof(T)) cpx {

@@ -173,8 +173,8 @@ extern "C" flagfftResult flagfftB200ExecC2CNoAlloc(const flagfftComplex *idata, 
                                                    int batch, int direction, flagfftStream_t stream) {
   if (idata == nullptr || odata == nullptr || batch <= 0) return FLAGFFT_INVALID_VALUE;
   if (direction != FLAGFFT_FORWARD && direction != FLAGFFT_INVERSE) return FLAGFFT_INVALID_VALUE;
-  if (n < 2 * kRootLen || n > (1 << 24) || (n & (n - 1)) != 0) {
-    std::fprintf(stderr, "[flagfft] ExecC2CNoAlloc: n=%d must be a power of two in [8192, 2^24]\n", n);
+  if (n < 2 * kRootLen || (long long)n > kNoAllocMaxElems || (n & (n - 1)) != 0) {
+    std::fprintf(stderr, "[flagfft] ExecC2CNoAlloc: n=%d must be a power of two in [8192, 2^22]\n", n);
     return FLAGFFT_INVALID_SIZE;
   }
   if ((long long)n * batch > kNoAllocMaxElems || batch > 65535) {

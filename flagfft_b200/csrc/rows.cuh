@@ -507,12 +507,9 @@ size_t rows_smem(const TileArgs<T> &a) {
 #ifndef FFB_HOST_EMULATION
 template <typename T, int KIND, bool INV, int MB, int L, int... Rs>
 cudaError_t launch_rows_mb(const TileArgs<T> &a, cudaStream_t s) {
-  static bool configured = false;
-  if (!configured) {
-    cudaError_t e = cudaFuncSetAttribute(k_rows<T, KIND, INV, MB, L, Rs...>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, 232448);
+  {
+    cudaError_t e = set_smem_limit_once<k_rows<T, KIND, INV, MB, L, Rs...>>(232448);
     if (e != cudaSuccess) return e;
-    configured = true;
   }
   constexpr int TPT = rows_tpt<T, L, Rs...>();
   dim3 grid((unsigned)((a.G + a.W - 1) / a.W), (unsigned)a.nbatch, 1);

@@ -555,12 +555,9 @@ FFB_HD bool core_is(const Core &c) {
 #ifndef FFB_HOST_EMULATION
 template <typename T, int KIND, bool INV, int L, int... Rs>
 cudaError_t launch_pp_fixed(const TileArgs<T> &a, size_t smem, cudaStream_t s) {
-  static bool configured = false;
-  if (!configured) {
-    cudaError_t e = cudaFuncSetAttribute(k_tile_pp_fixed<T, KIND, INV, L, Rs...>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, 232448);
+  {
+    cudaError_t e = set_smem_limit_once<k_tile_pp_fixed<T, KIND, INV, L, Rs...>>(232448);
     if (e != cudaSuccess) return e;
-    configured = true;
   }
   dim3 grid((unsigned)((a.G + a.W - 1) / a.W), (unsigned)a.nbatch, 1);
   dim3 block((unsigned)(a.W * a.tpt), 1, 1);
@@ -598,11 +595,9 @@ cudaError_t launch_pp_fixed_any(const TileArgs<T> &a, size_t smem, cudaStream_t 
 #ifndef FFB_HOST_EMULATION
 template <typename T, int KIND, int IO>
 cudaError_t launch_one(const TileArgs<T> &a, size_t smem, cudaStream_t s) {
-  static bool configured = false;
-  if (!configured) {
-    cudaError_t e = cudaFuncSetAttribute(k_tile<T, KIND, IO>, cudaFuncAttributeMaxDynamicSharedMemorySize, 232448);
+  {
+    cudaError_t e = set_smem_limit_once<k_tile<T, KIND, IO>>(232448);
     if (e != cudaSuccess) return e;
-    configured = true;
   }
   dim3 grid((unsigned)((a.G + a.W - 1) / a.W), (unsigned)a.nbatch, 1);
   dim3 block((unsigned)(a.W * a.tpt), 1, 1);
@@ -611,12 +606,9 @@ cudaError_t launch_one(const TileArgs<T> &a, size_t smem, cudaStream_t s) {
 }
 template <typename T, int KIND, bool INV>
 cudaError_t launch_pp(const TileArgs<T> &a, size_t smem, cudaStream_t s) {
-  static bool configured = false;
-  if (!configured) {
-    cudaError_t e =
-        cudaFuncSetAttribute(k_tile_pp<T, KIND, INV>, cudaFuncAttributeMaxDynamicSharedMemorySize, 232448);
+  {
+    cudaError_t e = set_smem_limit_once<k_tile_pp<T, KIND, INV>>(232448);
     if (e != cudaSuccess) return e;
-    configured = true;
   }
   dim3 grid((unsigned)((a.G + a.W - 1) / a.W), (unsigned)a.nbatch, 1);
   dim3 block((unsigned)(a.W * a.tpt), 1, 1);

@@ -237,12 +237,9 @@ constexpr size_t smem_of() {
 #ifndef FFB_HOST_EMULATION
 template <typename T, bool INV, int L, int... Rs>
 cudaError_t launch(const TileArgs<T> &a, cudaStream_t s) {
-  static bool configured = false;
-  if (!configured) {
-    cudaError_t e = cudaFuncSetAttribute(k_tiles<T, INV, L, Rs...>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem_of<T, L, Rs...>());
+  {
+    cudaError_t e = set_smem_limit_once<k_tiles<T, INV, L, Rs...>>((int)smem_of<T, L, Rs...>());
     if (e != cudaSuccess) return e;
-    configured = true;
   }
   using Sh = Shape<T, L, Rs...>;
   dim3 grid((unsigned)((a.G + Sh::W - 1) / Sh::W), (unsigned)a.nbatch, 1);

@@ -107,7 +107,7 @@ FLAGFFT_API flagfftResult flagfftB200ServerStats(flagfftB200Server srv, long lon
                                                 long long *bytes_in_use);
 FLAGFFT_API flagfftResult flagfftB200ServerDestroy(flagfftB200Server srv);
 
-/* Batched complex64 FFT of power-of-two length n (8192 <= n <= 2^24) that
+/* Batched complex64 FFT of power-of-two length n (8192 <= n <= 2^22) that
  * allocates no memory.  No counterpart in the reference.
  *
  * For callers that cannot call cudaMalloc when they transform: code running

@@ -22,11 +22,14 @@
  *   direct     [4, n]
  */
 #include <math.h>
+#include <pthread.h>
 #include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
+#include <unistd.h>
 
 #define FFO_PI 3.14159265358979323846264338327950288
+#define FFO_PI_L 3.14159265358979323846264338327950288L
 
 enum { FFO_LEAF = 0, FFO_FOUR_STEP = 1, FFO_BLUESTEIN = 2, FFO_RADER = 3, FFO_DIRECT = 4 };
 
@@ -37,12 +40,17 @@ typedef struct ffo_node {
   int nfactors;
   int64_t n1, n2, m, root;
   struct ffo_node *a, *b;
+  /* Bluestein / Rader: FFT of the kernel sequence for the sign `kern_sign`,
+   * computed once per call before the rows run (ffo_impl.h prepare) */
+  void *kern;
+  int kern_sign;
 } ffo_node;
 
 static void ffo_free(ffo_node *nd) {
   if (!nd) return;
   ffo_free(nd->a);
   ffo_free(nd->b);
+  free(nd->kern);
   free(nd);
 }
 
@@ -103,34 +111,102 @@ static ffo_node *ffo_parse(const int64_t *code, int64_t *pos) {
   return nd;
 }
 
-/* Cache of cos/sin(2*pi*m/n), m < n, for n up to 2^20 (computed in double,
- * the precision the reference builds its tables in).  The oracle is single-
- * threaded per process. */
-#define FFO_ROOT_SLOTS 1024
-static int64_t ffo_root_n[FFO_ROOT_SLOTS];
-static double *ffo_root_tab[FFO_ROOT_SLOTS];
+/* Parallel loop over [0, count) on the host's cores (pthreads): threads take
+ * indices from a shared counter.  `ffo_in_worker` marks the worker threads so
+ * a loop reached from inside one runs serially.  FFO_THREADS caps the threads. */
+static __thread int ffo_in_worker;
 
-static const double *ffo_unit_roots(int64_t n) {
-  if (n <= 0 || n > (1 << 20)) return NULL;
-  uint64_t h = ((uint64_t)n * 0x9e3779b97f4a7c15ULL) >> 54;
-  for (int probe = 0; probe < FFO_ROOT_SLOTS; ++probe) {
-    int slot = (int)((h + (uint64_t)probe) % FFO_ROOT_SLOTS);
-    if (ffo_root_n[slot] == n) return ffo_root_tab[slot];
-    if (ffo_root_n[slot] == 0) {
-      double *t = (double *)malloc(sizeof(double) * 2 * (size_t)n);
-      for (int64_t m = 0; m < n; ++m) {
-        double a = 2.0 * FFO_PI * (double)m / (double)n;
-        t[2 * m] = cos(a);
-        t[2 * m + 1] = sin(a);
-      }
-      ffo_root_n[slot] = n;
-      ffo_root_tab[slot] = t;
-      return t;
-    }
+typedef struct {
+  void (*body)(void *ctx, int64_t i);
+  void *ctx;
+  int64_t count;
+  int64_t next;
+} ffo_loop;
+
+static void *ffo_loop_worker(void *arg) {
+  ffo_loop *lp = (ffo_loop *)arg;
+  ffo_in_worker = 1;
+  for (;;) {
+    int64_t i = __atomic_fetch_add(&lp->next, 1, __ATOMIC_RELAXED);
+    if (i >= lp->count) break;
+    lp->body(lp->ctx, i);
   }
   return NULL;
 }
 
+static int ffo_threads(void) {
+  const char *e = getenv("FFO_THREADS");
+  long t = e ? strtol(e, NULL, 10) : sysconf(_SC_NPROCESSORS_ONLN);
+  if (t < 1) t = 1;
+  if (t > 256) t = 256;
+  return (int)t;
+}
+
+static void ffo_parallel_for(int64_t count, void (*body)(void *, int64_t), void *ctx) {
+  int nt = ffo_in_worker ? 1 : ffo_threads();
+  if (nt > count) nt = (int)count;
+  if (nt <= 1) {
+    for (int64_t i = 0; i < count; ++i) body(ctx, i);
+    return;
+  }
+  ffo_loop lp = {body, ctx, count, 0};
+  pthread_t th[256];
+  int started = 0;
+  for (int t = 0; t < nt - 1; ++t)
+    if (pthread_create(&th[started], NULL, ffo_loop_worker, &lp) == 0) ++started;
+  ffo_loop_worker(&lp);
+  ffo_in_worker = 0;
+  for (int t = 0; t < started; ++t) pthread_join(th[t], NULL);
+}
+
+/* Cache of cos/sin(2*pi*m/n), m < n, for n up to 2^20 (computed in double,
+ * the precision the reference builds its tables in).  Rows run on several
+ * OpenMP threads: a slot is claimed under a lock and published by storing its
+ * length after its table (release), which readers load with acquire. */
+#define FFO_ROOT_SLOTS 1024
+#define FFO_ROOT_CACHE(NAME, T, COS, SIN, PI)                                                          \
+  static int64_t NAME##_n[FFO_ROOT_SLOTS];                                                             \
+  static T *NAME##_tab[FFO_ROOT_SLOTS];                                                                \
+  static pthread_mutex_t NAME##_lock = PTHREAD_MUTEX_INITIALIZER;                                      \
+  static const T *NAME(int64_t n) {                                                                    \
+    if (n <= 0 || n > (1 << 20)) return NULL;                                                          \
+    uint64_t h = ((uint64_t)n * 0x9e3779b97f4a7c15ULL) >> 54;                                          \
+    for (int pass = 0; pass < 2; ++pass) {                                                             \
+      if (pass == 1) pthread_mutex_lock(&NAME##_lock);                                                 \
+      for (int probe = 0; probe < FFO_ROOT_SLOTS; ++probe) {                                           \
+        int slot = (int)((h + (uint64_t)probe) % FFO_ROOT_SLOTS);                                      \
+        int64_t have = __atomic_load_n(&NAME##_n[slot], __ATOMIC_ACQUIRE);                             \
+        if (have == n) {                                                                               \
+          if (pass == 1) pthread_mutex_unlock(&NAME##_lock);                                           \
+          return NAME##_tab[slot];                                                                     \
+        }                                                                                              \
+        if (have == 0) {                                                                               \
+          if (pass == 0) break; /* not cached: claim a slot under the lock */                          \
+          T *t = (T *)malloc(sizeof(T) * 2 * (size_t)n);                                               \
+          for (int64_t m = 0; m < n; ++m) {                                                            \
+            T a = 2 * (PI) * (T)m / (T)n;                                                              \
+            t[2 * m] = COS(a);                                                                         \
+            t[2 * m + 1] = SIN(a);                                                                     \
+          }                                                                                            \
+          NAME##_tab[slot] = t;                                                                        \
+          __atomic_store_n(&NAME##_n[slot], n, __ATOMIC_RELEASE);                                      \
+          pthread_mutex_unlock(&NAME##_lock);                                                          \
+          return t;                                                                                    \
+        }                                                                                              \
+      }                                                                                                \
+    }                                                                                                  \
+    pthread_mutex_unlock(&NAME##_lock);                                                                \
+    return NULL;                                                                                       \
+  }
+
+FFO_ROOT_CACHE(ffo_unit_roots, double, cos, sin, FFO_PI)
+FFO_ROOT_CACHE(ffo_unit_roots_l, long double, cosl, sinl, FFO_PI_L)
+
+#define TREAL double
+#define TROOTS ffo_unit_roots
+#define TCOS cos
+#define TSIN sin
+#define TPI FFO_PI
 #define REAL double
 #define SFX(name) name##_d
 #include "ffo_impl.h"
@@ -142,6 +218,31 @@ static const double *ffo_unit_roots(int64_t n) {
 #include "ffo_impl.h"
 #undef REAL
 #undef SFX
+#undef TREAL
+#undef TROOTS
+#undef TCOS
+#undef TSIN
+#undef TPI
+
+/* Long double: the same algorithms with tables, angles and arithmetic in
+ * long double -- a truth about 2^11 times more precise than FP64, used to
+ * measure the error of the FP64 restatement itself (an estimate of the
+ * reference's own FP64 Exec error). */
+#define TREAL long double
+#define TROOTS ffo_unit_roots_l
+#define TCOS cosl
+#define TSIN sinl
+#define TPI FFO_PI_L
+#define REAL long double
+#define SFX(name) name##_l
+#include "ffo_impl.h"
+#undef REAL
+#undef SFX
+#undef TREAL
+#undef TROOTS
+#undef TCOS
+#undef TSIN
+#undef TPI
 
 /* O(n^2) DFT accumulated in long double with the phase index j*k reduced
  * exactly mod n: the independent pin for the FP64 restatement. */

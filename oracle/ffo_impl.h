@@ -8,7 +8,12 @@
  * arithmetic, used to estimate the error the reference's own FP32 Exec
  * output carries).
  *
- * Required macros: REAL, SFX(name) (appends the precision suffix).
+ * Required macros: REAL, SFX(name) (appends the precision suffix), and the
+ * precision tables and angles are built in: TREAL (the table type), TROOTS(n)
+ * (the cached table of n-th roots of unity in TREAL, or NULL), TCOS / TSIN
+ * and TPI.  The FP64 and float builds take their tables in double, as the
+ * reference builds its tables; the long-double build (a more precise truth
+ * used to measure the FP64 restatement's own error) in long double.
  */
 
 typedef struct {
@@ -40,15 +45,15 @@ static SFX(cpx) SFX(conj)(SFX(cpx) a) {
 static SFX(cpx) SFX(root)(int64_t num, int64_t den, int sign) {
   int64_t m = num % den;
   if (m < 0) m += den;
-  const double *tab = ffo_unit_roots(den);
+  const TREAL *tab = TROOTS(den);
   SFX(cpx) r;
   if (tab) {
     r.re = (REAL)tab[2 * m];
     r.im = (REAL)(sign > 0 ? tab[2 * m + 1] : -tab[2 * m + 1]);
   } else {
-    double a = (double)sign * 2.0 * FFO_PI * (double)m / (double)den;
-    r.re = (REAL)cos(a);
-    r.im = (REAL)sin(a);
+    TREAL a = (TREAL)sign * 2 * TPI * (TREAL)m / (TREAL)den;
+    r.re = (REAL)TCOS(a);
+    r.im = (REAL)TSIN(a);
   }
   return r;
 }
@@ -112,35 +117,82 @@ static void SFX(direct)(int64_t n, const SFX(cpx) *in, SFX(cpx) *out, int sign) 
  * python/flagfft_codegen/kernels.py:710-742,796-815): Y[j2][k1] =
  * DFT_n1 over j1 of x[j1*n2 + j2]; Y *= W_N^{j2*k1} (the N-entry table of
  * src/codegen/tables.cpp:116-147); X[k1 + n1*k2] = DFT_n2 over j2. */
-static void SFX(four_step)(const ffo_node *nd, const SFX(cpx) *in, SFX(cpx) *out, int sign) {
+typedef struct {
+  const ffo_node *nd;
+  const SFX(cpx) *in;
+  SFX(cpx) *out, *y;
+  int sign;
+} SFX(fs_ctx);
+
+/* column j2: Y[j2][k1] = DFT_n1 over j1 of x[j1*n2 + j2], times W_N^{j2*k1} */
+static void SFX(fs_column)(void *vc, int64_t j2) {
+  const SFX(fs_ctx) *c = (const SFX(fs_ctx) *)vc;
+  const ffo_node *nd = c->nd;
   int64_t n1 = nd->n1, n2 = nd->n2, n = nd->length;
-  SFX(cpx) *col = (SFX(cpx) *)malloc(sizeof(SFX(cpx)) * (size_t)(n1 > n2 ? n1 : n2));
-  SFX(cpx) *res = (SFX(cpx) *)malloc(sizeof(SFX(cpx)) * (size_t)(n1 > n2 ? n1 : n2));
-  SFX(cpx) *y = (SFX(cpx) *)malloc(sizeof(SFX(cpx)) * (size_t)n);
-  for (int64_t j2 = 0; j2 < n2; ++j2) {
-    for (int64_t j1 = 0; j1 < n1; ++j1) col[j1] = in[j1 * n2 + j2];
-    SFX(exec_node)(nd->a, col, res, sign);
-    for (int64_t k1 = 0; k1 < n1; ++k1) y[j2 * n1 + k1] = SFX(cmul)(res[k1], SFX(root)(j2 * k1, n, sign));
-  }
-  for (int64_t k1 = 0; k1 < n1; ++k1) {
-    for (int64_t j2 = 0; j2 < n2; ++j2) col[j2] = y[j2 * n1 + k1];
-    SFX(exec_node)(nd->b, col, res, sign);
-    for (int64_t k2 = 0; k2 < n2; ++k2) out[k1 + n1 * k2] = res[k2];
-  }
+  SFX(cpx) *col = (SFX(cpx) *)malloc(sizeof(SFX(cpx)) * 2 * (size_t)n1);
+  SFX(cpx) *res = col + n1;
+  for (int64_t j1 = 0; j1 < n1; ++j1) col[j1] = c->in[j1 * n2 + j2];
+  SFX(exec_node)(nd->a, col, res, c->sign);
+  for (int64_t k1 = 0; k1 < n1; ++k1) c->y[j2 * n1 + k1] = SFX(cmul)(res[k1], SFX(root)(j2 * k1, n, c->sign));
   free(col);
-  free(res);
-  free(y);
+}
+
+/* row k1: X[k1 + n1*k2] = DFT_n2 over j2 of Y[j2][k1] */
+static void SFX(fs_row)(void *vc, int64_t k1) {
+  const SFX(fs_ctx) *c = (const SFX(fs_ctx) *)vc;
+  const ffo_node *nd = c->nd;
+  int64_t n1 = nd->n1, n2 = nd->n2;
+  SFX(cpx) *col = (SFX(cpx) *)malloc(sizeof(SFX(cpx)) * 2 * (size_t)n2);
+  SFX(cpx) *res = col + n2;
+  for (int64_t j2 = 0; j2 < n2; ++j2) col[j2] = c->y[j2 * n1 + k1];
+  SFX(exec_node)(nd->b, col, res, c->sign);
+  for (int64_t k2 = 0; k2 < n2; ++k2) c->out[k1 + n1 * k2] = res[k2];
+  free(col);
+}
+
+/* A long transform reached outside a worker thread spreads its (independent)
+ * columns and rows over the host threads. */
+static void SFX(four_step)(const ffo_node *nd, const SFX(cpx) *in, SFX(cpx) *out, int sign) {
+  int64_t n = nd->length;
+  SFX(fs_ctx) c = {nd, in, out, (SFX(cpx) *)malloc(sizeof(SFX(cpx)) * (size_t)n), sign};
+  if (n >= (1 << 15)) {
+    ffo_parallel_for(nd->n2, SFX(fs_column), &c);
+    ffo_parallel_for(nd->n1, SFX(fs_row), &c);
+  } else {
+    for (int64_t j2 = 0; j2 < nd->n2; ++j2) SFX(fs_column)(&c, j2);
+    for (int64_t k1 = 0; k1 < nd->n1; ++k1) SFX(fs_row)(&c, k1);
+  }
+  free(c.y);
 }
 
 /* exp(sign * i*pi * (k^2 mod 2n) / n): the chirp of
  * src/codegen/tables.cpp:149-216 (k^2 reduced mod 2n before the angle). */
 static SFX(cpx) SFX(chirp)(int64_t k, int64_t n, double sign) {
   int64_t red = (int64_t)(((__int128)k * k) % (2 * n));
-  double a = sign * FFO_PI * (double)red / (double)n;
+  TREAL a = (TREAL)sign * TPI * (TREAL)red / (TREAL)n;
   SFX(cpx) r;
-  r.re = (REAL)cos(a);
-  r.im = (REAL)sin(a);
+  r.re = (REAL)TCOS(a);
+  r.im = (REAL)TSIN(a);
   return r;
+}
+
+/* B = FFT_m(b), b[k] = chirp(k) with the conjugate sign, mirrored at m - k
+ * (the reference's lazily built b_fft_buf, src/exec/raw_nodes.cpp:140-151):
+ * the node's cached copy when prepare() made one for this sign. */
+static SFX(cpx) *SFX(bluestein_kernel)(const ffo_node *nd, int sign) {
+  if (nd->kern && nd->kern_sign == sign) return (SFX(cpx) *)nd->kern;
+  int64_t n = nd->length, m = nd->m;
+  double csign = sign > 0 ? 1.0 : -1.0;
+  SFX(cpx) *b = (SFX(cpx) *)calloc((size_t)m, sizeof(SFX(cpx)));
+  SFX(cpx) *bf = (SFX(cpx) *)malloc(sizeof(SFX(cpx)) * (size_t)m);
+  for (int64_t k = 0; k < n; ++k) {
+    SFX(cpx) v = SFX(chirp)(k, n, -csign);
+    b[k] = v;
+    if (k) b[m - k] = v;
+  }
+  SFX(exec_node)(nd->a, b, bf, -1);
+  free(b);
+  return bf;
 }
 
 /* Bluestein chain (src/exec/raw_nodes.cpp:140-204, kernels
@@ -151,16 +203,9 @@ static SFX(cpx) SFX(chirp)(int64_t k, int64_t n, double sign) {
 static void SFX(bluestein)(const ffo_node *nd, const SFX(cpx) *in, SFX(cpx) *out, int sign) {
   int64_t n = nd->length, m = nd->m;
   double csign = sign > 0 ? 1.0 : -1.0;
-  SFX(cpx) *b = (SFX(cpx) *)calloc((size_t)m, sizeof(SFX(cpx)));
-  SFX(cpx) *bf = (SFX(cpx) *)malloc(sizeof(SFX(cpx)) * (size_t)m);
+  SFX(cpx) *bf = SFX(bluestein_kernel)(nd, sign);
   SFX(cpx) *a = (SFX(cpx) *)calloc((size_t)m, sizeof(SFX(cpx)));
   SFX(cpx) *af = (SFX(cpx) *)malloc(sizeof(SFX(cpx)) * (size_t)m);
-  for (int64_t k = 0; k < n; ++k) {
-    SFX(cpx) v = SFX(chirp)(k, n, -csign);
-    b[k] = v;
-    if (k) b[m - k] = v;
-  }
-  SFX(exec_node)(nd->a, b, bf, -1);
   for (int64_t k = 0; k < n; ++k) a[k] = SFX(cmul)(in[k], SFX(chirp)(k, n, csign));
   SFX(exec_node)(nd->a, a, af, -1);
   for (int64_t k = 0; k < m; ++k) a[k] = SFX(conj)(SFX(cmul)(af[k], bf[k]));
@@ -171,10 +216,26 @@ static void SFX(bluestein)(const ffo_node *nd, const SFX(cpx) *in, SFX(cpx) *out
     c.im = -af[k].im / (REAL)m;
     out[k] = SFX(cmul)(c, SFX(chirp)(k, n, csign));
   }
-  free(b);
-  free(bf);
+  if (bf != (SFX(cpx) *)nd->kern) free(bf);
   free(a);
   free(af);
+}
+
+/* FFT_m of b[q] = W_p^{sign g^q} (src/codegen/tables.cpp:218-258): the
+ * node's cached copy when prepare() made one for this sign. */
+static SFX(cpx) *SFX(rader_kernel)(const ffo_node *nd, int sign) {
+  if (nd->kern && nd->kern_sign == sign) return (SFX(cpx) *)nd->kern;
+  int64_t p = nd->length, m = p - 1, g = nd->root;
+  SFX(cpx) *b = (SFX(cpx) *)malloc(sizeof(SFX(cpx)) * (size_t)m);
+  SFX(cpx) *bf = (SFX(cpx) *)malloc(sizeof(SFX(cpx)) * (size_t)m);
+  int64_t v = 1;
+  for (int64_t q = 0; q < m; ++q) {
+    b[q] = SFX(root)(v, p, sign);
+    v = (v * g) % p;
+  }
+  SFX(exec_node)(nd->a, b, bf, -1);
+  free(b);
+  return bf;
 }
 
 /* Rader chain (src/exec/raw_nodes.cpp:240-305, kernels
@@ -191,12 +252,9 @@ static void SFX(rader)(const ffo_node *nd, const SFX(cpx) *in, SFX(cpx) *out, in
     idx[q] = v;
     v = (v * g) % p;
   }
-  SFX(cpx) *b = (SFX(cpx) *)malloc(sizeof(SFX(cpx)) * (size_t)m);
-  SFX(cpx) *bf = (SFX(cpx) *)malloc(sizeof(SFX(cpx)) * (size_t)m);
+  SFX(cpx) *bf = SFX(rader_kernel)(nd, sign);
   SFX(cpx) *a = (SFX(cpx) *)malloc(sizeof(SFX(cpx)) * (size_t)m);
   SFX(cpx) *af = (SFX(cpx) *)malloc(sizeof(SFX(cpx)) * (size_t)m);
-  for (int64_t q = 0; q < m; ++q) b[q] = SFX(root)(idx[q], p, sign);
-  SFX(exec_node)(nd->a, b, bf, -1);
   for (int64_t q = 0; q < m; ++q) a[q] = in[idx[q == 0 ? 0 : m - q]];
   SFX(exec_node)(nd->a, a, af, -1);
   for (int64_t q = 0; q < m; ++q) a[q] = SFX(conj)(SFX(cmul)(af[q], bf[q]));
@@ -211,8 +269,7 @@ static void SFX(rader)(const ffo_node *nd, const SFX(cpx) *in, SFX(cpx) *out, in
   }
   out[0] = s;
   free(idx);
-  free(b);
-  free(bf);
+  if (bf != (SFX(cpx) *)nd->kern) free(bf);
   free(a);
   free(af);
 }
@@ -237,6 +294,75 @@ static void SFX(exec_node)(const ffo_node *nd, const SFX(cpx) *in, SFX(cpx) *out
   }
 }
 
+/* Builds, before the rows run, every Bluestein / Rader kernel spectrum the
+ * tree needs for a transform of this sign (the children of a convolution
+ * always run forward; a four-step's children take its sign).  The rows then
+ * share them read-only. */
+static void SFX(prepare)(ffo_node *nd, int sign) {
+  if (!nd) return;
+  if (nd->kind == FFO_FOUR_STEP) {
+    SFX(prepare)(nd->a, sign);
+    SFX(prepare)(nd->b, sign);
+  } else if (nd->kind == FFO_BLUESTEIN || nd->kind == FFO_RADER) {
+    SFX(prepare)(nd->a, -1);
+    if (nd->kern && nd->kern_sign != sign) {
+      free(nd->kern);
+      nd->kern = NULL;
+    }
+    if (!nd->kern) {
+      nd->kern = nd->kind == FFO_BLUESTEIN ? SFX(bluestein_kernel)(nd, sign) : SFX(rader_kernel)(nd, sign);
+      nd->kern_sign = sign;
+    }
+  }
+}
+
+/* Rows of a batch run on the host threads; a long row runs alone and its
+ * four-step spreads its columns over them instead. */
+typedef struct {
+  const ffo_node *nd;
+  const REAL *in;
+  REAL *out;
+  int64_t idist, odist;
+  int sign, mode; /* mode 0 C2C, 1 R2C, 2 C2R */
+} SFX(rows_ctx);
+
+static void SFX(one_row)(void *vc, int64_t b) {
+  const SFX(rows_ctx) *c = (const SFX(rows_ctx) *)vc;
+  int64_t n = c->nd->length, half = n / 2 + 1;
+  SFX(cpx) *x = (SFX(cpx) *)malloc(sizeof(SFX(cpx)) * 2 * (size_t)n);
+  SFX(cpx) *y = x + n;
+  if (c->mode == 0) {
+    memcpy(x, c->in + 2 * b * c->idist, sizeof(SFX(cpx)) * (size_t)n);
+    SFX(exec_node)(c->nd, x, y, c->sign);
+    memcpy(c->out + 2 * b * c->odist, y, sizeof(SFX(cpx)) * (size_t)n);
+  } else if (c->mode == 1) {
+    for (int64_t k = 0; k < n; ++k) {
+      x[k].re = c->in[b * c->idist + k];
+      x[k].im = 0;
+    }
+    SFX(exec_node)(c->nd, x, y, -1);
+    memcpy(c->out + 2 * b * c->odist, y, sizeof(SFX(cpx)) * (size_t)half);
+  } else {
+    const REAL *row = c->in + 2 * b * c->idist;
+    for (int64_t k = 0; k < n; ++k) {
+      int64_t src = k < half ? k : n - k;
+      x[k].re = row[2 * src];
+      x[k].im = k < half ? row[2 * src + 1] : -row[2 * src + 1];
+      if (k == 0 || (n % 2 == 0 && k == n / 2)) x[k].im = 0;
+    }
+    SFX(exec_node)(c->nd, x, y, 1);
+    for (int64_t k = 0; k < n; ++k) c->out[b * c->odist + k] = y[k].re;
+  }
+  free(x);
+}
+
+static void SFX(run_rows)(const SFX(rows_ctx) *c, int64_t batch) {
+  if (batch > 1 && c->nd->length < (1 << 16))
+    ffo_parallel_for(batch, SFX(one_row), (void *)c);
+  else
+    for (int64_t b = 0; b < batch; ++b) SFX(one_row)((void *)c, b);
+}
+
 /* Batched C2C with element distances idist/odist (contiguous rows). */
 int SFX(ffo_c2c)(const int64_t *code, const REAL *in, REAL *out, int64_t batch, int64_t idist, int64_t odist,
                  int direction) {
@@ -244,16 +370,9 @@ int SFX(ffo_c2c)(const int64_t *code, const REAL *in, REAL *out, int64_t batch, 
   ffo_node *nd = ffo_parse(code, &pos);
   if (!nd) return -1;
   int sign = direction > 0 ? 1 : -1;
-  int64_t n = nd->length;
-  SFX(cpx) *x = (SFX(cpx) *)malloc(sizeof(SFX(cpx)) * (size_t)n);
-  SFX(cpx) *y = (SFX(cpx) *)malloc(sizeof(SFX(cpx)) * (size_t)n);
-  for (int64_t b = 0; b < batch; ++b) {
-    memcpy(x, in + 2 * b * idist, sizeof(SFX(cpx)) * (size_t)n);
-    SFX(exec_node)(nd, x, y, sign);
-    memcpy(out + 2 * b * odist, y, sizeof(SFX(cpx)) * (size_t)n);
-  }
-  free(x);
-  free(y);
+  SFX(prepare)(nd, sign);
+  SFX(rows_ctx) c = {nd, in, out, idist, odist, sign, 0};
+  SFX(run_rows)(&c, batch);
   ffo_free(nd);
   return 0;
 }
@@ -264,19 +383,9 @@ int SFX(ffo_r2c)(const int64_t *code, const REAL *in, REAL *out, int64_t batch, 
   int64_t pos = 0;
   ffo_node *nd = ffo_parse(code, &pos);
   if (!nd) return -1;
-  int64_t n = nd->length, half = n / 2 + 1;
-  SFX(cpx) *x = (SFX(cpx) *)malloc(sizeof(SFX(cpx)) * (size_t)n);
-  SFX(cpx) *y = (SFX(cpx) *)malloc(sizeof(SFX(cpx)) * (size_t)n);
-  for (int64_t b = 0; b < batch; ++b) {
-    for (int64_t k = 0; k < n; ++k) {
-      x[k].re = in[b * idist + k];
-      x[k].im = 0;
-    }
-    SFX(exec_node)(nd, x, y, -1);
-    memcpy(out + 2 * b * odist, y, sizeof(SFX(cpx)) * (size_t)half);
-  }
-  free(x);
-  free(y);
+  SFX(prepare)(nd, -1);
+  SFX(rows_ctx) c = {nd, in, out, idist, odist, -1, 1};
+  SFX(run_rows)(&c, batch);
   ffo_free(nd);
   return 0;
 }
@@ -288,22 +397,9 @@ int SFX(ffo_c2r)(const int64_t *code, const REAL *in, REAL *out, int64_t batch, 
   int64_t pos = 0;
   ffo_node *nd = ffo_parse(code, &pos);
   if (!nd) return -1;
-  int64_t n = nd->length, half = n / 2 + 1;
-  SFX(cpx) *x = (SFX(cpx) *)malloc(sizeof(SFX(cpx)) * (size_t)n);
-  SFX(cpx) *y = (SFX(cpx) *)malloc(sizeof(SFX(cpx)) * (size_t)n);
-  for (int64_t b = 0; b < batch; ++b) {
-    const REAL *row = in + 2 * b * idist;
-    for (int64_t k = 0; k < n; ++k) {
-      int64_t src = k < half ? k : n - k;
-      x[k].re = row[2 * src];
-      x[k].im = k < half ? row[2 * src + 1] : -row[2 * src + 1];
-      if (k == 0 || (n % 2 == 0 && k == n / 2)) x[k].im = 0;
-    }
-    SFX(exec_node)(nd, x, y, 1);
-    for (int64_t k = 0; k < n; ++k) out[b * odist + k] = y[k].re;
-  }
-  free(x);
-  free(y);
+  SFX(prepare)(nd, 1);
+  SFX(rows_ctx) c = {nd, in, out, idist, odist, 1, 2};
+  SFX(run_rows)(&c, batch);
   ffo_free(nd);
   return 0;
 }
@@ -312,6 +408,69 @@ int SFX(ffo_c2r)(const int64_t *code, const REAL *in, REAL *out, int64_t batch, 
  * column FFT along n0; R2C = row R2C along n1, column C2C along n0 over the
  * n1/2+1 kept columns; C2R = column inverse C2C first, then row C2R.
  * kind: 0 C2C, 1 R2C, 2 C2R.  row_code/col_code are the n1 and n0 plans. */
+typedef struct {
+  const ffo_node *row, *col;
+  const REAL *src;
+  REAL *dst;
+  SFX(cpx) *grid;
+  int64_t n0, n1, h1;
+  int sign, csign, kind;
+} SFX(grid_ctx);
+
+/* first half of a 2-D transform, row r of the grid: C2C row FFT, or R2C
+ * (expand, forward FFT, keep the half spectrum) */
+static void SFX(grid_row_in)(void *vc, int64_t r) {
+  const SFX(grid_ctx) *c = (const SFX(grid_ctx) *)vc;
+  int64_t n1 = c->n1;
+  SFX(cpx) *t = (SFX(cpx) *)malloc(sizeof(SFX(cpx)) * 2 * (size_t)n1);
+  SFX(cpx) *u = t + n1;
+  if (c->kind == 0) {
+    SFX(exec_node)(c->row, (const SFX(cpx) *)c->src + r * n1, c->grid + r * n1, c->sign);
+  } else {
+    for (int64_t k = 0; k < n1; ++k) {
+      t[k].re = c->src[r * n1 + k];
+      t[k].im = 0;
+    }
+    SFX(exec_node)(c->row, t, u, -1);
+    memcpy(c->grid + r * n1, u, sizeof(SFX(cpx)) * (size_t)c->h1);
+  }
+  free(t);
+}
+
+/* column cc of the grid */
+static void SFX(grid_col)(void *vc, int64_t cc) {
+  const SFX(grid_ctx) *c = (const SFX(grid_ctx) *)vc;
+  int64_t n0 = c->n0, n1 = c->n1;
+  SFX(cpx) *t = (SFX(cpx) *)malloc(sizeof(SFX(cpx)) * 2 * (size_t)n0);
+  SFX(cpx) *u = t + n0;
+  for (int64_t r = 0; r < n0; ++r) t[r] = c->grid[r * n1 + cc];
+  SFX(exec_node)(c->col, t, u, c->csign);
+  for (int64_t r = 0; r < n0; ++r) c->grid[r * n1 + cc] = u[r];
+  free(t);
+}
+
+/* last half of a 2-D C2R, row r: Hermitian expansion, inverse FFT, real part */
+static void SFX(grid_row_out)(void *vc, int64_t r) {
+  const SFX(grid_ctx) *c = (const SFX(grid_ctx) *)vc;
+  int64_t n1 = c->n1, h1 = c->h1;
+  SFX(cpx) *t = (SFX(cpx) *)malloc(sizeof(SFX(cpx)) * 2 * (size_t)n1);
+  SFX(cpx) *u = t + n1;
+  for (int64_t k = 0; k < n1; ++k) {
+    int64_t s = k < h1 ? k : n1 - k;
+    t[k] = c->grid[r * n1 + s];
+    if (k >= h1) t[k].im = -t[k].im;
+    if (k == 0 || (n1 % 2 == 0 && k == n1 / 2)) t[k].im = 0;
+  }
+  SFX(exec_node)(c->row, t, u, 1);
+  for (int64_t k = 0; k < n1; ++k) c->dst[r * n1 + k] = u[k].re;
+  free(t);
+}
+
+/* 2-D RTRT (src/exec/raw_nodes.cpp:549-852): C2C = row FFT along n1 then
+ * column FFT along n0; R2C = row R2C along n1, column C2C along n0 over the
+ * n1/2+1 kept columns; C2R = column inverse C2C first, then row C2R.
+ * kind: 0 C2C, 1 R2C, 2 C2R.  row_code/col_code are the n1 and n0 plans.
+ * The rows, then the columns, run on the host threads. */
 int SFX(ffo_2d)(int kind, const int64_t *row_code, const int64_t *col_code, int64_t n0, int64_t n1,
                 const REAL *in, REAL *out, int64_t batch, int direction) {
   int64_t p0 = 0, p1 = 0;
@@ -321,55 +480,34 @@ int SFX(ffo_2d)(int kind, const int64_t *row_code, const int64_t *col_code, int6
   int sign = direction > 0 ? 1 : -1;
   int64_t h1 = n1 / 2 + 1;
   int64_t ncols = kind == 0 ? n1 : h1;
+  int csign = kind == 1 ? -1 : (kind == 2 ? 1 : sign);
+  SFX(prepare)(row, kind == 0 ? sign : (kind == 1 ? -1 : 1));
+  SFX(prepare)(col, csign);
   SFX(cpx) *grid = (SFX(cpx) *)malloc(sizeof(SFX(cpx)) * (size_t)(n0 * n1));
-  SFX(cpx) *t = (SFX(cpx) *)malloc(sizeof(SFX(cpx)) * (size_t)(n0 > n1 ? n0 : n1));
-  SFX(cpx) *u = (SFX(cpx) *)malloc(sizeof(SFX(cpx)) * (size_t)(n0 > n1 ? n0 : n1));
   for (int64_t b = 0; b < batch; ++b) {
+    SFX(grid_ctx) c = {row, col, NULL, NULL, grid, n0, n1, h1, sign, csign, kind};
     if (kind == 0) {
-      const SFX(cpx) *src = (const SFX(cpx) *)in + b * n0 * n1;
-      for (int64_t r = 0; r < n0; ++r) SFX(exec_node)(row, src + r * n1, grid + r * n1, sign);
+      c.src = in + 2 * b * n0 * n1;
+      ffo_parallel_for(n0, SFX(grid_row_in), &c);
     } else if (kind == 1) {
-      const REAL *src = in + b * n0 * n1;
-      for (int64_t r = 0; r < n0; ++r) {
-        for (int64_t k = 0; k < n1; ++k) {
-          t[k].re = src[r * n1 + k];
-          t[k].im = 0;
-        }
-        SFX(exec_node)(row, t, u, -1);
-        memcpy(grid + r * n1, u, sizeof(SFX(cpx)) * (size_t)h1);
-      }
+      c.src = in + b * n0 * n1;
+      ffo_parallel_for(n0, SFX(grid_row_in), &c);
     } else {
       const SFX(cpx) *src = (const SFX(cpx) *)in + b * n0 * h1;
       for (int64_t r = 0; r < n0; ++r) memcpy(grid + r * n1, src + r * h1, sizeof(SFX(cpx)) * (size_t)h1);
     }
-    int csign = kind == 1 ? -1 : (kind == 2 ? 1 : sign);
-    for (int64_t c = 0; c < ncols; ++c) {
-      for (int64_t r = 0; r < n0; ++r) t[r] = grid[r * n1 + c];
-      SFX(exec_node)(col, t, u, csign);
-      for (int64_t r = 0; r < n0; ++r) grid[r * n1 + c] = u[r];
-    }
+    ffo_parallel_for(ncols, SFX(grid_col), &c);
     if (kind == 0) {
       memcpy((SFX(cpx) *)out + b * n0 * n1, grid, sizeof(SFX(cpx)) * (size_t)(n0 * n1));
     } else if (kind == 1) {
       SFX(cpx) *dst = (SFX(cpx) *)out + b * n0 * h1;
       for (int64_t r = 0; r < n0; ++r) memcpy(dst + r * h1, grid + r * n1, sizeof(SFX(cpx)) * (size_t)h1);
     } else {
-      REAL *dst = out + b * n0 * n1;
-      for (int64_t r = 0; r < n0; ++r) {
-        for (int64_t k = 0; k < n1; ++k) {
-          int64_t s = k < h1 ? k : n1 - k;
-          t[k] = grid[r * n1 + s];
-          if (k >= h1) t[k].im = -t[k].im;
-          if (k == 0 || (n1 % 2 == 0 && k == n1 / 2)) t[k].im = 0;
-        }
-        SFX(exec_node)(row, t, u, 1);
-        for (int64_t k = 0; k < n1; ++k) dst[r * n1 + k] = u[k].re;
-      }
+      c.dst = out + b * n0 * n1;
+      ffo_parallel_for(n0, SFX(grid_row_out), &c);
     }
   }
   free(grid);
-  free(t);
-  free(u);
   ffo_free(row);
   ffo_free(col);
   return 0;

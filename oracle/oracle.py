@@ -51,7 +51,7 @@ def lib():
             build()
         _LIB = ctypes.CDLL(str(path))
         i64, vp, ci = ctypes.c_int64, ctypes.c_void_p, ctypes.c_int
-        for sfx in ("_d", "_f"):
+        for sfx in ("_d", "_f", "_l"):
             getattr(_LIB, "ffo_c2c" + sfx).argtypes = [vp, vp, vp, i64, i64, i64, ci]
             getattr(_LIB, "ffo_r2c" + sfx).argtypes = [vp, vp, vp, i64, i64, i64]
             getattr(_LIB, "ffo_c2r" + sfx).argtypes = [vp, vp, vp, i64, i64, i64]
@@ -167,8 +167,20 @@ def _ptr(a: np.ndarray):
     return a.ctypes.data_as(ctypes.c_void_p)
 
 
+_PRECISIONS = {"f64": ("_d", np.float64, np.complex128), "f32": ("_f", np.float32, np.complex64),
+               "f80": ("_l", np.longdouble, np.clongdouble)}
+
+
 def _real_dtype(precision: str):
-    return np.float64 if precision == "f64" else np.float32
+    return _PRECISIONS[precision][1]
+
+
+def _cplx_dtype(precision: str):
+    return _PRECISIONS[precision][2]
+
+
+def _fn(name: str, precision: str):
+    return getattr(lib(), name + _PRECISIONS[precision][0])
 
 
 def c2c(x: np.ndarray, direction: int, plan: dict | None = None, precision: str = "f64") -> np.ndarray:
@@ -177,11 +189,11 @@ def c2c(x: np.ndarray, direction: int, plan: dict | None = None, precision: str 
     n = x.shape[-1]
     plan = plan or default_plan(n)
     rd = _real_dtype(precision)
-    cd = np.complex128 if precision == "f64" else np.complex64
+    cd = _cplx_dtype(precision)
     xin = np.ascontiguousarray(x.reshape(-1, n), dtype=cd)
     out = np.empty_like(xin)
     code = plan_code(plan)
-    fn = lib().ffo_c2c_d if precision == "f64" else lib().ffo_c2c_f
+    fn = _fn("ffo_c2c", precision)
     rc = fn(_ptr(code), _ptr(xin.view(rd)), _ptr(out.view(rd)), xin.shape[0], n, n, int(direction))
     if rc != 0:
         raise ValueError("oracle rejected the plan tree")
@@ -193,12 +205,12 @@ def r2c(x: np.ndarray, plan: dict | None = None, precision: str = "f64") -> np.n
     n = x.shape[-1]
     plan = plan or default_plan(n)
     rd = _real_dtype(precision)
-    cd = np.complex128 if precision == "f64" else np.complex64
+    cd = _cplx_dtype(precision)
     xin = np.ascontiguousarray(x.reshape(-1, n), dtype=rd)
     half = n // 2 + 1
     out = np.empty((xin.shape[0], half), dtype=cd)
     code = plan_code(plan)
-    fn = lib().ffo_r2c_d if precision == "f64" else lib().ffo_r2c_f
+    fn = _fn("ffo_r2c", precision)
     if fn(_ptr(code), _ptr(xin), _ptr(out.view(rd)), xin.shape[0], n, half) != 0:
         raise ValueError("oracle rejected the plan tree")
     return out.reshape(*x.shape[:-1], half)
@@ -210,11 +222,11 @@ def c2r(x: np.ndarray, n: int, plan: dict | None = None, precision: str = "f64")
     assert x.shape[-1] == half
     plan = plan or default_plan(n)
     rd = _real_dtype(precision)
-    cd = np.complex128 if precision == "f64" else np.complex64
+    cd = _cplx_dtype(precision)
     xin = np.ascontiguousarray(x.reshape(-1, half), dtype=cd)
     out = np.empty((xin.shape[0], n), dtype=rd)
     code = plan_code(plan)
-    fn = lib().ffo_c2r_d if precision == "f64" else lib().ffo_c2r_f
+    fn = _fn("ffo_c2r", precision)
     if fn(_ptr(code), _ptr(xin.view(rd)), _ptr(out), xin.shape[0], half, n) != 0:
         raise ValueError("oracle rejected the plan tree")
     return out.reshape(*x.shape[:-1], n)
@@ -233,7 +245,7 @@ def fft2(x: np.ndarray, kind: str, direction: int = -1, n1: int | None = None,
     row_plan = row_plan or default_plan(n1)
     col_plan = col_plan or default_plan(n0)
     rd = _real_dtype(precision)
-    cd = np.complex128 if precision == "f64" else np.complex64
+    cd = _cplx_dtype(precision)
     k = {"c2c": 0, "r2c": 1, "c2r": 2}[kind]
     if k == 1:
         xin = np.ascontiguousarray(x.reshape(-1, n0, n1), dtype=rd)
@@ -248,7 +260,7 @@ def fft2(x: np.ndarray, kind: str, direction: int = -1, n1: int | None = None,
         out = np.empty_like(xin)
         outshape = x.shape
     rc_, cc_ = plan_code(row_plan), plan_code(col_plan)
-    fn = lib().ffo_2d_d if precision == "f64" else lib().ffo_2d_f
+    fn = _fn("ffo_2d", precision)
     if fn(k, _ptr(rc_), _ptr(cc_), n0, n1, _ptr(xin), _ptr(out), xin.shape[0], int(direction)) != 0:
         raise ValueError("oracle rejected the plan tree")
     return out.reshape(outshape)

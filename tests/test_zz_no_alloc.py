@@ -30,7 +30,8 @@ def _plan_path(ffb, x, n, batch, direction):
     return out
 
 
-@pytest.mark.parametrize("n,batch", [(8192, 8), (65536, 4), (1 << 20, 2), (1 << 22, 1)])
+# (1 << 17, 8) reaches the 512-point pass (radices 16, 16, 2)
+@pytest.mark.parametrize("n,batch", [(8192, 8), (65536, 4), (1 << 17, 8), (1 << 20, 2), (1 << 22, 1)])
 def test_no_alloc_matches_plan_path_twice(ffb, torch_cuda, n, batch):
     torch = torch_cuda
     fn = ffb.LIB.flagfftB200ExecC2CNoAlloc
@@ -59,7 +60,28 @@ def test_no_alloc_rejects_oversize_and_bad_lengths(ffb, torch_cuda):
     x = torch.zeros(16, dtype=torch.complex64, device="cuda")
     p = ctypes.c_void_p(x.data_ptr())
     assert fn(p, p, 1 << 22, 2, ffb.FORWARD, None) == 8        # batch * n above the fixed workspace
+    assert fn(p, p, 1 << 23, 1, ffb.FORWARD, None) == 8        # n above the fixed workspace
     assert fn(p, p, 12288, 1, ffb.FORWARD, None) == 8          # not a power of two
     assert fn(p, p, 4096, 1, ffb.FORWARD, None) == 8           # below the four-step range
     assert fn(None, p, 8192, 1, ffb.FORWARD, None) == 4
     assert fn(p, p, 8192, 1, 0, None) == 4
+
+
+def test_no_alloc_matches_fp64_oracle_2p20(ffb, torch_cuda):
+    """2^20 x 4 against the FP64 oracle itself (relative L2 <= 5e-7 log2 N per
+    transform), forward and inverse, on the reference harness's seeded input."""
+    from oracle import oracle as O
+    torch = torch_cuda
+    fn = ffb.LIB.flagfftB200ExecC2CNoAlloc
+    fn.restype = ctypes.c_int
+    fn.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
+    n, batch = 1 << 20, 4
+    x = O.random_complex(n * batch, O.accuracy_seed(O.C2C, n, batch)).reshape(batch, n)
+    dx = torch.from_numpy(x).cuda()
+    dy = torch.empty_like(dx)
+    for direction in (ffb.FORWARD, ffb.INVERSE):
+        rc = fn(ctypes.c_void_p(dx.data_ptr()), ctypes.c_void_p(dy.data_ptr()), n, batch, direction, None)
+        assert rc == 0
+        torch.cuda.synchronize()
+        err = O.error_stats(dy.cpu().numpy(), O.c2c(x.astype(np.complex128), direction))
+        assert err["finite"] and err["rel_l2"] <= O.north_star_bound(O.C2C, n), err
