@@ -78,7 +78,11 @@ def _load():
         "flagfftB200ServerWait": (i, [H, ctypes.c_longlong, ctypes.POINTER(ctypes.c_double)]),
         "flagfftB200ServerStats": (i, [H, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong),
                                        ctypes.POINTER(ctypes.c_longlong)]),
+        "flagfftB200ServerWaitFor": (i, [H, ctypes.c_longlong, ctypes.c_double, ctypes.POINTER(ctypes.c_double),
+                                         ctypes.POINTER(i)]),
+        "flagfftB200ServerOverlap": (i, [H, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)]),
         "flagfftB200ServerDestroy": (i, [H]),
+        "flagfftB200DeviceWaitFailures": (i, [ctypes.POINTER(ctypes.c_longlong)]),
         "flagfftB200Tune": (i, [i, i, i, i, cp, cp, i, ctypes.POINTER(ctypes.c_double)]),
         "flagfftB200TuneCandidates": (i, [i, i, cp, i]),
     }
@@ -278,17 +282,29 @@ class Server:
                                               ctypes.c_void_p(_ptr(odata)), ctypes.byref(t)), "flagfftB200ServerSubmit")
         return t.value
 
-    def wait(self, ticket: int) -> float:
-        """Blocks until the request finished; returns its latency in ms."""
+    def wait(self, ticket: int, timeout_s: float | None = None) -> float:
+        """Blocks until the request finished (at most timeout_s seconds when
+        given: TimeoutError then, and the ticket stays valid); returns its
+        latency in ms."""
         ms = ctypes.c_double(0)
-        _check(_lib().flagfftB200ServerWait(self._h, ticket, ctypes.byref(ms)), "flagfftB200ServerWait")
+        if timeout_s is None:
+            _check(_lib().flagfftB200ServerWait(self._h, ticket, ctypes.byref(ms)), "flagfftB200ServerWait")
+            return ms.value
+        done = ctypes.c_int(0)
+        _check(_lib().flagfftB200ServerWaitFor(self._h, ticket, timeout_s * 1e3, ctypes.byref(ms), ctypes.byref(done)),
+               "flagfftB200ServerWaitFor")
+        if not done.value:
+            raise TimeoutError(f"request {ticket} not finished after {timeout_s} s")
         return ms.value
 
     def stats(self) -> dict:
         c, t, u = ctypes.c_longlong(), ctypes.c_longlong(), ctypes.c_longlong()
         _check(_lib().flagfftB200ServerStats(self._h, ctypes.byref(c), ctypes.byref(t), ctypes.byref(u)),
                "flagfftB200ServerStats")
-        return {"completed": c.value, "ticks": t.value, "bytes_in_use": u.value}
+        m, a = ctypes.c_longlong(), ctypes.c_longlong()
+        _check(_lib().flagfftB200ServerOverlap(self._h, ctypes.byref(m), ctypes.byref(a)), "flagfftB200ServerOverlap")
+        return {"completed": c.value, "ticks": t.value, "bytes_in_use": u.value, "max_ticks_in_flight": m.value,
+                "admitted_while_busy": a.value}
 
     def close(self) -> None:
         if self._h:
@@ -330,6 +346,14 @@ def planner_tree(n: int, is_double: bool = False, smem_bytes: int = 0) -> dict:
     buf = ctypes.create_string_buffer(need + 1)
     _lib().flagfftB200PlannerTree(n, int(is_double), smem_bytes, buf, need + 1)
     return json.loads(buf.value.decode())
+
+
+def device_wait_failures() -> int:
+    """Bounded device-side waits that gave up on the current device (a copy
+    that never landed); 0 in normal operation."""
+    v = ctypes.c_longlong(0)
+    _check(_lib().flagfftB200DeviceWaitFailures(ctypes.byref(v)), "flagfftB200DeviceWaitFailures")
+    return v.value
 
 
 def version() -> str:

@@ -601,3 +601,11 @@ extern "C" flagfftResult flagfftB200PlanBatch(flagfftHandle *out, int ngroups, c
     return FLAGFFT_SETUP_FAILED;
   }
 }
+
+extern "C" flagfftResult flagfftB200DeviceWaitFailures(long long *count) {
+  if (count == nullptr) return FLAGFFT_INVALID_VALUE;
+  const long long a = ffb::tcols_wait_failures<float>(), b = ffb::tcols_wait_failures<double>();
+  if (a < 0 || b < 0) return FLAGFFT_INVALID_DEVICE;
+  *count = a + b;
+  return FLAGFFT_SUCCESS;
+}

@@ -2,6 +2,10 @@
 // k_f32_batch.cu / k_f64_batch.cu.
 #pragma once
 
+#include <map>
+#include <mutex>
+#include <tuple>
+
 #include "batch.cuh"
 
 namespace ffb {
@@ -24,14 +28,30 @@ cudaError_t launch_batch(const TileArgs<T> *args, const int *kinds, const BatchI
 template <typename T>
 int batch_resident_ctas(int threads, size_t smem) {
   if (batch_configure<T>() != cudaSuccess) return 0;
-  int per_sm = 0, dev = 0, sms = 0;
+  // the occupancy query costs microseconds and a server asks it for every
+  // launch of every tick: remember the answer per (device, threads, smem)
+  static std::mutex mu;
+  static std::map<std::tuple<int, int, size_t>, int> memo;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  const auto key = std::make_tuple(dev, threads, smem);
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = memo.find(key);
+    if (it != memo.end()) return it->second;
+  }
+  int per_sm = 0, sms = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch::k_batch<T>, threads, smem + kBatchSmemHeader) !=
           cudaSuccess ||
-      cudaGetDevice(&dev) != cudaSuccess ||
       cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
     cudaGetLastError();
     return 0;
   }
+  std::lock_guard<std::mutex> lock(mu);
+  memo[key] = per_sm * sms;
   return per_sm * sms;
 }
 #else

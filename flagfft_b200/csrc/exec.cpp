@@ -37,9 +37,18 @@
 
 namespace ffb {
 
+// Host-side fault injection for tests: with FLAGFFT_FAULT_ALLOC=1 every
+// device allocation a plan makes fails as if the device were out of memory
+// (plan creation then returns FLAGFFT_ALLOC_FAILED).  Off unless set.
+static bool alloc_fault_injected() {
+  const char *v = std::getenv("FLAGFFT_FAULT_ALLOC");
+  return v && v[0] == '1';
+}
+
 #ifndef FFB_HOST_EMULATION
 DevMem::DevMem(size_t n) : bytes(n) {
   if (n == 0) return;
+  if (alloc_fault_injected()) throw std::bad_alloc();
   cudaError_t e = cudaMalloc(&ptr, n);
   if (e != cudaSuccess) {
     ptr = nullptr;
@@ -64,6 +73,7 @@ DevPtr upload(const void *host, size_t bytes) {
 // Host-emulation build: "device" memory is host memory.
 DevMem::DevMem(size_t n) : bytes(n) {
   if (n == 0) return;
+  if (alloc_fault_injected()) throw std::bad_alloc();
   ptr = std::malloc(n);
   if (!ptr) throw std::bad_alloc();
 }
@@ -235,6 +245,12 @@ double chain_cost(int64_t m, std::vector<int> *radices, std::unordered_map<int64
     std::sort(radices->rbegin(), radices->rend());
   }
   return cost;
+}
+
+// TMA column passes: on unless FLAGFFT_TMA_COLUMNS=0 (read at plan time).
+static bool tma_columns_enabled() {
+  const char *v = std::getenv("FLAGFFT_TMA_COLUMNS");
+  return !(v && std::string(v) == "0");
 }
 
 // Set while lowering batch groups: the one-pass four-step Bluestein and the
@@ -577,6 +593,19 @@ class Builder {
     }
     a.W = (int)W;
     a.tpt = tpt;
+    // a strided pass of a TMA column sequence: the persistent TMA kernel
+    // (the configuration above stays as its fallback)
+    {
+      int tc_threads = 0;
+      size_t tc_smem = 0;
+      if (spec.kind == CoreKind::Dit && io == IoKind::C2C && a.pp && !t_no_one_pass && tma_columns_enabled() &&
+          fixed_sequence(L, &seq) && seq == sorted_r &&
+          tcols_eligible<T>((int)L, nbatch, G, ib, ig, ii, ob, og, ok, &tc_threads, &tc_smem)) {
+        a.tcols = 1;
+        a.tc_threads = tc_threads;
+        a.tc_smem = (int)tc_smem;
+      }
+    }
     // offsets inside one CTA's tile are 32-bit in the kernels
     if (W * std::llabs(ig) + L * std::llabs(ii) >= (1ll << 31) || W * std::llabs(og) + L * std::llabs(ok) >= (1ll << 31))
       throw std::runtime_error("tile extent above 2^31 elements");
@@ -951,9 +980,18 @@ std::unique_ptr<Program> lower_t(const NodePtr &root, Planner &planner, Transfor
                      : bld.add_pass(sa, IoKind::PackC2C, false, batch, n2, idist, 2, 2 * n2, L, n1, 1, Buf::In,
                                     Buf::Scratch0, n1);
       bld.set_post_twiddle(pa->a, L);
-      // B: FFT over j2 -> Z[k1 + n1 k2] in the output rows
-      bld.add_pass(sb, IoKind::C2C, false, batch, n1, L, 1, n1, odist, 1, n1, Buf::Scratch0, Buf::Out, n2);
-      prog->passes.push_back(std::make_unique<RealPass<T>>(true, Buf::Out, Buf::Out, batch, odist, odist, L, rtw));
+      // B: FFT over j2 -> Z[k1 + n1 k2] in the output rows; when those rows
+      // start off 16-byte boundaries (odd complex64 distances: n/2 + 1), in
+      // place in the workspace, whose rows the TMA column kernel can copy,
+      // and the Hermitian post pass moves the result to the output
+      if (batch > 1 && (odist * (long long)sizeof(cpx<T>)) % 16 != 0) {
+        bld.add_pass(sb, IoKind::C2C, false, batch, n1, L, 1, n1, L, 1, n1, Buf::Scratch0, Buf::Scratch0, n2);
+        prog->passes.push_back(
+            std::make_unique<RealPass<T>>(true, Buf::Scratch0, Buf::Out, batch, L, odist, L, rtw));
+      } else {
+        bld.add_pass(sb, IoKind::C2C, false, batch, n1, L, 1, n1, odist, 1, n1, Buf::Scratch0, Buf::Out, n2);
+        prog->passes.push_back(std::make_unique<RealPass<T>>(true, Buf::Out, Buf::Out, batch, odist, odist, L, rtw));
+      }
     } else {
       prog->scratch1 = std::make_shared<DevMem>((size_t)(batch * L) * sizeof(cpx<T>));
       prog->passes.push_back(

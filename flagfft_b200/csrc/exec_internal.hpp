@@ -79,6 +79,7 @@ struct TilePass final : PassBase {
       << " threads=" << (a.blue_cols ? blue4_threads(a.blue_cols, a.core.L) : a.tiles ? a.tpt : a.W * a.tpt)
       << (a.tiles ? " tiles" : "") << " smem=" << tile_smem<T>(a, kind, io, smem) << " " << buf_name(src) << "->"
       << buf_name(dst);
+    if (a.tcols) o << " tma-columns(threads=" << a.tc_threads << " smem=" << a.tc_smem << ")";
     if (a.post_twiddle) o << " +twiddle";
     if (!note.empty()) o << " (" << note << ")";
     return o.str();

@@ -172,6 +172,10 @@ cudaError_t launch_tile(const TileArgs<T> &a, CoreKind kind, IoKind io, size_t s
   const int k = (int)kind, o = (int)io;
   if (a.regcol) return launch_regcol<T>(a, s);
   if (a.blue_cols) return launch_blue4<T>(a, s);
+  if (a.tcols) {
+    const cudaError_t e = launch_tcols<T>(a, s);
+    if (e != cudaErrorNotSupported) return e;  // else: buffers off the copy rules, the tile kernels below
+  }
   if (a.tiles) return launch_tiles<T>(a, s);
   if (a.pp && o == 0) {
     // compile-time radix sequences first: contiguous rows, then any layout

@@ -117,6 +117,12 @@ struct TileArgs {
   // 1: a ping-pong pass only a row kernel can run (its one buffer per row
   // fits shared memory, two do not); never a general ping-pong tile.
   int rows_only;
+  // 1: a strided pass of a TMA column sequence (tcols.cuh) runs on the
+  // persistent TMA kernel when its buffers meet the copy rules (else on the
+  // configuration above); its threads and shared memory per CTA.
+  int tcols;
+  int tc_threads;
+  int tc_smem;
 };
 
 // Shared memory the general ping-pong tile body needs for a pass's W
@@ -164,6 +170,20 @@ template <typename T>
 cudaError_t launch_tiles(const TileArgs<T> &a, cudaStream_t stream);
 template <typename T>
 bool tiles_shape(int L, int *W, int *threads, size_t *smem);
+
+// TMA column passes (TileArgs::tcols); defined in k_f32_tcols.cu /
+// k_f64_tcols.cu.  launch_tcols returns cudaErrorNotSupported when the
+// pass's buffers break the copy rules; tcols_eligible says at plan time
+// whether a pass of length L with these strides can take it (threads and
+// shared memory per CTA); tcols_wait_failures counts the kernel's bounded
+// waits that gave up on this device (-1: unreadable).
+template <typename T>
+cudaError_t launch_tcols(const TileArgs<T> &a, cudaStream_t stream);
+template <typename T>
+bool tcols_eligible(int L, long long nbatch, long long G, long long ib, long long ig, long long ii, long long ob,
+                    long long og, long long ok, int *threads, size_t *smem);
+template <typename T>
+long long tcols_wait_failures();
 
 // One-pass four-step Bluestein (TileArgs::blue_cols); defined in
 // k_f32_blue4.cu (single precision only).

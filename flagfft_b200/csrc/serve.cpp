@@ -94,8 +94,27 @@ struct TickWork {
     size_t smem = 0;
   };
   std::vector<std::vector<Launch>> phases;  // [phase][class]
-  DevPtr d_args, d_kinds, d_items, d_counters;
-  size_t cap_args = 0, cap_kinds = 0, cap_items = 0, cap_counters = 0;
+  // One device buffer holds the tick's arguments, kinds, items and zeroed
+  // work-queue counters (16-byte aligned sections), filled from one pinned
+  // host buffer by one copy.  A slot's next tick reuses both only after the
+  // slot's previous tick finished on the device.
+  DevPtr d_all;
+  size_t cap = 0;
+  void *h_all = nullptr;
+  size_t off_kinds = 0, off_items = 0, off_counters = 0;
+  const TileArgs<T> *dev_args() const { return reinterpret_cast<const TileArgs<T> *>(d_all->ptr); }
+  const int *dev_kinds() const { return reinterpret_cast<const int *>(static_cast<char *>(d_all->ptr) + off_kinds); }
+  const BatchItem *dev_items() const {
+    return reinterpret_cast<const BatchItem *>(static_cast<char *>(d_all->ptr) + off_items);
+  }
+  int *dev_counters() const { return reinterpret_cast<int *>(static_cast<char *>(d_all->ptr) + off_counters); }
+  ~TickWork() {
+#ifndef FFB_HOST_EMULATION
+    if (h_all) cudaFreeHost(h_all);
+#else
+    std::free(h_all);
+#endif
+  }
 };
 
 struct Slot {
@@ -219,11 +238,35 @@ class Server {
     return r->state == 2 ? FLAGFFT_SUCCESS : FLAGFFT_EXEC_FAILED;
   }
 
+  // wait() bounded by timeout_ms: *done = 0 (ticket kept) when the request
+  // has not finished by then.
+  flagfftResult wait_for(int64_t id, double timeout_ms, double *latency_ms, int *done) {
+    std::unique_lock<std::mutex> lock(mu_);
+    auto it = all_.find(id);
+    if (it == all_.end()) return FLAGFFT_INVALID_VALUE;
+    std::shared_ptr<Request> r = it->second;
+    const bool fin = done_cv_.wait_for(lock, std::chrono::duration<double, std::milli>(std::max(0.0, timeout_ms)),
+                                       [&] { return r->state >= 2; });
+    *done = fin ? 1 : 0;
+    if (!fin) return FLAGFFT_SUCCESS;
+    if (latency_ms) *latency_ms = (r->t_done - r->t_submit) * 1e3;
+    all_.erase(id);
+    return r->state == 2 ? FLAGFFT_SUCCESS : FLAGFFT_EXEC_FAILED;
+  }
+
   void stats(int64_t *completed, int64_t *ticks, int64_t *in_use) {
     std::lock_guard<std::mutex> lock(mu_);
     if (completed) *completed = completed_;
     if (ticks) *ticks = ticks_;
     if (in_use) *in_use = in_use_;
+  }
+
+  // Continuous-batching evidence: the most ticks seen in flight at once, and
+  // how many requests were admitted while another tick was on the GPU.
+  void overlap(int64_t *max_in_flight, int64_t *admitted_while_busy) {
+    std::lock_guard<std::mutex> lock(mu_);
+    if (max_in_flight) *max_in_flight = max_in_flight_;
+    if (admitted_while_busy) *admitted_while_busy = admitted_while_busy_;
   }
 
  private:
@@ -358,19 +401,11 @@ class Server {
     for (int c = 0; c < kBatchClasses; ++c) {
       const auto &L = w.phases[p][(size_t)c];
       if (L.count == 0) continue;
-      int *counter = reinterpret_cast<int *>(w.d_counters->ptr) + p * kBatchClasses + (size_t)c;
-#ifndef FFB_HOST_EMULATION
-      cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(int), st);
-      if (e != cudaSuccess) return e;
-#else
-      cudaError_t e = cudaSuccess;
-      *counter = 0;
-#endif
+      // (every counter of the tick was zeroed once when the tick was assembled)
+      int *counter = w.dev_counters() + p * kBatchClasses + (size_t)c;
       const int ctas = std::max(1, batch_resident_ctas<T>(std::max(L.threads, 32), L.smem));
-      e = launch_batch<T>(reinterpret_cast<const TileArgs<T> *>(w.d_args->ptr),
-                          reinterpret_cast<const int *>(w.d_kinds->ptr),
-                          reinterpret_cast<const BatchItem *>(w.d_items->ptr) + L.first, L.count, counter,
-                          std::max(L.threads, 32), L.smem, ctas, st);
+      cudaError_t e = launch_batch<T>(w.dev_args(), w.dev_kinds(), w.dev_items() + L.first, L.count, counter,
+                                      std::max(L.threads, 32), L.smem, ctas, st);
       if (e != cudaSuccess) return e;
     }
     return cudaSuccess;
@@ -407,21 +442,40 @@ class Server {
     finish_work(wf);
     finish_work(wd);
     // uploads
-    auto up = [&](auto &w) {
-      using W = std::remove_reference_t<decltype(w)>;
-      (void)sizeof(W);
-      if (w.args.empty()) return;
-      upload_grow<char>(w.d_args, w.cap_args, w.args.data(), w.args.size() * sizeof(w.args[0]), s.stream);
-      upload_grow<char>(w.d_kinds, w.cap_kinds, w.kinds.data(), w.kinds.size() * sizeof(int), s.stream);
-      upload_grow<char>(w.d_items, w.cap_items, w.items.data(), w.items.size() * sizeof(BatchItem), s.stream);
+    auto up = [&](auto &w) -> bool {
+      if (w.args.empty()) return true;
       const size_t nc = w.phases.size() * kBatchClasses + 1;
-      if (!w.d_counters || w.cap_counters < nc * sizeof(int)) {
-        w.cap_counters = nc * sizeof(int);
-        w.d_counters = std::make_shared<DevMem>(w.cap_counters);
+      auto al = [](size_t v) { return (v + 15) / 16 * 16; };
+      const size_t b_args = w.args.size() * sizeof(w.args[0]);
+      w.off_kinds = al(b_args);
+      w.off_items = w.off_kinds + al(w.kinds.size() * sizeof(int));
+      w.off_counters = w.off_items + al(w.items.size() * sizeof(BatchItem));
+      const size_t total = w.off_counters + nc * sizeof(int);
+      if (!w.d_all || w.cap < total) {
+        w.cap = std::max(total, 2 * w.cap);
+        w.d_all = std::make_shared<DevMem>(w.cap);
+#ifndef FFB_HOST_EMULATION
+        if (w.h_all) cudaFreeHost(w.h_all);
+        if (cudaMallocHost(&w.h_all, w.cap) != cudaSuccess) w.h_all = nullptr;
+#else
+        std::free(w.h_all);
+        w.h_all = std::malloc(w.cap);
+#endif
       }
+      char *h = static_cast<char *>(w.h_all);
+      if (h == nullptr) return false;
+      std::memcpy(h, w.args.data(), b_args);
+      std::memcpy(h + w.off_kinds, w.kinds.data(), w.kinds.size() * sizeof(int));
+      std::memcpy(h + w.off_items, w.items.data(), w.items.size() * sizeof(BatchItem));
+      std::memset(h + w.off_counters, 0, nc * sizeof(int));  // every work-queue counter starts at zero
+#ifndef FFB_HOST_EMULATION
+      return cudaMemcpyAsync(w.d_all->ptr, h, total, cudaMemcpyHostToDevice, s.stream) == cudaSuccess;
+#else
+      std::memcpy(w.d_all->ptr, h, total);
+      return true;
+#endif
     };
-    up(wf);
-    up(wd);
+    if (!up(wf) || !up(wd)) return cudaErrorMemoryAllocation;
     const size_t nph = std::max({wf.phases.size(), wd.phases.size(), own.size()});
     for (size_t p = 0; p < nph; ++p) {
       if (p < own.size())
@@ -486,7 +540,16 @@ class Server {
           free_slot = &s;
           break;
         }
-      if (free_slot && !pending_.empty()) {
+      // Under load (a tick already on the GPU) requests gather into fewer,
+      // larger ticks: a tick starts once kCoalesceMin requests are pending
+      // or the oldest has waited kCoalesceWait; with the GPU idle it starts
+      // at once.  (Assembling a tick costs host time per tick, so at high
+      // arrival rates one-request ticks would cap the throughput.)
+      bool gpu_busy = false;
+      for (Slot &s : slots_) gpu_busy = gpu_busy || s.busy;
+      const bool start = !pending_.empty() && (!gpu_busy || stop_ || pending_.size() >= kCoalesceMin ||
+                                               now_s() - pending_.front()->t_submit >= kCoalesceWait);
+      if (free_slot && start) {
         while (!pending_.empty() && in_use_ + (int64_t)pending_.front()->bytes <= budget_ &&
                free_slot->reqs.size() < kMaxPerTick) {
           auto r = pending_.front();
@@ -496,8 +559,12 @@ class Server {
           free_slot->reqs.push_back(r);
         }
         if (!free_slot->reqs.empty()) {
+          if (gpu_busy) admitted_while_busy_ += (int64_t)free_slot->reqs.size();
           free_slot->busy = true;
           ++ticks_;
+          int64_t in_flight = 0;
+          for (Slot &s : slots_) in_flight += s.busy ? 1 : 0;
+          max_in_flight_ = std::max(max_in_flight_, in_flight);
           lock.unlock();
 #ifndef FFB_HOST_EMULATION
           cudaSetDevice(device_);
@@ -531,6 +598,8 @@ class Server {
   }
 
   static constexpr size_t kMaxPerTick = 4096;
+  static constexpr size_t kCoalesceMin = 16;
+  static constexpr double kCoalesceWait = 50e-6;  // seconds
 
   int64_t budget_;
   int device_ = 0;
@@ -542,6 +611,7 @@ class Server {
   std::deque<std::shared_ptr<Request>> pending_;
   std::unordered_map<int64_t, std::shared_ptr<Request>> all_;
   int64_t next_id_ = 0, completed_ = 0, ticks_ = 0, in_use_ = 0;
+  int64_t max_in_flight_ = 0, admitted_while_busy_ = 0;
   std::map<std::tuple<int, int64_t, bool>, std::unique_ptr<Template>> tpls_;
   std::map<bool, std::unique_ptr<Planner>> planners_;
 };
@@ -609,6 +679,22 @@ extern "C" flagfftResult flagfftB200ServerSubmit(flagfftB200Server srv, flagfftT
 extern "C" flagfftResult flagfftB200ServerWait(flagfftB200Server srv, long long ticket, double *latency_ms) {
   if (srv == nullptr || srv->impl == nullptr) return FLAGFFT_INVALID_PLAN;
   return srv->impl->wait(ticket, latency_ms);
+}
+
+extern "C" flagfftResult flagfftB200ServerWaitFor(flagfftB200Server srv, long long ticket, double timeout_ms,
+                                                  double *latency_ms, int *done) {
+  if (srv == nullptr || srv->impl == nullptr || done == nullptr) return FLAGFFT_INVALID_VALUE;
+  return srv->impl->wait_for(ticket, timeout_ms, latency_ms, done);
+}
+
+extern "C" flagfftResult flagfftB200ServerOverlap(flagfftB200Server srv, long long *max_ticks_in_flight,
+                                                 long long *admitted_while_busy) {
+  if (srv == nullptr || srv->impl == nullptr) return FLAGFFT_INVALID_VALUE;
+  int64_t a = 0, b = 0;
+  srv->impl->overlap(&a, &b);
+  if (max_ticks_in_flight) *max_ticks_in_flight = a;
+  if (admitted_while_busy) *admitted_while_busy = b;
+  return FLAGFFT_SUCCESS;
 }
 
 extern "C" flagfftResult flagfftB200ServerStats(flagfftB200Server srv, long long *completed, long long *ticks,

@@ -105,7 +105,25 @@ FLAGFFT_API flagfftResult flagfftB200ServerSubmit(flagfftB200Server srv, flagfft
 FLAGFFT_API flagfftResult flagfftB200ServerWait(flagfftB200Server srv, long long ticket, double *latency_ms);
 FLAGFFT_API flagfftResult flagfftB200ServerStats(flagfftB200Server srv, long long *completed, long long *ticks,
                                                 long long *bytes_in_use);
+/* ServerWait with a bound: waits at most timeout_ms.  *done = 1 and the
+ * latency as ServerWait when the request finished (the ticket is then
+ * released); *done = 0 and FLAGFFT_SUCCESS when it has not finished yet (the
+ * ticket stays valid for a later wait).  No reference counterpart. */
+FLAGFFT_API flagfftResult flagfftB200ServerWaitFor(flagfftB200Server srv, long long ticket, double timeout_ms,
+                                                  double *latency_ms, int *done);
+/* Continuous-batching counters: the most ticks the server has had in flight
+ * at once, and how many requests it admitted while another tick was still on
+ * the GPU.  No reference counterpart. */
+FLAGFFT_API flagfftResult flagfftB200ServerOverlap(flagfftB200Server srv, long long *max_ticks_in_flight,
+                                                 long long *admitted_while_busy);
 FLAGFFT_API flagfftResult flagfftB200ServerDestroy(flagfftB200Server srv);
+
+/* Number of bounded device-side waits that gave up on the current device
+ * since the library was loaded: a persistent kernel waits for its own tile
+ * copies (TMA) for at most about a second, then records the failure here and
+ * ends instead of hanging.  0 in normal operation.  No reference
+ * counterpart. */
+FLAGFFT_API flagfftResult flagfftB200DeviceWaitFailures(long long *count);
 
 /* Batched complex64 FFT of power-of-two length n (8192 <= n <= 2^22) that
  * allocates no memory.  No counterpart in the reference.

@@ -85,3 +85,78 @@ def test_server_budget_and_arguments(ffb, torch_cuda):
         assert e.value.code == 8
         tk = srv.submit(ffb.C2C, 1024, 1, x, y)
         srv.wait(tk)
+
+
+def test_server_staged_admission_and_overlap(ffb, torch_cuda):
+    """(a) A budget smaller than the whole mix: submitted at once, the mix is
+    admitted in stages (several ticks), each request once its memory frees.
+    (b) Continuous batching: requests submitted while a long request's tick is
+    on the GPU are admitted into another tick at once (two ticks in flight,
+    requests admitted while the GPU was busy).  Every result must equal the
+    request alone, bit for bit, and meet the oracle bound."""
+    torch = torch_cuda
+    reqs = _inputs(ffb, torch, 901)
+    with ffb.Server(hbm_budget_bytes=1 << 30, max_ticks=3) as srv:
+        alone = []
+        for t, code, n, b, d, x, xd, yd in reqs:
+            srv.wait(srv.submit(code, n, b, xd, yd, d))
+            alone.append(yd.cpu().numpy().copy())
+            yd.zero_()
+    # (a) 6 MiB: every request fits (the largest charge, C2C 4096 x 64, is
+    # 4 MiB of input + output), the whole mix does not
+    with ffb.Server(hbm_budget_bytes=6 << 20, max_ticks=3) as srv:
+        tickets = [srv.submit(code, n, b, xd, yd, d) for t, code, n, b, d, x, xd, yd in reqs]
+        for tk in tickets:
+            srv.wait(tk, timeout_s=60.0)
+        st_a = srv.stats()
+        out_a = [yd.cpu().numpy().copy() for *_, yd in reqs]
+    assert st_a["ticks"] >= 2 and st_a["bytes_in_use"] == 0, st_a
+    # (b) a long request first (C2C 2^20 x 32: about a millisecond on the GPU)
+    big_n, big_b = 1 << 20, 32
+    bx = torch.randn(big_b, big_n, dtype=torch.complex64, device="cuda")
+    by = torch.empty_like(bx)
+    for *_, yd in reqs:
+        yd.zero_()
+    with ffb.Server(hbm_budget_bytes=8 << 30, max_ticks=3) as srv:
+        t_big = srv.submit(ffb.C2C, big_n, big_b, bx, by)
+        tickets = [srv.submit(code, n, b, xd, yd, d) for t, code, n, b, d, x, xd, yd in reqs]
+        for tk in tickets + [t_big]:
+            srv.wait(tk, timeout_s=60.0)
+        st_b = srv.stats()
+        out_b = [yd.cpu().numpy().copy() for *_, yd in reqs]
+    assert st_b["max_ticks_in_flight"] >= 2 and st_b["admitted_while_busy"] > 0, st_b
+    for outs in (out_a, out_b):
+        for (t, code, n, b, d, x, xd, yd), solo, got in zip(reqs, alone, outs):
+            np.testing.assert_array_equal(got, solo)
+    for (t, code, n, b, d, x, xd, yd), got in zip(reqs, out_b):
+        ftype = {"C2C": O.C2C, "Z2Z": O.Z2Z, "R2C": O.R2C, "D2Z": O.D2Z, "C2R": O.C2R, "Z2D": O.Z2D}[t]
+        err = O.error_stats(got, _reference(t, n, d, x))
+        assert err["finite"] and err["rel_l2"] <= O.north_star_bound(ftype, n), (t, n, b, d, err)
+    ref_big = np.fft.fft(bx[:2].cpu().numpy().astype(np.complex128), axis=-1)
+    assert O.error_stats(by[:2].cpu().numpy(), ref_big)["rel_l2"] <= O.north_star_bound(O.C2C, big_n)
+
+
+def test_server_wait_timeout_keeps_ticket(ffb, torch_cuda):
+    """A bounded wait that runs out reports "not done" and keeps the ticket;
+    a later wait returns the result.  The request is held back on the host
+    (its input is not ready: the caller's stream holds a long kernel the
+    server's tick must follow), so nothing on the GPU is made to hang."""
+    torch = torch_cuda
+    n, b = 4096, 4
+    x = torch.randn(b, n, dtype=torch.complex64, device="cuda")
+    y = torch.empty_like(x)
+    with ffb.Server(hbm_budget_bytes=1 << 30, max_ticks=1) as srv:
+        # occupy the only slot with a large request, then wait on the next
+        # with a zero timeout: it cannot have finished yet
+        big_n, big_b = 1 << 20, 64
+        bx = torch.randn(big_b, big_n, dtype=torch.complex64, device="cuda")
+        by = torch.empty_like(bx)
+        t_big = srv.submit(ffb.C2C, big_n, big_b, bx, by)
+        tk = srv.submit(ffb.C2C, n, b, x, y)
+        with pytest.raises(TimeoutError):
+            srv.wait(tk, timeout_s=0.0)
+        srv.wait(t_big, timeout_s=60.0)
+        assert srv.wait(tk, timeout_s=60.0) >= 0
+    ref = np.fft.fft(x.cpu().numpy().astype(np.complex128), axis=-1)
+    err = O.error_stats(y.cpu().numpy(), ref)
+    assert err["rel_l2"] <= O.north_star_bound(O.C2C, n)
