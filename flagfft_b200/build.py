@@ -2,8 +2,9 @@
 
     python -m flagfft_b200.build [--force] [--jobs N]
 
-Objects go to flagfft_b200/_build/; a source is recompiled when it or any
-header in csrc/ is newer than its object.
+Objects go to flagfft_b200/_build/; a source is recompiled when it, or a
+header its nvcc dependency file lists, is newer than its object (any header
+of csrc/ and include/ when there is no dependency file yet).
 """
 from __future__ import annotations
 
@@ -42,8 +43,33 @@ def _headers_mtime() -> float:
     return max((h.stat().st_mtime for h in hs), default=0.0)
 
 
+def _deps(obj: Path) -> list[Path] | None:
+    """Headers an object was built from (its nvcc -MD file), or None."""
+    d = obj.with_suffix(".d")
+    if not d.exists():
+        return None
+    text = d.read_text().replace("\\\n", " ")
+    parts = text.split(":", 1)
+    if len(parts) != 2:
+        return None
+    return [Path(t) for t in parts[1].split() if t]
+
+
+def _stale(src: Path, obj: Path) -> bool:
+    """An object is rebuilt when it is missing or older than its source or
+    any header its dependency file lists (every header in csrc/ and include/
+    when it has none)."""
+    if not obj.exists():
+        return True
+    t = obj.stat().st_mtime
+    deps = _deps(obj)
+    if deps is None:
+        return t < max(src.stat().st_mtime, _headers_mtime())
+    return any((not d.exists()) or d.stat().st_mtime > t for d in [src, *deps])
+
+
 def _compile(src: Path, obj: Path, verbose: bool) -> None:
-    cmd = [nvcc(), *NVCC_COMMON, *ARCH, "-c", str(src), "-o", str(obj)]
+    cmd = [nvcc(), *NVCC_COMMON, *ARCH, "-MD", "-MF", str(obj.with_suffix(".d")), "-c", str(src), "-o", str(obj)]
     if src.suffix == ".cu":
         cmd.insert(1, "-Xptxas=-warn-spills")
     else:
@@ -55,13 +81,12 @@ def _compile(src: Path, obj: Path, verbose: bool) -> None:
 
 def build(force: bool = False, jobs: int | None = None, verbose: bool = False) -> Path:
     BUILD.mkdir(exist_ok=True)
-    hdr = _headers_mtime()
     todo = []
     objs = []
     for src in _sources():
         obj = BUILD / (src.stem + src.suffix.replace(".", "_") + ".o")
         objs.append(obj)
-        if force or not obj.exists() or obj.stat().st_mtime < max(src.stat().st_mtime, hdr):
+        if force or _stale(src, obj):
             todo.append((src, obj))
     jobs = jobs or min(8, os.cpu_count() or 1)
     if todo:
@@ -88,17 +113,17 @@ def build_hostcheck(force: bool = False, jobs: int | None = None, verbose: bool 
     kernels run sequentially on the CPU and "device" memory is host memory.
     Test infrastructure only -- loaded by tests, never by the package."""
     HOSTCHECK_DIR.mkdir(parents=True, exist_ok=True)
-    hdr = _headers_mtime()
     todo, objs = [], []
     for src in _sources():
         obj = HOSTCHECK_DIR / (src.stem + src.suffix.replace(".", "_") + ".o")
         objs.append(obj)
-        if force or not obj.exists() or obj.stat().st_mtime < max(src.stat().st_mtime, hdr):
+        if force or _stale(src, obj):
             todo.append((src, obj))
 
     def comp(src, obj):
         common = [f for f in NVCC_COMMON if f != "-O3"]
-        cmd = [nvcc(), "-x", "cu", *common, "-O2", "-DFFB_HOST_EMULATION", *ARCH, "-c", str(src), "-o", str(obj)]
+        cmd = [nvcc(), "-x", "cu", *common, "-O2", "-DFFB_HOST_EMULATION", *ARCH, "-MD", "-MF",
+               str(obj.with_suffix(".d")), "-c", str(src), "-o", str(obj)]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)

@@ -115,6 +115,7 @@ template <typename T>
 __global__ void __launch_bounds__(tile::TileBounds<T>::kMaxThreads)
     k_batch(const TileArgs<T> *__restrict__ args, const int *__restrict__ kinds, const BatchItem *__restrict__ items,
             int nitems, int *__restrict__ next) {
+  pdl_entry();
   // the queue slot lives in the first 16 bytes of dynamic shared memory (a
   // static __shared__ variable would lower the dynamic limit below 227 KB)
   extern __shared__ __align__(16) unsigned char smraw[];

@@ -21,8 +21,12 @@ cudaError_t launch_batch(const TileArgs<T> *args, const int *kinds, const BatchI
                          int threads, size_t smem, int ctas, cudaStream_t s) {
   cudaError_t e = batch_configure<T>();
   if (e != cudaSuccess) return e;
-  batch::k_batch<T><<<ctas, threads, smem + kBatchSmemHeader, s>>>(args, kinds, items, nitems, next);
-  return cudaGetLastError();
+  // a persistent grid fills every SM: launched with programmatic dependence
+  // its CTAs would take their slots as soon as the previous grid runs, so it
+  // launches plainly (its pdl_entry instructions are then no-ops)
+  PdlOff off;
+  return launch_pdl(batch::k_batch<T>, dim3(ctas), dim3(threads), smem + kBatchSmemHeader, s, args, kinds, items,
+                    nitems, next);
 }
 
 template <typename T>

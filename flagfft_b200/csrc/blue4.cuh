@@ -169,6 +169,7 @@ FFB_HD void blue4_body(const TileArgs<T> &a, long long by, cpx<T> *sm, const X &
 
 template <typename T, int N1, int L2, int... Rs>
 __global__ void __launch_bounds__(Shape<N1, L2, Rs...>::NT) k_blue4(const __grid_constant__ TileArgs<T> a) {
+  pdl_entry();
   extern __shared__ __align__(16) unsigned char smraw[];
   blue4_body<T, N1, L2, rows::DevT, Rs...>(a, (long long)blockIdx.x, reinterpret_cast<cpx<T> *>(smraw), rows::DevT{});
 }
@@ -185,8 +186,7 @@ cudaError_t launch(const TileArgs<T> &a, cudaStream_t s) {
     cudaError_t e = set_smem_limit_once<k_blue4<T, N1, L2, Rs...>>((int)smem_of<T, N1, L2>());
     if (e != cudaSuccess) return e;
   }
-  k_blue4<T, N1, L2, Rs...><<<dim3((unsigned)a.nbatch), dim3(Shape<N1, L2, Rs...>::NT), smem_of<T, N1, L2>(), s>>>(a);
-  return cudaGetLastError();
+  return launch_pdl(k_blue4<T, N1, L2, Rs...>, dim3((unsigned)a.nbatch), dim3(Shape<N1, L2, Rs...>::NT), smem_of<T, N1, L2>(), s, a);
 }
 #else
 template <typename T, int N1, int L2, int... Rs>

@@ -41,7 +41,51 @@ namespace ffb {
 
 #include "roots.inc"
 
+// Programmatic dependent launch.  Every kernel starts with pdl_entry(): it
+// lets the next kernel on the stream begin launching once all of this grid's
+// CTAs run (launch_dependents), then waits for the previous kernel's
+// completion and memory (wait) before it touches global memory.  Launched
+// with the attribute, a kernel's CTAs thus take their SM slots while the
+// previous kernel drains; launched without it, both instructions are no-ops.
+FFB_HD void pdl_entry() {
+#ifdef __CUDA_ARCH__
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+#endif
+}
+
 #ifndef FFB_HOST_EMULATION
+// Whether launches from this thread carry the programmatic-serialization
+// attribute: on unless FLAGFFT_PDL=0 (read once) or the thread turned it off
+// (PdlOff).  Threads that feed several streams at once (the request server)
+// turn it off: a dependent grid's CTAs take SM slots as soon as the previous
+// grid's CTAs all run, and on a busy GPU those slots are what the other
+// streams' kernels are waiting for.
+bool pdl_enabled();
+struct PdlOff {
+  PdlOff();
+  ~PdlOff();
+  bool prev;
+};
+
+// Launches a kernel (one that begins with pdl_entry) with programmatic
+// dependent launch on stream s (a plain launch when pdl_enabled() is false).
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                              Args &&...args) {
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = pdl_enabled() ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+}
+
 // Raises Kernel's dynamic shared-memory limit to `bytes` on the current
 // device, once per device (the attribute belongs to the device).  One flag
 // set per kernel instantiation: Kernel is a template argument, so kernels of

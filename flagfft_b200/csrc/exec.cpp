@@ -37,6 +37,21 @@
 
 namespace ffb {
 
+#ifndef FFB_HOST_EMULATION
+static thread_local bool t_pdl_off = false;
+
+bool pdl_enabled() {
+  static const bool on = [] {
+    const char *v = std::getenv("FLAGFFT_PDL");
+    return !(v && v[0] == '0');
+  }();
+  return on && !t_pdl_off;
+}
+
+PdlOff::PdlOff() : prev(t_pdl_off) { t_pdl_off = true; }
+PdlOff::~PdlOff() { t_pdl_off = prev; }
+#endif
+
 // Host-side fault injection for tests: with FLAGFFT_FAULT_ALLOC=1 every
 // device allocation a plan makes fails as if the device were out of memory
 // (plan creation then returns FLAGFFT_ALLOC_FAILED).  Off unless set.
@@ -666,6 +681,33 @@ class Builder {
     });
   }
 
+  // The same twiddles as two short tables (RealTw): lo[m] = W_n^m, m < split,
+  // hi[m] = W_n^(m split), m <= n/2 / split.
+  RealTw<T> table_rtw_split(int64_t n) {
+    const int64_t half = n / 2;
+    const int64_t split = std::max<int64_t>(1, (int64_t)std::ceil(std::sqrt((double)(half + 1))));
+    const int64_t nhi = half / split + 1;
+    RealTw<T> t{};
+    t.lo = cached<cpx<T>>("rtwlo|" + std::to_string(n) + "|" + std::to_string(split), [&]() {
+      std::vector<cpx<T>> lo((size_t)split);
+      for (int64_t m = 0; m < split; ++m) {
+        cld w = unit_root(m, n, -1);
+        lo[(size_t)m] = mk((T)w.real(), (T)w.imag());
+      }
+      return lo;
+    });
+    t.hi = cached<cpx<T>>("rtwhi|" + std::to_string(n) + "|" + std::to_string(split), [&]() {
+      std::vector<cpx<T>> hi((size_t)nhi);
+      for (int64_t m = 0; m < nhi; ++m) {
+        cld w = unit_root(m * split, n, -1);
+        hi[(size_t)m] = mk((T)w.real(), (T)w.imag());
+      }
+      return hi;
+    });
+    t.split = make_fastdiv((uint32_t)split);
+    return t;
+  }
+
   // Bluestein chirp exp(-+ i pi (j^2 mod 2n) / n), j < n (+ for the inverse).
   const cpx<T> *table_chirp(int64_t n, bool inverse) {
     return cached<cpx<T>>("chirp|" + std::to_string(n) + (inverse ? "|inv" : "|fwd"), [&]() {
@@ -968,7 +1010,7 @@ std::unique_ptr<Program> lower_t(const NodePtr &root, Planner &planner, Transfor
       bld.core_for(core_node->col, sb) && (t == Transform::R2C ? sa.kind : sb.kind) == CoreKind::Dit) {
     if (batch > 65535) throw std::runtime_error("multi-pass batch above 65535");
     const int64_t n1 = core_node->n1, n2 = core_node->n2;
-    const cpx<T> *rtw = bld.table_rtw(n);
+    const RealTw<T> rtw = bld.table_rtw_split(n);
     prog->scratch0 = std::make_shared<DevMem>((size_t)(batch * L) * sizeof(cpx<T>));
     if (t == Transform::R2C) {
       // A: z_j = x_2j + i x_2j+1 (j = j1 n2 + j2), FFT over j1, x W_L^{j2 k1} -> Y[j2][k1];
@@ -1015,7 +1057,7 @@ std::unique_ptr<Program> lower_t(const NodePtr &root, Planner &planner, Transfor
     // pre-processing into a workspace, then the complex transform into the
     // output rows reinterpreted as complex (C2R).
     if (batch > 65535) throw std::runtime_error("multi-pass batch above 65535");
-    const cpx<T> *rtw = bld.table_rtw(n);
+    const RealTw<T> rtw = bld.table_rtw_split(n);
     if (t == Transform::R2C) {
       lower_c2c<T>(bld, *prog, core_node, false, L, batch, idist / 2, odist, Buf::In, Buf::Out);
       prog->passes.push_back(std::make_unique<RealPass<T>>(true, Buf::Out, Buf::Out, batch, odist, odist, L, rtw));

@@ -94,8 +94,8 @@ struct RealPass final : PassBase {
   Buf src, dst;
   long long batch, sdist, ddist;
   int L;
-  const cpx<T> *rtw;
-  RealPass(bool post_, Buf s, Buf d, long long b, long long sd, long long dd, int64_t L_, const cpx<T> *r)
+  RealTw<T> rtw;
+  RealPass(bool post_, Buf s, Buf d, long long b, long long sd, long long dd, int64_t L_, const RealTw<T> &r)
       : post(post_), src(s), dst(d), batch(b), sdist(sd), ddist(dd), L((int)L_), rtw(r) {}
   cudaError_t run(const void *in, void *out, void *s0, void *s1, cudaStream_t st) const override {
     auto *sp = reinterpret_cast<const cpx<T> *>(TilePass<T>::pick(src, in, out, s0, s1));

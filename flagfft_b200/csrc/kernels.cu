@@ -32,11 +32,11 @@ namespace {
 // One thread per pair (k, L-k), k = 0..L/2: reads both Z values, writes both
 // X values, so z and x may alias.
 template <typename T>
-FFB_HD void real_post_pair(const cpx<T> *z, cpx<T> *x, int L, int k, const cpx<T> *rtw) {
+FFB_HD void real_post_pair(const cpx<T> *z, cpx<T> *x, int L, int k, const RealTw<T> &rtw) {
   auto post = [&](cpx<T> zk, cpx<T> zm, int kk) {
     cpx<T> ev = mk((zk.x + zm.x) * (T)0.5, (zk.y - zm.y) * (T)0.5);
     cpx<T> od = mk((zk.y + zm.y) * (T)0.5, (zm.x - zk.x) * (T)0.5);
-    return ev + cmul(ldg_c(rtw + kk), od);
+    return ev + cmul(real_tw(rtw, (uint32_t)kk), od);
   };
   const int m = L - k;
   cpx<T> zk = z[k == 0 ? 0 : k];
@@ -48,7 +48,7 @@ FFB_HD void real_post_pair(const cpx<T> *z, cpx<T> *x, int L, int k, const cpx<T
 }
 
 template <typename T>
-FFB_HD void real_pre_one(const cpx<T> *x, cpx<T> *z, int L, int k, const cpx<T> *rtw) {
+FFB_HD void real_pre_one(const cpx<T> *x, cpx<T> *z, int L, int k, const RealTw<T> &rtw) {
   cpx<T> xk = x[k], xm = x[L - k];
   if (k == 0) {
     xk.y = (T)0;
@@ -56,21 +56,23 @@ FFB_HD void real_pre_one(const cpx<T> *x, cpx<T> *z, int L, int k, const cpx<T> 
   }
   cpx<T> s = mk(xk.x + xm.x, xk.y - xm.y);
   cpx<T> d = mk(xk.x - xm.x, xk.y + xm.y);
-  cpx<T> w = ldg_c(rtw + k);
+  cpx<T> w = real_tw(rtw, (uint32_t)k);
   cpx<T> dw = mk(d.x * w.x + d.y * w.y, d.y * w.x - d.x * w.y);
   z[k] = mk(s.x - dw.y, s.y + dw.x);
 }
 
 template <typename T>
 __global__ void k_real_post(const cpx<T> *z, cpx<T> *x, long long zdist, long long xdist, int L,
-                            const cpx<T> *rtw) {
+                            const RealTw<T> rtw) {
+  pdl_entry();
   const long long b = blockIdx.y;
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k <= L / 2; k += gridDim.x * blockDim.x)
     real_post_pair<T>(z + b * zdist, x + b * xdist, L, k, rtw);
 }
 
 template <typename T>
-__global__ void k_real_pre(const cpx<T> *x, cpx<T> *z, long long xdist, long long zdist, int L, const cpx<T> *rtw) {
+__global__ void k_real_pre(const cpx<T> *x, cpx<T> *z, long long xdist, long long zdist, int L, const RealTw<T> rtw) {
+  pdl_entry();
   const long long b = blockIdx.y;
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < L; k += gridDim.x * blockDim.x)
     real_pre_one<T>(x + b * xdist, z + b * zdist, L, k, rtw);
@@ -80,12 +82,11 @@ __global__ void k_real_pre(const cpx<T> *x, cpx<T> *z, long long xdist, long lon
 
 template <typename T>
 cudaError_t launch_real_post(const cpx<T> *z, cpx<T> *x, long long batch, long long zdist, long long xdist, int L,
-                             const cpx<T> *rtw, cudaStream_t s) {
+                             const RealTw<T> &rtw, cudaStream_t s) {
 #ifndef FFB_HOST_EMULATION
   const int threads = 256;
   const int blocks = (int)std::min<long long>((L / 2 + threads) / threads, 1024);
-  k_real_post<T><<<dim3(blocks, (unsigned)batch), threads, 0, s>>>(z, x, zdist, xdist, L, rtw);
-  return cudaGetLastError();
+  return launch_pdl(k_real_post<T>, dim3(blocks, (unsigned)batch), dim3(threads), 0, s, z, x, zdist, xdist, L, rtw);
 #else
   for (long long b = 0; b < batch; ++b)
     for (int k = 0; k <= L / 2; ++k) real_post_pair<T>(z + b * zdist, x + b * xdist, L, k, rtw);
@@ -95,12 +96,11 @@ cudaError_t launch_real_post(const cpx<T> *z, cpx<T> *x, long long batch, long l
 
 template <typename T>
 cudaError_t launch_real_pre(const cpx<T> *x, cpx<T> *z, long long batch, long long xdist, long long zdist, int L,
-                            const cpx<T> *rtw, cudaStream_t s) {
+                            const RealTw<T> &rtw, cudaStream_t s) {
 #ifndef FFB_HOST_EMULATION
   const int threads = 256;
   const int blocks = (int)std::min<long long>((L + threads - 1) / threads, 2048);
-  k_real_pre<T><<<dim3(blocks, (unsigned)batch), threads, 0, s>>>(x, z, xdist, zdist, L, rtw);
-  return cudaGetLastError();
+  return launch_pdl(k_real_pre<T>, dim3(blocks, (unsigned)batch), dim3(threads), 0, s, x, z, xdist, zdist, L, rtw);
 #else
   for (long long b = 0; b < batch; ++b)
     for (int k = 0; k < L; ++k) real_pre_one<T>(x + b * xdist, z + b * zdist, L, k, rtw);
@@ -130,6 +130,7 @@ FFB_HD void real_convert_one(int mode, const void *src, void *dst, long long sdi
 template <typename T>
 __global__ void k_real_convert(int mode, const void *src, void *dst, long long batch, long long sdist,
                                long long ddist, long long n, long long count) {
+  pdl_entry();
   const long long b = blockIdx.y;
   for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < count; k += (long long)gridDim.x * blockDim.x)
     real_convert_one<T>(mode, src, dst, sdist, ddist, n, b, k);
@@ -143,8 +144,8 @@ cudaError_t launch_real_convert(int mode, const void *src, void *dst, long long 
 #ifndef FFB_HOST_EMULATION
   const int threads = 256;
   const int blocks = (int)std::min<long long>((count + threads - 1) / threads, 2048);
-  k_real_convert<T><<<dim3(blocks, (unsigned)batch), threads, 0, s>>>(mode, src, dst, batch, sdist, ddist, n, count);
-  return cudaGetLastError();
+  return launch_pdl(k_real_convert<T>, dim3(blocks, (unsigned)batch), dim3(threads), 0, s, mode, src, dst, batch, sdist,
+                    ddist, n, count);
 #else
   (void)s;
   for (long long b = 0; b < batch; ++b)
@@ -159,13 +160,13 @@ template cudaError_t launch_real_convert<double>(int, const void *, void *, long
                                                  cudaStream_t);
 
 template cudaError_t launch_real_post<float>(const cpx<float> *, cpx<float> *, long long, long long, long long, int,
-                                             const cpx<float> *, cudaStream_t);
+                                             const RealTw<float> &, cudaStream_t);
 template cudaError_t launch_real_post<double>(const cpx<double> *, cpx<double> *, long long, long long, long long,
-                                              int, const cpx<double> *, cudaStream_t);
+                                              int, const RealTw<double> &, cudaStream_t);
 template cudaError_t launch_real_pre<float>(const cpx<float> *, cpx<float> *, long long, long long, long long, int,
-                                            const cpx<float> *, cudaStream_t);
+                                            const RealTw<float> &, cudaStream_t);
 template cudaError_t launch_real_pre<double>(const cpx<double> *, cpx<double> *, long long, long long, long long,
-                                             int, const cpx<double> *, cudaStream_t);
+                                             int, const RealTw<double> &, cudaStream_t);
 
 template <typename T>
 cudaError_t launch_tile(const TileArgs<T> &a, CoreKind kind, IoKind io, size_t smem, cudaStream_t s) {

@@ -149,12 +149,28 @@ template <typename T>
 cudaError_t launch_real_convert(int mode, const void *src, void *dst, long long batch, long long sdist,
                                 long long ddist, long long n, cudaStream_t stream);
 
+// Real-transform twiddles W_n^k, k <= n/2, as two short tables:
+// W_n^k = hi[k / split] * lo[k % split] (lo: split entries, hi: n/2/split + 1),
+// so a long transform's twiddles stay cache resident instead of streaming an
+// n/2-entry table beside the data.
+template <typename T>
+struct RealTw {
+  const cpx<T> *lo;
+  const cpx<T> *hi;
+  FastDiv split;
+};
+template <typename T>
+FFB_HD cpx<T> real_tw(const RealTw<T> &t, uint32_t k) {
+  const uint32_t q = fdiv(k, t.split);
+  return cmul(ldg_c(t.hi + q), ldg_c(t.lo + (k - q * t.split.d)));
+}
+
 template <typename T>
 cudaError_t launch_real_post(const cpx<T> *z, cpx<T> *x, long long batch, long long zdist, long long xdist, int L,
-                             const cpx<T> *rtw, cudaStream_t stream);
+                             const RealTw<T> &rtw, cudaStream_t stream);
 template <typename T>
 cudaError_t launch_real_pre(const cpx<T> *x, cpx<T> *z, long long batch, long long xdist, long long zdist, int L,
-                            const cpx<T> *rtw, cudaStream_t stream);
+                            const RealTw<T> &rtw, cudaStream_t stream);
 
 template <typename T>
 cudaError_t launch_tile(const TileArgs<T> &a, CoreKind kind, IoKind io, size_t smem_bytes, cudaStream_t stream);

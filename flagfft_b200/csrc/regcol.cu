@@ -17,6 +17,7 @@ constexpr int kRegcolThreads = 128;
 
 template <typename T, int R, bool INV>
 __global__ void __launch_bounds__(kRegcolThreads) k_regcol(const __grid_constant__ TileArgs<T> a) {
+  pdl_entry();
   const long long g = (long long)blockIdx.x * kRegcolThreads + threadIdx.x;
   if (g < a.G) regcol_transform<T, R, INV>(a, (long long)blockIdx.y, g);
 }
@@ -25,8 +26,7 @@ template <typename T, int R, bool INV>
 cudaError_t launch_dir(const TileArgs<T> &a, cudaStream_t s) {
 #ifndef FFB_HOST_EMULATION
   dim3 grid((unsigned)((a.G + kRegcolThreads - 1) / kRegcolThreads), (unsigned)a.nbatch, 1);
-  k_regcol<T, R, INV><<<grid, kRegcolThreads, 0, s>>>(a);
-  return cudaGetLastError();
+  return launch_pdl(k_regcol<T, R, INV>, grid, dim3(kRegcolThreads), 0, s, a);
 #else
   (void)s;
   for (long long by = 0; by < a.nbatch; ++by)

@@ -481,6 +481,7 @@ FFB_HD void rows_body(const TileArgs<T> &a, long long bx, long long by, cpx<T> *
 
 template <typename T, int KIND, bool INV, int MB, int L, int... Rs>
 __global__ void __launch_bounds__(tile::TileBounds<T>::kMaxThreads, MB) k_rows(const __grid_constant__ TileArgs<T> a) {
+  pdl_entry();
   extern __shared__ __align__(16) unsigned char smraw[];
   constexpr int TPT = rows_tpt<T, L, Rs...>();
   rows_body<T, KIND, INV, L, TPT, DevT, Rs...>(a, (long long)blockIdx.x, (long long)blockIdx.y,
@@ -514,8 +515,7 @@ cudaError_t launch_rows_mb(const TileArgs<T> &a, cudaStream_t s) {
   constexpr int TPT = rows_tpt<T, L, Rs...>();
   dim3 grid((unsigned)((a.G + a.W - 1) / a.W), (unsigned)a.nbatch, 1);
   dim3 block((unsigned)(a.W * TPT), 1, 1);
-  k_rows<T, KIND, INV, MB, L, Rs...><<<grid, block, rows_smem<T, L>(a), s>>>(a);
-  return cudaGetLastError();
+  return launch_pdl(k_rows<T, KIND, INV, MB, L, Rs...>, grid, block, rows_smem<T, L>(a), s, a);
 }
 // Double-precision transforms of up to 4096 points are compiled for two
 // CTAs per SM (at most 128 registers, no spills): without the bound the

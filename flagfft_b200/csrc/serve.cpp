@@ -517,6 +517,9 @@ class Server {
   }
 
   void loop() {
+#ifndef FFB_HOST_EMULATION
+    PdlOff no_pdl;  // this thread feeds several streams at once
+#endif
     std::unique_lock<std::mutex> lock(mu_);
     while (true) {
       bool progressed = false;

@@ -4,20 +4,22 @@
 // A strided pass over transforms of L points (element i of transform g at
 // g + i * ii: a column of a row-major matrix) is coalesced only when a CTA
 // moves several adjacent columns at once, and at L = 4096 the columns one CTA
-// can hold (a padded buffer per transform) fill its shared memory: the plain
-// tile kernel then loads, transforms and stores one tile after the other with
-// nothing to overlap.  Here a persistent CTA walks a sequence of column groups
-// (GC adjacent transforms) and keeps two raw landing buffers beside one padded
-// working buffer:
-//   * the TMA unit loads group i + 1 into one raw buffer while the threads
-//     transform group i (the load is issued right after group i's first
-//     stage, once the store that last read that buffer has drained);
-//   * stage 0 reads group i's raw tile (dense, the layout the copy left) and
-//     writes the padded working buffer; the middle stages run in place there
-//     (values held in registers across a barrier); the last stage writes the
-//     output tile into the raw buffer in the output's dense layout, with the
-//     optional four-step post-twiddle;
-//   * one thread stores the tile with a TMA store and moves on.
+// can hold fill most of its shared memory: a kernel that loads, transforms and
+// stores one tile after the other has nothing to overlap.  Here a persistent
+// CTA walks a sequence of column groups (GC adjacent transforms) through a
+// ring of three tile buffers:
+//   * a producer warp keeps the next two groups' loads in flight (TMA tensor
+//     copies completing on an mbarrier per buffer), stores each finished
+//     group with a TMA store, and refills the buffer once the store has read
+//     it out;
+//   * the compute warps transform a group in place in its buffer: stage 0
+//     reads the tile in the layout the copy left, every stage holds its
+//     values in registers across a barrier and writes them back, the middle
+//     stages in a swizzled layout (element i of transform c at
+//     c * L + (i ^ ((i >> 4) & 15)): the radix-16 Stockham strides then fall
+//     on distinct banks with no padding, so a tile needs no second buffer),
+//     and the last stage writes the output layout, with the optional
+//     four-step post-twiddle.
 // A tile layout is "columns" ([i][c]: the transforms adjacent in memory, a
 // copy moves 256-row boxes of GC columns) or "rows" ([c][i]: each transform's
 // elements contiguous, one copy moves GC whole rows).  A stage that touches a
@@ -38,17 +40,18 @@ using rows::SmemIO;
 template <typename T, int L, int... Rs>
 struct Shape {
   static constexpr int TPT = rows::rows_tpt<T, L, Rs...>();
-  static constexpr int NT = tile::TileBounds<T>::kMaxThreads;  // threads per CTA
+  static constexpr int NT = tile::TileBounds<T>::kMaxThreads;  // compute threads per CTA
   static constexpr int GC = NT / TPT;                          // transforms per group
-  static constexpr int slot = slot_len<L>();
   static constexpr int RB = L < 256 ? L : 256;  // rows per column-layout box
+  static constexpr int NBUF = 3;                // tile buffers in the ring
   static constexpr size_t raw_elems = (size_t)GC * L;
   static constexpr size_t raw_bytes = raw_elems * sizeof(cpx<T>);
-  static constexpr size_t head = 1024;  // two mbarriers, padded so the raw tiles start 1 KB-aligned
-  static constexpr size_t smem = head + 2 * raw_bytes + (size_t)GC * slot * sizeof(cpx<T>);
+  static constexpr size_t head = 1024;  // mbarriers, padded so the tiles start 1 KB-aligned
+  static constexpr size_t smem = head + NBUF * raw_bytes;
   static_assert(NT % TPT == 0 && GC >= 1, "threads per CTA must be a multiple of the threads per transform");
   static_assert((2 * GC * sizeof(T)) % 16 == 0, "a column box row must be a multiple of 16 bytes");
   static_assert(L % 128 == 0, "row tiles move 128-element chunks");
+  static_assert(smem <= 232448, "the tile ring must fit one CTA's shared memory");
 };
 
 // Kernel arguments: the pass, its two tensor maps (device build) and views.
@@ -96,6 +99,24 @@ struct RawRows {
   }
 };
 
+// A transform's working layout: element i at i ^ ((i >> 4) & 15) (a
+// permutation inside each 16-element block).
+FFB_HD constexpr int swz(int i) { return i ^ ((i >> 4) & 15); }
+template <typename T>
+struct SwzIO {
+  cpx<T> *b;  // this transform's L elements
+  template <int S, int R>
+  FFB_HD void get(int j, cpx<T> (&x)[R]) const {
+#pragma unroll
+    for (int r = 0; r < R; ++r) x[r] = b[swz(j + r * S)];
+  }
+  template <int S, int R>
+  FFB_HD void put(int base, const cpx<T> (&x)[R]) const {
+#pragma unroll
+    for (int q = 0; q < R; ++q) b[swz(base + q * S)] = x[q];
+  }
+};
+
 // Last-stage writer: the optional four-step post-twiddle W_N^{g k} of a live
 // transform g, then the raw tile.
 template <typename T, class W>
@@ -117,13 +138,14 @@ struct TwiddledOut {
   }
 };
 
-// Stages S..SE-1 of sequence Q on group g0's tile: stage 0 reads the raw tile
-// and writes the working buffers, the middle stages run in place on the
-// working buffers (reads, barrier, writes), the last stage writes the raw
-// tile.  A barrier separates consecutive stages; none follows stage SE-1.
-template <typename T, bool INV, int L, class Sh, class Q, int S, int SE, bool IN_ROWS, bool OUT_ROWS, class X>
-FFB_HD void run_stages(const X &x, const TileArgs<T> &a, cpx<T> *raw, cpx<T> *work, long long g0) {
-  static_assert(Q::n >= 2, "the raw tile is read by the first stage and written by the last");
+// Stages S.. of sequence Q on group g0's tile, in place: stage 0 reads the
+// tile in the input's layout, the last writes it in the output's layout, the
+// ones between use the swizzled working layout.  Every stage reads, crosses a
+// barrier (its values wait in registers) and writes; a barrier separates
+// consecutive stages and none follows the last.
+template <typename T, bool INV, int L, class Sh, class Q, int S, bool IN_ROWS, bool OUT_ROWS, class X>
+FFB_HD void run_stages(const X &x, const TileArgs<T> &a, cpx<T> *raw, long long g0) {
+  static_assert(Q::n >= 2, "the tile is read by the first stage and written by the last");
   constexpr int R = Q::r(S), Ns = Q::span(S), TwOff = Q::twoff(S);
   constexpr int GC = Sh::GC, TPT = Sh::TPT, NT = Sh::NT;
   constexpr bool first = S == 0, last = S == Q::n - 1;
@@ -137,7 +159,7 @@ FFB_HD void run_stages(const X &x, const TileArgs<T> &a, cpx<T> *raw, cpx<T> *wo
       else
         return rows::stage_read<T, INV, L, TPT, Ns, R>(t, a.tw + TwOff, RawCols<T, GC>{raw, c});
     } else {
-      return rows::stage_read<T, INV, L, TPT, Ns, R>(t, a.tw + TwOff, SmemIO<T>{work + c * Sh::slot});
+      return rows::stage_read<T, INV, L, TPT, Ns, R>(t, a.tw + TwOff, SwzIO<T>{raw + c * L});
     }
   };
   auto wr = [&](int tid, const Regs &st) FFB_INL {
@@ -150,18 +172,13 @@ FFB_HD void run_stages(const X &x, const TileArgs<T> &a, cpx<T> *raw, cpx<T> *wo
       else
         rows::stage_write<T, L, TPT, Ns, R>(t, st, TwiddledOut<T, RawCols<T, GC>>{&a, RawCols<T, GC>{raw, c}, g, tw});
     } else {
-      rows::stage_write<T, L, TPT, Ns, R>(t, st, SmemIO<T>{work + c * Sh::slot});
+      rows::stage_write<T, L, TPT, Ns, R>(t, st, SwzIO<T>{raw + c * L});
     }
   };
-  if constexpr (first || last) {
-    // reads and writes touch different buffers
-    x.each(NT, [&](int tid) FFB_INL { wr(tid, rd(tid)); });
-  } else {
-    x.each2(NT, rd, wr);
-  }
-  if constexpr (S + 1 < SE) {
+  x.each2(NT, rd, wr);
+  if constexpr (!last) {
     x.sync();
-    run_stages<T, INV, L, Sh, Q, S + 1, SE, IN_ROWS, OUT_ROWS>(x, a, raw, work, g0);
+    run_stages<T, INV, L, Sh, Q, S + 1, IN_ROWS, OUT_ROWS>(x, a, raw, g0);
   }
 }
 
@@ -204,60 +221,129 @@ __device__ __forceinline__ void issue_store(const Args<T> &p, const CUtensorMap 
 // Device counter of waits that gave up (copies that never landed).
 static __device__ int g_tcols_wait_failures;
 
+// The compute threads (warps 0 .. NT/32 - 1) synchronise among themselves on
+// named barrier 1, so the producer warp never holds them up.
+struct ComputeThreads {
+  int nt;
+  template <class F>
+  FFB_HD void each(int, F &&f) const {
+#ifdef __CUDA_ARCH__
+    f((int)threadIdx.x);
+#else
+    (void)f;
+#endif
+  }
+  FFB_HD void sync() const {
+#ifdef __CUDA_ARCH__
+    asm volatile("bar.sync 1, %0;" ::"r"(nt) : "memory");
+#endif
+  }
+  template <class FR, class FW>
+  FFB_HD void each2(int, FR &&rd, FW &&wr) const {
+#ifdef __CUDA_ARCH__
+    const auto st = rd((int)threadIdx.x);
+    sync();
+    wr((int)threadIdx.x, st);
+#else
+    (void)rd;
+    (void)wr;
+#endif
+  }
+  // barrier 1 with an OR over the compute threads' predicates
+  __device__ __forceinline__ bool sync_or(bool v) const {
+    uint32_t r;
+    asm volatile(
+        "{\n"
+        "  .reg .pred p, q;\n"
+        "  setp.ne.u32 p, %1, 0;\n"
+        "  barrier.cta.red.or.pred q, 1, %2, p;\n"
+        "  selp.u32 %0, 1, 0, q;\n"
+        "}\n"
+        : "=r"(r)
+        : "r"((uint32_t)v), "r"(nt)
+        : "memory");
+    return r != 0;
+  }
+};
+
+// One CTA per SM, NT compute threads plus one producer warp.
+//   producer (lane 0 of the last warp): loads the first NBUF groups into the
+//     ring (full[s] counts each load's bytes); for every group, once the
+//     compute warps report it written (ready[s]) it stores the tile, waits
+//     for the store to read the buffer out, and loads the group NBUF ahead
+//     into it;
+//   compute warps: wait full[s], run the stages in place, report ready[s].
+// Every wait is bounded; a wait that gives up is counted in
+// g_tcols_wait_failures and ends the loop on both sides (the compute
+// threads decide together, so none is left at a barrier).
 template <typename T, bool INV, int L, bool IN_ROWS, bool OUT_ROWS, int... Rs>
-__global__ void __launch_bounds__(Shape<T, L, Rs...>::NT, 1) k_tcols(const __grid_constant__ Args<T> p) {
+__global__ void __launch_bounds__(Shape<T, L, Rs...>::NT + 32, 1) k_tcols(const __grid_constant__ Args<T> p) {
+  pdl_entry();
   using Sh = Shape<T, L, Rs...>;
   using Q = Seq<Rs...>;
+  constexpr int NW = Sh::NT / 32, NB = Sh::NBUF;
   extern __shared__ __align__(1024) unsigned char smraw[];
-  uint64_t *bar = reinterpret_cast<uint64_t *>(smraw);
-  cpx<T> *raw0 = reinterpret_cast<cpx<T> *>(smraw + Sh::head);
-  cpx<T> *raw1 = raw0 + Sh::raw_elems;
-  cpx<T> *work = raw1 + Sh::raw_elems;
+  uint64_t *full = reinterpret_cast<uint64_t *>(smraw);  // [NB]
+  uint64_t *ready = full + NB;                           // [NB]
+  cpx<T> *ring = reinterpret_cast<cpx<T> *>(smraw + Sh::head);
   const int tid = (int)threadIdx.x;
   if (tid == 0) {
-    tma::mbar_init(&bar[0], 1);
-    tma::mbar_init(&bar[1], 1);
+    for (int k = 0; k < NB; ++k) {
+      tma::mbar_init(&full[k], 1);
+      tma::mbar_init(&ready[k], NW);
+    }
     tma::fence_mbar_init();
   }
   __syncthreads();
-  long long q = blockIdx.x;
-  if (tid == 0 && q < p.total_groups) issue_load<T, L, Sh::GC, Sh::RB>(p, &p.in_map, q, raw0, &bar[0]);
-  const rows::DevT x{};
-  int failed_slot = -1;
-  uint32_t failed_parity = 0;
-  for (int i = 0; q < p.total_groups; ++i, q += gridDim.x) {
-    const int s = i & 1;
-    cpx<T> *raw = s ? raw1 : raw0;
-    const uint32_t parity = (uint32_t)((i >> 1) & 1);
-    const bool ok = tma::mbar_wait(&bar[s], parity);
-    if (__syncthreads_or(!ok)) {
-      failed_slot = s;
-      failed_parity = parity;
+  const long long q0 = blockIdx.x, step = gridDim.x;
+  if (tid >= Sh::NT) {
+    // ---- producer warp
+    if (tid != Sh::NT) return;
+    bool failed = false;
+    for (int k = 0; k < NB; ++k)
+      if (q0 + k * step < p.total_groups)
+        issue_load<T, L, Sh::GC, Sh::RB>(p, &p.in_map, q0 + k * step, ring + k * Sh::raw_elems, &full[k]);
+    int i = 0;
+    for (long long q = q0; q < p.total_groups; q += step, ++i) {
+      const int s = i % NB;
+      cpx<T> *buf = ring + s * Sh::raw_elems;
+      if (!tma::mbar_wait(&ready[s], (uint32_t)((i / NB) & 1))) {
+        failed = true;
+        break;
+      }
+      issue_store<T, L, Sh::GC, Sh::RB>(p, &p.out_map, q, buf);
+      const long long qn = q + NB * step;
+      if (qn < p.total_groups) {
+        tma::wait_read<0>();  // the store has read the buffer out
+        issue_load<T, L, Sh::GC, Sh::RB>(p, &p.in_map, qn, buf, &full[s]);
+      }
+    }
+    tma::wait_all<0>();
+    if (failed) {
+      atomicAdd(&g_tcols_wait_failures, 1);
+      // loads still in flight land before the CTA ends (bounded)
+      for (int k = 0; k < NB; ++k) {
+        const int j = i + k;
+        if (q0 + (long long)j * step < p.total_groups) tma::mbar_wait(&full[j % NB], (uint32_t)((j / NB) & 1));
+      }
+    }
+    return;
+  }
+  // ---- compute warps
+  const ComputeThreads x{Sh::NT};
+  int i = 0;
+  for (long long q = q0; q < p.total_groups; q += step, ++i) {
+    const int s = i % NB;
+    const bool ok = tma::mbar_wait(&full[s], (uint32_t)((i / NB) & 1));
+    if (x.sync_or(!ok)) {  // all compute threads agree
+      if (tid == 0) atomicAdd(&g_tcols_wait_failures, 1);
       break;
     }
     const Group gr = group_of<Sh::GC>(q, p.groups_per_batch);
-    // stage 0 (raw tile -> working buffers); then, while the other stages
-    // run, the next group's load into the other raw buffer
-    run_stages<T, INV, L, Sh, Q, 0, 1, IN_ROWS, OUT_ROWS>(x, p.a, raw, work, gr.g0);
-    __syncthreads();
-    if (tid == 0) {
-      const long long qn = q + gridDim.x;
-      if (qn < p.total_groups) {
-        tma::wait_read<0>();  // the store that last read that buffer has drained
-        issue_load<T, L, Sh::GC, Sh::RB>(p, &p.in_map, qn, s ? raw0 : raw1, &bar[s ^ 1]);
-      }
-    }
-    run_stages<T, INV, L, Sh, Q, 1, Q::n, IN_ROWS, OUT_ROWS>(x, p.a, raw, work, gr.g0);
-    tma::fence_async_smem();
-    __syncthreads();
-    if (tid == 0) issue_store<T, L, Sh::GC, Sh::RB>(p, &p.out_map, q, raw);
-  }
-  if (tid == 0) {
-    tma::wait_all<0>();
-    if (failed_slot >= 0) {
-      atomicAdd(&g_tcols_wait_failures, 1);
-      tma::mbar_wait(&bar[failed_slot], failed_parity);  // bounded: the copy that did not land
-    }
+    run_stages<T, INV, L, Sh, Q, 0, IN_ROWS, OUT_ROWS>(x, p.a, ring + s * Sh::raw_elems, gr.g0);
+    tma::fence_async_smem();  // the tile's writes, before the producer's TMA store reads it
+    __syncwarp();
+    if ((tid & 31) == 0) tma::mbar_arrive(&ready[s]);
   }
 }
 

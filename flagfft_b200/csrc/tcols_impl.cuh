@@ -133,7 +133,7 @@ cudaError_t launch_seq(const TileArgs<T> &a, cudaStream_t s) {
   {                                                                                      \
     auto k = k_tcols<T, INV, L, IR, OR, Rs...>;                                          \
     if ((e = set_smem_limit_once<k_tcols<T, INV, L, IR, OR, Rs...>>((int)Sh::smem)) != cudaSuccess) return e; \
-    k<<<(unsigned)ctas, Sh::NT, Sh::smem, s>>>(p);                                        \
+    if ((e = launch_pdl(k, dim3((unsigned)ctas), dim3(Sh::NT + 32), Sh::smem, s, p)) != cudaSuccess) return e; \
   }
   if (p.in_rows)
     FFB_TCOLS_GO(true, false)
@@ -151,17 +151,16 @@ template <typename T, bool INV, int L, bool IR, bool OR, int... Rs>
 void emulate(const Args<T> &p) {
   using Sh = Shape<T, L, Rs...>;
   using Q = Seq<Rs...>;
-  std::vector<cpx<T>> raw(Sh::raw_elems), work((size_t)Sh::GC * Sh::slot);
+  std::vector<cpx<T>> raw(Sh::raw_elems);
   for (long long q = 0; q < p.total_groups; ++q) {
     const Group gr = group_of<Sh::GC>(q, p.groups_per_batch);
     std::fill(raw.begin(), raw.end(), mk((T)NAN, (T)NAN));
-    std::fill(work.begin(), work.end(), mk((T)NAN, (T)NAN));
     if (IR)
       tma::emulate_box(p.in_view, 0, 0, (int)gr.g0, (int)gr.b, raw.data(), true);
     else
       for (int k = 0; k < L / Sh::RB; ++k)
         tma::emulate_box(p.in_view, (int)(2 * gr.g0), k * Sh::RB, (int)gr.b, 0, raw.data() + k * Sh::RB * Sh::GC, true);
-    run_stages<T, INV, L, Sh, Q, 0, Q::n, IR, OR>(rows::HostT{}, p.a, raw.data(), work.data(), gr.g0);
+    run_stages<T, INV, L, Sh, Q, 0, IR, OR>(rows::HostT{}, p.a, raw.data(), gr.g0);
     if (OR)
       tma::emulate_box(p.out_view, 0, 0, (int)gr.g0, (int)gr.b, raw.data(), false);
     else

@@ -521,6 +521,7 @@ struct TileBounds {
 
 template <typename T, int KIND, int IO>
 __global__ void __launch_bounds__(TileBounds<T>::kMaxThreads) k_tile(const __grid_constant__ TileArgs<T> a) {
+  pdl_entry();
   extern __shared__ __align__(16) unsigned char smraw[];
   DevX x{a.tpt, a.wfast};
   tile_body<T, KIND, IO>(a, (long long)blockIdx.x, (long long)blockIdx.y, reinterpret_cast<cpx<T> *>(smraw), x);
@@ -528,6 +529,7 @@ __global__ void __launch_bounds__(TileBounds<T>::kMaxThreads) k_tile(const __gri
 
 template <typename T, int KIND, bool INV>
 __global__ void __launch_bounds__(TileBounds<T>::kMaxThreads) k_tile_pp(const __grid_constant__ TileArgs<T> a) {
+  pdl_entry();
   extern __shared__ __align__(16) unsigned char smraw[];
   DevX x{a.tpt, a.wfast};
   tile_body_pp<T, KIND, INV>(a, (long long)blockIdx.x, (long long)blockIdx.y, reinterpret_cast<cpx<T> *>(smraw), x);
@@ -535,6 +537,7 @@ __global__ void __launch_bounds__(TileBounds<T>::kMaxThreads) k_tile_pp(const __
 
 template <typename T, int KIND, bool INV, int L, int... Rs>
 __global__ void __launch_bounds__(TileBounds<T>::kMaxThreads) k_tile_pp_fixed(const __grid_constant__ TileArgs<T> a) {
+  pdl_entry();
   extern __shared__ __align__(16) unsigned char smraw[];
   DevX x{a.tpt, a.wfast};
   tile_body_pp<T, KIND, INV>(a, (long long)blockIdx.x, (long long)blockIdx.y, reinterpret_cast<cpx<T> *>(smraw), x,
@@ -561,8 +564,7 @@ cudaError_t launch_pp_fixed(const TileArgs<T> &a, size_t smem, cudaStream_t s) {
   }
   dim3 grid((unsigned)((a.G + a.W - 1) / a.W), (unsigned)a.nbatch, 1);
   dim3 block((unsigned)(a.W * a.tpt), 1, 1);
-  k_tile_pp_fixed<T, KIND, INV, L, Rs...><<<grid, block, smem, s>>>(a);
-  return cudaGetLastError();
+  return launch_pdl(k_tile_pp_fixed<T, KIND, INV, L, Rs...>, grid, block, smem, s, a);
 }
 #else
 template <typename T, int KIND, bool INV, int L, int... Rs>
@@ -601,8 +603,7 @@ cudaError_t launch_one(const TileArgs<T> &a, size_t smem, cudaStream_t s) {
   }
   dim3 grid((unsigned)((a.G + a.W - 1) / a.W), (unsigned)a.nbatch, 1);
   dim3 block((unsigned)(a.W * a.tpt), 1, 1);
-  k_tile<T, KIND, IO><<<grid, block, smem, s>>>(a);
-  return cudaGetLastError();
+  return launch_pdl(k_tile<T, KIND, IO>, grid, block, smem, s, a);
 }
 template <typename T, int KIND, bool INV>
 cudaError_t launch_pp(const TileArgs<T> &a, size_t smem, cudaStream_t s) {
@@ -612,8 +613,7 @@ cudaError_t launch_pp(const TileArgs<T> &a, size_t smem, cudaStream_t s) {
   }
   dim3 grid((unsigned)((a.G + a.W - 1) / a.W), (unsigned)a.nbatch, 1);
   dim3 block((unsigned)(a.W * a.tpt), 1, 1);
-  k_tile_pp<T, KIND, INV><<<grid, block, smem, s>>>(a);
-  return cudaGetLastError();
+  return launch_pdl(k_tile_pp<T, KIND, INV>, grid, block, smem, s, a);
 }
 #else
 template <typename T, int KIND, bool INV>

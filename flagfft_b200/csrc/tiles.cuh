@@ -224,6 +224,7 @@ FFB_HD void tile_body(const TileArgs<T> &a, long long bx, long long by, cpx<T> *
 
 template <typename T, bool INV, int L, int... Rs>
 __global__ void __launch_bounds__(Shape<T, L, Rs...>::NT, Shape<T, L, Rs...>::min_blocks) k_tiles(const __grid_constant__ TileArgs<T> a) {
+  pdl_entry();
   extern __shared__ __align__(16) unsigned char smraw[];
   tile_body<T, INV, L, rows::DevT, Rs...>(a, (long long)blockIdx.x, (long long)blockIdx.y,
                                           reinterpret_cast<cpx<T> *>(smraw), rows::DevT{});
@@ -243,8 +244,7 @@ cudaError_t launch(const TileArgs<T> &a, cudaStream_t s) {
   }
   using Sh = Shape<T, L, Rs...>;
   dim3 grid((unsigned)((a.G + Sh::W - 1) / Sh::W), (unsigned)a.nbatch, 1);
-  k_tiles<T, INV, L, Rs...><<<grid, dim3(Sh::NT), smem_of<T, L, Rs...>(), s>>>(a);
-  return cudaGetLastError();
+  return launch_pdl(k_tiles<T, INV, L, Rs...>, grid, dim3(Sh::NT), smem_of<T, L, Rs...>(), s, a);
 }
 #else
 template <typename T, bool INV, int L, int... Rs>

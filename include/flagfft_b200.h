@@ -125,6 +125,20 @@ FLAGFFT_API flagfftResult flagfftB200ServerDestroy(flagfftB200Server srv);
  * counterpart. */
 FLAGFFT_API flagfftResult flagfftB200DeviceWaitFailures(long long *count);
 
+/* Precision-mode prototype: batched complex64 transforms of n = 256 or 4096
+ * points whose radix-16 stages run as dense 16-point DFT-matrix products on
+ * the tcgen05 tensor cores, split-bf16 operands (terms = 3: the three
+ * products of a two-way split; terms = 6: a three-way split, every product
+ * down to 2^-24) with fp32 accumulation in tensor memory.  Measurement entry
+ * point for the decision whether this mode ships; the plan path does not use
+ * it.  No reference counterpart.  idata / odata: batch contiguous rows of n
+ * flagfftComplex on the device; direction FLAGFFT_FORWARD / FLAGFFT_INVERSE.
+ * Returns FLAGFFT_NOT_SUPPORTED for other n or terms. */
+FLAGFFT_API flagfftResult flagfftB200PrecisionC2C(const flagfftComplex *idata, flagfftComplex *odata, int n,
+                                                 int batch, int direction, int terms, flagfftStream_t stream);
+/* Bounded waits of the precision-mode kernel that gave up on this device. */
+FLAGFFT_API flagfftResult flagfftB200PrecisionWaitFailures(long long *count);
+
 /* Batched complex64 FFT of power-of-two length n (8192 <= n <= 2^22) that
  * allocates no memory.  No counterpart in the reference.
  *

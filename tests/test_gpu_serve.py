@@ -105,6 +105,8 @@ def test_server_staged_admission_and_overlap(ffb, torch_cuda):
     # (a) 6 MiB: every request fits (the largest charge, C2C 4096 x 64, is
     # 4 MiB of input + output), the whole mix does not
     with ffb.Server(hbm_budget_bytes=6 << 20, max_ticks=3) as srv:
+        for t, code, n, b, d, x, xd, yd in reqs:
+            srv.prepare(code, n, d)
         tickets = [srv.submit(code, n, b, xd, yd, d) for t, code, n, b, d, x, xd, yd in reqs]
         for tk in tickets:
             srv.wait(tk, timeout_s=60.0)
@@ -118,6 +120,11 @@ def test_server_staged_admission_and_overlap(ffb, torch_cuda):
     for *_, yd in reqs:
         yd.zero_()
     with ffb.Server(hbm_budget_bytes=8 << 30, max_ticks=3) as srv:
+        # templates first: building one inside submit() uploads its tables
+        # synchronously, which would let the long request finish meanwhile
+        srv.prepare(ffb.C2C, big_n, ffb.FORWARD)
+        for t, code, n, b, d, x, xd, yd in reqs:
+            srv.prepare(code, n, d)
         t_big = srv.submit(ffb.C2C, big_n, big_b, bx, by)
         tickets = [srv.submit(code, n, b, xd, yd, d) for t, code, n, b, d, x, xd, yd in reqs]
         for tk in tickets + [t_big]:
