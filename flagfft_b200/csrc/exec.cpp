@@ -334,6 +334,22 @@ int64_t choose_split_conv(int64_t n, int64_t maxL, bool one_pass, int64_t *n1_ou
         best_n1 = n1;
       }
     }
+  if (!best_m) {
+    // a convolution too long for a one-codelet column: columns of a
+    // compile-time power-of-two sequence (strided tile passes, which carry
+    // the chirp on load and store like the codelet columns), rows of at most
+    // maxL points: M = n1 * n2 the smallest power of two >= 2n - 1
+    int64_t m = 1;
+    while (m < lo) m <<= 1;
+    for (int64_t n1 = 32; n1 <= 16384 && !best_m; n1 <<= 1) {
+      const int64_t n2 = m / n1;
+      std::vector<int> r1;
+      if (n2 >= 2 && n2 <= maxL && n2 <= 16384 && fixed_sequence(n1, &r1) && chain_cost(n2, nullptr, memo) < 1e29) {
+        best_m = m;
+        best_n1 = n1;
+      }
+    }
+  }
   if (best_m) {
     *n1_out = best_n1;
     if (!fixed_sequence(best_m / best_n1, row_radices)) chain_cost(best_m / best_n1, row_radices, memo);
@@ -846,6 +862,12 @@ class Builder {
 // every transform that fits one CTA in one pass.
 thread_local int t_policy_override = -1;  // set while lowering batch groups
 
+// A program workspace of at least `bytes` (several lowerings of one program
+// share it: they run one after the other).
+static void ensure_scratch(DevPtr &d, size_t bytes) {
+  if (!d || d->bytes < bytes) d = std::make_shared<DevMem>(bytes);
+}
+
 static int onchip_policy() {
   if (t_policy_override >= 0) return t_policy_override;
   const char *v = std::getenv("FLAGFFT_ONCHIP_POLICY");
@@ -893,7 +915,7 @@ void lower_c2c(Builder<T> &bld, Program &prog, const NodePtr &root, bool inverse
   if (f1) {
     {
       const int64_t n1 = f1, n2 = n / f1;
-      prog.scratch0 = std::make_shared<DevMem>((size_t)(batch * n) * sizeof(cpx<T>));
+      ensure_scratch(prog.scratch0, (size_t)(batch * n) * sizeof(cpx<T>));
       // pass A: columns j2 (stride n2) of length n1, x W_n^{j2 k1}, rows Y[j2][k1]
       auto *pa = bld.add_pass(sa, IoKind::C2C, inverse, batch, n2, idist, 1, n2, n, n1, 1, src, Buf::Scratch0, n1);
       bld.set_post_twiddle(pa->a, n);
@@ -937,9 +959,12 @@ void lower_c2c(Builder<T> &bld, Program &prog, const NodePtr &root, bool inverse
     }
     if (M) {
       const int64_t n2 = M / n1;
-      const CoreSpec sa{CoreKind::Dit, n1, n1, {(int)n1}, nullptr};
+      // the column core: one codelet, or (long convolutions) a compile-time sequence
+      std::vector<int> col_radices{(int)n1};
+      if (n1 > 19) fixed_sequence(n1, &col_radices);
+      const CoreSpec sa{CoreKind::Dit, n1, n1, col_radices, nullptr};
       const CoreSpec sb{CoreKind::Dit, n2, n2, row_radices, nullptr};
-      prog.scratch0 = std::make_shared<DevMem>((size_t)(batch * M) * sizeof(cpx<T>));
+      ensure_scratch(prog.scratch0, (size_t)(batch * M) * sizeof(cpx<T>));
       const cpx<T> *chirp = bld.table_chirp(n, inverse);
       // A: a_j = x_j c_j (j = j1 n2 + j2 < n), FFT over j1, x W_M^{j2 k1} -> Y[k1][j2]
       auto *pa = bld.add_pass(sa, IoKind::C2C, false, batch, n2, idist, 1, n2, M, 1, n2, src, Buf::Scratch0, n);
@@ -1100,29 +1125,61 @@ std::unique_ptr<Program> lower_2d_t(const NodePtr &root, Planner &planner, Trans
   const int64_t h1 = n1 / 2 + 1;
   if (batch > 65535) throw std::runtime_error("2-D batch above 65535");
   if (t == Transform::C2C) {
-    if (!bld.core_for(root->row, rs) || !bld.core_for(root->col, cs))
-      throw std::runtime_error("2-D axis has no on-chip lowering yet");
-    bld.add_pass(rs, IoKind::C2C, inverse, 1, batch * n0, 0, n1, 1, 0, n1, 1, Buf::In, Buf::Out, n1);
-    bld.add_pass(cs, IoKind::C2C, inverse, batch, n1, n0 * n1, 1, n1, n0 * n1, 1, n1, Buf::Out, Buf::Out, n0);
+    if (bld.core_for(root->row, rs) && bld.core_for(root->col, cs)) {
+      bld.add_pass(rs, IoKind::C2C, inverse, 1, batch * n0, 0, n1, 1, 0, n1, 1, Buf::In, Buf::Out, n1);
+      bld.add_pass(cs, IoKind::C2C, inverse, batch, n1, n0 * n1, 1, n1, n0 * n1, 1, n1, Buf::Out, Buf::Out, n0);
+      return prog;
+    }
+    // An axis too long for one CTA (src/exec/raw_nodes.cpp:549-610 runs any
+    // child per axis): the rows with whatever lowering their tree takes,
+    // the matrix transposed, the other axis as rows, transposed back.
+    lower_c2c<T>(bld, *prog, root->row, inverse, n1, batch * n0, n1, n1, Buf::In, Buf::Out);
+    ensure_scratch(prog->scratch1, (size_t)(batch * n0 * n1) * sizeof(cpx<T>));
+    prog->passes.push_back(std::make_unique<TransposePass<T>>(Buf::Out, Buf::Scratch1, batch, n0, n1));
+    lower_c2c<T>(bld, *prog, root->col, inverse, n0, batch * n1, n0, n0, Buf::Scratch1, Buf::Scratch1);
+    prog->passes.push_back(std::make_unique<TransposePass<T>>(Buf::Scratch1, Buf::Out, batch, n1, n0));
     return prog;
   }
-  if (!bld.core_for(root->col, cs)) throw std::runtime_error("2-D column axis has no on-chip lowering yet");
   const bool even = (n1 % 2) == 0;
   NodePtr row_core = even ? build_raw_root(planner, n1 / 2, nullptr, nullptr) : root->row;
-  if (!bld.core_for(row_core, rs)) throw std::runtime_error("2-D row axis has no on-chip lowering yet");
-  prog->scratch0 = std::make_shared<DevMem>((size_t)(batch * n0 * h1) * sizeof(cpx<T>));
+  if (!bld.core_for(row_core, rs)) throw std::runtime_error("2-D real row axis too long for one CTA");
+  const bool col_onchip = bld.core_for(root->col, cs);
   if (t == Transform::R2C) {
-    // rows into the workspace, then column tiles into the output (safe in place)
+    if (col_onchip) {
+      // rows into the workspace, then column tiles into the output (safe in place)
+      ensure_scratch(prog->scratch0, (size_t)(batch * n0 * h1) * sizeof(cpx<T>));
+      auto *p = bld.add_pass(rs, even ? IoKind::R2C : IoKind::R2CFull, false, 1, batch * n0, 0, n1, even ? 2 : 1, 0,
+                             h1, 1, Buf::In, Buf::Scratch0, n1);
+      if (even) p->a.rtw = bld.table_rtw(n1);
+      bld.add_pass(cs, IoKind::C2C, false, batch, h1, n0 * h1, 1, h1, n0 * h1, 1, h1, Buf::Scratch0, Buf::Out, n0);
+      return prog;
+    }
+    // a column axis too long for one CTA: rows into the output, transpose,
+    // the columns as rows (any lowering), transpose back
     auto *p = bld.add_pass(rs, even ? IoKind::R2C : IoKind::R2CFull, false, 1, batch * n0, 0, n1, even ? 2 : 1, 0,
-                           h1, 1, Buf::In, Buf::Scratch0, n1);
+                           h1, 1, Buf::In, Buf::Out, n1);
     if (even) p->a.rtw = bld.table_rtw(n1);
-    bld.add_pass(cs, IoKind::C2C, false, batch, h1, n0 * h1, 1, h1, n0 * h1, 1, h1, Buf::Scratch0, Buf::Out, n0);
-  } else {
-    bld.add_pass(cs, IoKind::C2C, true, batch, h1, n0 * h1, 1, h1, n0 * h1, 1, h1, Buf::In, Buf::Scratch0, n0);
-    auto *p = bld.add_pass(rs, even ? IoKind::C2R : IoKind::C2RFull, true, 1, batch * n0, 0, h1, 1, 0, n1,
-                           even ? 2 : 1, Buf::Scratch0, Buf::Out, n1);
-    if (even) p->a.rtw = bld.table_rtw(n1);
+    ensure_scratch(prog->scratch1, (size_t)(batch * n0 * h1) * sizeof(cpx<T>));
+    prog->passes.push_back(std::make_unique<TransposePass<T>>(Buf::Out, Buf::Scratch1, batch, n0, h1));
+    lower_c2c<T>(bld, *prog, root->col, false, n0, batch * h1, n0, n0, Buf::Scratch1, Buf::Scratch1);
+    prog->passes.push_back(std::make_unique<TransposePass<T>>(Buf::Scratch1, Buf::Out, batch, h1, n0));
+    return prog;
   }
+  if (col_onchip) {
+    ensure_scratch(prog->scratch0, (size_t)(batch * n0 * h1) * sizeof(cpx<T>));
+    bld.add_pass(cs, IoKind::C2C, true, batch, h1, n0 * h1, 1, h1, n0 * h1, 1, h1, Buf::In, Buf::Scratch0, n0);
+  } else {
+    // columns first (transposed to rows, any lowering, transposed back into
+    // the workspace the row pass reads)
+    ensure_scratch(prog->scratch1, (size_t)(batch * n0 * h1) * sizeof(cpx<T>));
+    prog->passes.push_back(std::make_unique<TransposePass<T>>(Buf::In, Buf::Scratch1, batch, n0, h1));
+    lower_c2c<T>(bld, *prog, root->col, true, n0, batch * h1, n0, n0, Buf::Scratch1, Buf::Scratch1);
+    ensure_scratch(prog->scratch0, (size_t)(batch * n0 * h1) * sizeof(cpx<T>));
+    prog->passes.push_back(std::make_unique<TransposePass<T>>(Buf::Scratch1, Buf::Scratch0, batch, h1, n0));
+  }
+  auto *p = bld.add_pass(rs, even ? IoKind::C2R : IoKind::C2RFull, true, 1, batch * n0, 0, h1, 1, 0, n1, even ? 2 : 1,
+                         Buf::Scratch0, Buf::Out, n1);
+  if (even) p->a.rtw = bld.table_rtw(n1);
   return prog;
 }
 

@@ -111,6 +111,24 @@ struct RealPass final : PassBase {
   }
 };
 
+// Axis exchange between passes: (batch, R, C) -> (batch, C, R).
+template <typename T>
+struct TransposePass final : PassBase {
+  Buf src, dst;
+  long long batch, R, C;
+  TransposePass(Buf s, Buf d, long long b, long long r, long long c) : src(s), dst(d), batch(b), R(r), C(c) {}
+  cudaError_t run(const void *in, void *out, void *s0, void *s1, cudaStream_t st) const override {
+    return launch_transpose<T>(reinterpret_cast<const cpx<T> *>(TilePass<T>::pick(src, in, out, s0, s1)),
+                               reinterpret_cast<cpx<T> *>(TilePass<T>::pick(dst, in, out, s0, s1)), batch, R, C, st);
+  }
+  std::string describe() const override {
+    std::ostringstream o;
+    o << "transpose " << (sizeof(T) == 4 ? "f32" : "f64") << " " << R << "x" << C << " transforms=" << batch << " "
+      << buf_name(src) << "->" << buf_name(dst);
+    return o.str();
+  }
+};
+
 // Elementwise widen / take / expand around a full complex transform of a
 // real signal (launch_real_convert).
 template <typename T>

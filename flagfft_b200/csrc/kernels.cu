@@ -47,18 +47,25 @@ FFB_HD void real_post_pair(const cpx<T> *z, cpx<T> *x, int L, int k, const RealT
   if (m != k) x[m] = xm;
 }
 
+// One thread per pair (k, L-k), k = 0..L/2: reads X_k and X_{L-k} once and
+// writes Z_k and Z_{L-k} (Z_0 from X_0 and X_L; Im X_0 and Im X_L ignored).
 template <typename T>
-FFB_HD void real_pre_one(const cpx<T> *x, cpx<T> *z, int L, int k, const RealTw<T> &rtw) {
-  cpx<T> xk = x[k], xm = x[L - k];
+FFB_HD void real_pre_pair(const cpx<T> *x, cpx<T> *z, int L, int k, const RealTw<T> &rtw) {
+  auto pre = [&](cpx<T> a, cpx<T> b, int kk) {  // a = X_kk, b = X_{L-kk}
+    const cpx<T> s = mk(a.x + b.x, a.y - b.y);
+    const cpx<T> d = mk(a.x - b.x, a.y + b.y);
+    const cpx<T> w = real_tw(rtw, (uint32_t)kk);
+    const cpx<T> dw = mk(d.x * w.x + d.y * w.y, d.y * w.x - d.x * w.y);
+    return mk(s.x - dw.y, s.y + dw.x);
+  };
+  const int m = L - k;
+  cpx<T> xk = x[k], xm = x[m];
   if (k == 0) {
     xk.y = (T)0;
     xm.y = (T)0;
   }
-  cpx<T> s = mk(xk.x + xm.x, xk.y - xm.y);
-  cpx<T> d = mk(xk.x - xm.x, xk.y + xm.y);
-  cpx<T> w = real_tw(rtw, (uint32_t)k);
-  cpx<T> dw = mk(d.x * w.x + d.y * w.y, d.y * w.x - d.x * w.y);
-  z[k] = mk(s.x - dw.y, s.y + dw.x);
+  z[k] = pre(xk, xm, k);
+  if (m != k && m < L) z[m] = pre(xm, xk, m);
 }
 
 template <typename T>
@@ -74,11 +81,54 @@ template <typename T>
 __global__ void k_real_pre(const cpx<T> *x, cpx<T> *z, long long xdist, long long zdist, int L, const RealTw<T> rtw) {
   pdl_entry();
   const long long b = blockIdx.y;
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < L; k += gridDim.x * blockDim.x)
-    real_pre_one<T>(x + b * xdist, z + b * zdist, L, k, rtw);
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k <= L / 2; k += gridDim.x * blockDim.x)
+    real_pre_pair<T>(x + b * xdist, z + b * zdist, L, k, rtw);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_transpose(const cpx<T> *in, cpx<T> *out, long long R, long long C) {
+  pdl_entry();
+  __shared__ cpx<T> tile[32][33];
+  const long long b = blockIdx.z;
+  const long long r0 = (long long)blockIdx.y * 32, c0 = (long long)blockIdx.x * 32;
+  in += b * R * C;
+  out += b * R * C;
+#pragma unroll
+  for (int i = threadIdx.y; i < 32; i += 8) {
+    const long long r = r0 + i, c = c0 + threadIdx.x;
+    if (r < R && c < C) tile[i][threadIdx.x] = in[r * C + c];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int i = threadIdx.y; i < 32; i += 8) {
+    const long long c = c0 + i, r = r0 + threadIdx.x;
+    if (r < R && c < C) out[c * R + r] = tile[threadIdx.x][i];
+  }
 }
 
 }  // namespace
+
+template <typename T>
+cudaError_t launch_transpose(const cpx<T> *in, cpx<T> *out, long long batch, long long R, long long C,
+                             cudaStream_t s) {
+  if (batch <= 0 || R <= 0 || C <= 0) return cudaSuccess;
+  if ((R + 31) / 32 > 65535 || batch > 65535) return cudaErrorInvalidValue;
+#ifndef FFB_HOST_EMULATION
+  return launch_pdl(k_transpose<T>, dim3((unsigned)((C + 31) / 32), (unsigned)((R + 31) / 32), (unsigned)batch),
+                    dim3(32, 8), 0, s, in, out, R, C);
+#else
+  (void)s;
+  for (long long b = 0; b < batch; ++b)
+    for (long long r = 0; r < R; ++r)
+      for (long long c = 0; c < C; ++c) out[b * R * C + c * R + r] = in[b * R * C + r * C + c];
+  return cudaSuccess;
+#endif
+}
+
+template cudaError_t launch_transpose<float>(const cpx<float> *, cpx<float> *, long long, long long, long long,
+                                             cudaStream_t);
+template cudaError_t launch_transpose<double>(const cpx<double> *, cpx<double> *, long long, long long, long long,
+                                              cudaStream_t);
 
 template <typename T>
 cudaError_t launch_real_post(const cpx<T> *z, cpx<T> *x, long long batch, long long zdist, long long xdist, int L,
@@ -99,11 +149,11 @@ cudaError_t launch_real_pre(const cpx<T> *x, cpx<T> *z, long long batch, long lo
                             const RealTw<T> &rtw, cudaStream_t s) {
 #ifndef FFB_HOST_EMULATION
   const int threads = 256;
-  const int blocks = (int)std::min<long long>((L + threads - 1) / threads, 2048);
+  const int blocks = (int)std::min<long long>((L / 2 + threads) / threads, 1024);
   return launch_pdl(k_real_pre<T>, dim3(blocks, (unsigned)batch), dim3(threads), 0, s, x, z, xdist, zdist, L, rtw);
 #else
   for (long long b = 0; b < batch; ++b)
-    for (int k = 0; k < L; ++k) real_pre_one<T>(x + b * xdist, z + b * zdist, L, k, rtw);
+    for (int k = 0; k <= L / 2; ++k) real_pre_pair<T>(x + b * xdist, z + b * zdist, L, k, rtw);
   return cudaSuccess;
 #endif
 }

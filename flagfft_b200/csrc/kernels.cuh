@@ -33,8 +33,8 @@ enum class IoKind : int {
 // and writes element k at                          out + b*ob + g*og + k*ok
 // (units: elements of the pass's input / output type).
 // The compile-time radix sequences with their own kernels: radix-16 chains
-// of the power-of-two lengths 128..16384 (one smaller radix last), and the
-// mixed-radix 1701 = 9 * 9 * 7 * 3.  The executor runs a length that has one
+// of the power-of-two lengths 128..16384 (one smaller radix last), 1536 =
+// 16 * 16 * 6, and the mixed-radix 1701 = 9 * 9 * 7 * 3.  The executor runs a length that has one
 // on it (and prefers such lengths for convolutions).
 #define FFB_FIXED_SEQUENCES(X)        \
   X(1701, 9, 9, 7, 3)                 \
@@ -42,6 +42,7 @@ enum class IoKind : int {
   X(256, 16, 16)                      \
   X(512, 16, 16, 2)                   \
   X(1024, 16, 16, 4)                  \
+  X(1536, 16, 16, 6)                  \
   X(2048, 16, 16, 8)                  \
   X(4096, 16, 16, 16)                 \
   X(8192, 16, 16, 16, 2)              \
@@ -148,6 +149,14 @@ inline size_t pp_tile_smem(const TileArgs<T> &a) {
 template <typename T>
 cudaError_t launch_real_convert(int mode, const void *src, void *dst, long long batch, long long sdist,
                                 long long ddist, long long n, cudaStream_t stream);
+
+// Batched out-of-place transpose of complex matrices: in (batch, R, C)
+// row-major -> out (batch, C, R), through 32 x 32 shared-memory tiles (both
+// sides coalesced).  Used by the lowerings that exchange axes between
+// passes (2-D transforms with an axis too long for one CTA).
+template <typename T>
+cudaError_t launch_transpose(const cpx<T> *in, cpx<T> *out, long long batch, long long R, long long C,
+                             cudaStream_t stream);
 
 // Real-transform twiddles W_n^k, k <= n/2, as two short tables:
 // W_n^k = hi[k / split] * lo[k % split] (lo: split entries, hi: n/2/split + 1),

@@ -16,8 +16,9 @@
 //     reads the tile in the layout the copy left, every stage holds its
 //     values in registers across a barrier and writes them back, the middle
 //     stages in a swizzled layout (element i of transform c at
-//     c * L + (i ^ ((i >> 4) & 15)): the radix-16 Stockham strides then fall
-//     on distinct banks with no padding, so a tile needs no second buffer),
+//     c * (L + PAD) + (i ^ ((i >> 4) & 15)): the radix-16 Stockham strides
+//     then fall on distinct banks, and PAD spreads the transforms one
+//     wavefront touches over the banks, so a tile needs no second buffer),
 //     and the last stage writes the output layout, with the optional
 //     four-step post-twiddle.
 // A tile layout is "columns" ([i][c]: the transforms adjacent in memory, a
@@ -37,18 +38,30 @@ using rows::Seq;
 using rows::slot_len;
 using rows::SmemIO;
 
+// Transforms per group: as many as the precision's thread limit allows,
+// rounded down to an even count in single precision (a column box row must
+// be a multiple of 16 bytes).
+template <typename T>
+constexpr int tcols_gc(int tpt) {
+  const int g = tile::TileBounds<T>::kMaxThreads / tpt;
+  return sizeof(T) == 4 ? g / 2 * 2 : g;
+}
+
 template <typename T, int L, int... Rs>
 struct Shape {
   static constexpr int TPT = rows::rows_tpt<T, L, Rs...>();
-  static constexpr int NT = tile::TileBounds<T>::kMaxThreads;  // compute threads per CTA
-  static constexpr int GC = NT / TPT;                          // transforms per group
+  static constexpr int GC = tcols_gc<T>(TPT);  // transforms per group
+  static constexpr int NT = GC * TPT;          // compute threads per CTA
   static constexpr int RB = L < 256 ? L : 256;  // rows per column-layout box
   static constexpr int NBUF = 3;                // tile buffers in the ring
-  static constexpr size_t raw_elems = (size_t)GC * L;
+  // working layout: transform c at c * (L + PAD), so that the GC transforms
+  // of one shared-memory wavefront (128 bytes) start on distinct banks
+  static constexpr int PAD = (int)(128 / sizeof(cpx<T>)) / GC;
+  static constexpr size_t raw_elems = (size_t)GC * L + (size_t)(GC - 1) * PAD;
   static constexpr size_t raw_bytes = raw_elems * sizeof(cpx<T>);
   static constexpr size_t head = 1024;  // mbarriers, padded so the tiles start 1 KB-aligned
   static constexpr size_t smem = head + NBUF * raw_bytes;
-  static_assert(NT % TPT == 0 && GC >= 1, "threads per CTA must be a multiple of the threads per transform");
+  static_assert(GC >= 1 && NT % 32 == 0, "a group needs one or more transforms and whole warps");
   static_assert((2 * GC * sizeof(T)) % 16 == 0, "a column box row must be a multiple of 16 bytes");
   static_assert(L % 128 == 0, "row tiles move 128-element chunks");
   static_assert(smem <= 232448, "the tile ring must fit one CTA's shared memory");
@@ -159,7 +172,7 @@ FFB_HD void run_stages(const X &x, const TileArgs<T> &a, cpx<T> *raw, long long 
       else
         return rows::stage_read<T, INV, L, TPT, Ns, R>(t, a.tw + TwOff, RawCols<T, GC>{raw, c});
     } else {
-      return rows::stage_read<T, INV, L, TPT, Ns, R>(t, a.tw + TwOff, SwzIO<T>{raw + c * L});
+      return rows::stage_read<T, INV, L, TPT, Ns, R>(t, a.tw + TwOff, SwzIO<T>{raw + c * (L + Sh::PAD)});
     }
   };
   auto wr = [&](int tid, const Regs &st) FFB_INL {
@@ -172,7 +185,7 @@ FFB_HD void run_stages(const X &x, const TileArgs<T> &a, cpx<T> *raw, long long 
       else
         rows::stage_write<T, L, TPT, Ns, R>(t, st, TwiddledOut<T, RawCols<T, GC>>{&a, RawCols<T, GC>{raw, c}, g, tw});
     } else {
-      rows::stage_write<T, L, TPT, Ns, R>(t, st, SwzIO<T>{raw + c * L});
+      rows::stage_write<T, L, TPT, Ns, R>(t, st, SwzIO<T>{raw + c * (L + Sh::PAD)});
     }
   };
   x.each2(NT, rd, wr);

@@ -16,6 +16,7 @@ namespace tcols {
 // Sequences with a TMA column kernel.
 #define FFB_TCOLS_SEQUENCES(X) \
   X(1024, 16, 16, 4)           \
+  X(1536, 16, 16, 6)           \
   X(2048, 16, 16, 8)           \
   X(4096, 16, 16, 16)
 

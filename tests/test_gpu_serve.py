@@ -152,8 +152,9 @@ def test_server_wait_timeout_keeps_ticket(ffb, torch_cuda):
     n, b = 4096, 4
     x = torch.randn(b, n, dtype=torch.complex64, device="cuda")
     y = torch.empty_like(x)
-    with ffb.Server(hbm_budget_bytes=1 << 30, max_ticks=1) as srv:
-        # occupy the only slot with a large request, then wait on the next
+    with ffb.Server(hbm_budget_bytes=4 << 30, max_ticks=1) as srv:
+        # occupy the only slot with a large request (1.5 GB with its
+        # workspace), then wait on the next
         # with a zero timeout: it cannot have finished yet
         big_n, big_b = 1 << 20, 64
         bx = torch.randn(big_b, big_n, dtype=torch.complex64, device="cuda")
