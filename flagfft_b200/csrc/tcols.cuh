@@ -57,10 +57,15 @@ struct Shape {
   // working layout: transform c at c * (L + PAD), so that the GC transforms
   // of one shared-memory wavefront (128 bytes) start on distinct banks
   static constexpr int PAD = (int)(128 / sizeof(cpx<T>)) / GC;
-  static constexpr size_t raw_elems = (size_t)GC * L + (size_t)(GC - 1) * PAD;
-  static constexpr size_t raw_bytes = raw_elems * sizeof(cpx<T>);
+  static constexpr size_t raw_elems = (size_t)GC * L + (size_t)(GC - 1) * PAD;  // one tile, working layout included
+  // ring slots start 1 KB apart: a TMA copy's shared-memory address must be
+  // 128-byte aligned, and the working layout's padding makes a tile a little
+  // longer than GC * L elements
+  static constexpr size_t buf_bytes = (raw_elems * sizeof(cpx<T>) + 1023) / 1024 * 1024;
+  static constexpr size_t buf_elems = buf_bytes / sizeof(cpx<T>);
   static constexpr size_t head = 1024;  // mbarriers, padded so the tiles start 1 KB-aligned
-  static constexpr size_t smem = head + NBUF * raw_bytes;
+  static constexpr size_t smem = head + NBUF * buf_bytes;
+  static_assert(buf_bytes % 1024 == 0 && head % 1024 == 0, "ring slots must stay 1 KB-aligned");
   static_assert(GC >= 1 && NT % 32 == 0, "a group needs one or more transforms and whole warps");
   static_assert((2 * GC * sizeof(T)) % 16 == 0, "a column box row must be a multiple of 16 bytes");
   static_assert(L % 128 == 0, "row tiles move 128-element chunks");
@@ -315,11 +320,11 @@ __global__ void __launch_bounds__(Shape<T, L, Rs...>::NT + 32, 1) k_tcols(const 
     bool failed = false;
     for (int k = 0; k < NB; ++k)
       if (q0 + k * step < p.total_groups)
-        issue_load<T, L, Sh::GC, Sh::RB>(p, &p.in_map, q0 + k * step, ring + k * Sh::raw_elems, &full[k]);
+        issue_load<T, L, Sh::GC, Sh::RB>(p, &p.in_map, q0 + k * step, ring + k * Sh::buf_elems, &full[k]);
     int i = 0;
     for (long long q = q0; q < p.total_groups; q += step, ++i) {
       const int s = i % NB;
-      cpx<T> *buf = ring + s * Sh::raw_elems;
+      cpx<T> *buf = ring + s * Sh::buf_elems;
       if (!tma::mbar_wait(&ready[s], (uint32_t)((i / NB) & 1))) {
         failed = true;
         break;
@@ -353,7 +358,7 @@ __global__ void __launch_bounds__(Shape<T, L, Rs...>::NT + 32, 1) k_tcols(const 
       break;
     }
     const Group gr = group_of<Sh::GC>(q, p.groups_per_batch);
-    run_stages<T, INV, L, Sh, Q, 0, IN_ROWS, OUT_ROWS>(x, p.a, ring + s * Sh::raw_elems, gr.g0);
+    run_stages<T, INV, L, Sh, Q, 0, IN_ROWS, OUT_ROWS>(x, p.a, ring + s * Sh::buf_elems, gr.g0);
     tma::fence_async_smem();  // the tile's writes, before the producer's TMA store reads it
     __syncwarp();
     if ((tid & 31) == 0) tma::mbar_arrive(&ready[s]);

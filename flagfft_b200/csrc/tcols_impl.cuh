@@ -152,21 +152,26 @@ template <typename T, bool INV, int L, bool IR, bool OR, int... Rs>
 void emulate(const Args<T> &p) {
   using Sh = Shape<T, L, Rs...>;
   using Q = Seq<Rs...>;
-  std::vector<cpx<T>> raw(Sh::raw_elems);
+  // the shared-memory image of the kernel: a 1 KB head, then NBUF ring
+  // slots, the group q in slot q % NBUF
+  std::vector<unsigned char> image(Sh::smem + 1024);
+  unsigned char *base = image.data() + (1024 - (reinterpret_cast<uintptr_t>(image.data()) & 1023));
+  cpx<T> *const ring = reinterpret_cast<cpx<T> *>(base + Sh::head);
   for (long long q = 0; q < p.total_groups; ++q) {
     const Group gr = group_of<Sh::GC>(q, p.groups_per_batch);
-    std::fill(raw.begin(), raw.end(), mk((T)NAN, (T)NAN));
+    cpx<T> *const raw = ring + (size_t)(q % Sh::NBUF) * Sh::buf_elems;
+    std::fill(raw, raw + Sh::raw_elems, mk((T)NAN, (T)NAN));
     if (IR)
-      tma::emulate_box(p.in_view, 0, 0, (int)gr.g0, (int)gr.b, raw.data(), true);
+      tma::emulate_box(p.in_view, 0, 0, (int)gr.g0, (int)gr.b, raw, true);
     else
       for (int k = 0; k < L / Sh::RB; ++k)
-        tma::emulate_box(p.in_view, (int)(2 * gr.g0), k * Sh::RB, (int)gr.b, 0, raw.data() + k * Sh::RB * Sh::GC, true);
-    run_stages<T, INV, L, Sh, Q, 0, IR, OR>(rows::HostT{}, p.a, raw.data(), gr.g0);
+        tma::emulate_box(p.in_view, (int)(2 * gr.g0), k * Sh::RB, (int)gr.b, 0, raw + k * Sh::RB * Sh::GC, true);
+    run_stages<T, INV, L, Sh, Q, 0, IR, OR>(rows::HostT{}, p.a, raw, gr.g0);
     if (OR)
-      tma::emulate_box(p.out_view, 0, 0, (int)gr.g0, (int)gr.b, raw.data(), false);
+      tma::emulate_box(p.out_view, 0, 0, (int)gr.g0, (int)gr.b, raw, false);
     else
       for (int k = 0; k < L / Sh::RB; ++k)
-        tma::emulate_box(p.out_view, (int)(2 * gr.g0), k * Sh::RB, (int)gr.b, 0, raw.data() + k * Sh::RB * Sh::GC,
+        tma::emulate_box(p.out_view, (int)(2 * gr.g0), k * Sh::RB, (int)gr.b, 0, raw + k * Sh::RB * Sh::GC,
                          false);
   }
 }

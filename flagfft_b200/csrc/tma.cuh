@@ -127,9 +127,16 @@ __device__ __forceinline__ void wait_all() {
 // Host emulation of one box copy between a View and a dense shared-memory
 // box (box[0] innermost), zero-filling reads outside the view and dropping
 // writes outside it, as the hardware does.
+// A copy the hardware would refuse (shared-memory address not 128-byte
+// aligned, global base not 16-byte aligned, or an innermost coordinate whose
+// byte offset is not a multiple of 16) moves nothing, so the caller's result
+// comes out wrong instead of silently right.
 inline void emulate_box(const View &v, int c0, int c1, int c2, int c3, void *smem, bool load) {
   const size_t sb = (size_t)v.scalar_bytes;
   unsigned char *s = static_cast<unsigned char *>(smem);
+  if ((reinterpret_cast<uintptr_t>(smem) & 127) != 0 || (reinterpret_cast<uintptr_t>(v.base) & 15) != 0 ||
+      (((long long)c0 * (long long)sb) & 15) != 0)
+    return;
   for (unsigned i3 = 0; i3 < v.box[3]; ++i3)
     for (unsigned i2 = 0; i2 < v.box[2]; ++i2)
       for (unsigned i1 = 0; i1 < v.box[1]; ++i1)

@@ -1,0 +1,69 @@
+"""CPU checks of the engine's index arithmetic through its host-emulation
+build (the kernel and lowering sources compiled with FFB_HOST_EMULATION; the
+kernels run sequentially on the CPU and the TMA box copies are done by hand,
+refusing the ones the hardware would refuse for alignment).  Results are
+compared with the FP64 oracle.  These tests prove nothing about GPU timing or
+memory ordering; they catch layout, stride, ring-slot and table mistakes
+before a kernel reaches a GPU."""
+import numpy as np
+import pytest
+
+import hostcheck as H
+from oracle import oracle as O
+
+C2C, R2C, C2R, Z2Z, D2Z, Z2D = 0x29, 0x2A, 0x2C, 0x69, 0x6A, 0x6C
+
+
+def _rel(a, b):
+    a = np.asarray(a, np.complex128).reshape(-1)
+    b = np.asarray(b, np.complex128).reshape(-1)
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+def _bound(n, double):
+    return (1e-15 if double else 5e-7) * max(1.0, np.log2(n)) * 4
+
+
+def _describe(plan):
+    h = plan()
+    try:
+        return H.describe(h)
+    finally:
+        H.lib().flagfftDestroy(h)
+
+
+# (n0, n1, double): the column pass is a TMA column pass of length n0 whose
+# groups fill every ring slot (n1 / transforms-per-group > 3)
+@pytest.mark.parametrize("n0,n1,double", [(1024, 40, False), (2048, 24, False), (4096, 12, False),
+                                          (1536, 20, False), (1024, 20, True), (2048, 10, True),
+                                          (1536, 12, True)])
+def test_tma_column_pass_2d(n0, n1, double):
+    x = O.random_complex(n0 * n1, O.accuracy_seed(C2C, n0, n1), double=True).reshape(n0, n1)
+    d = _describe(lambda: H.plan2d(n0, n1, Z2Z if double else C2C))
+    assert "tma-columns" in d, d
+    for direction, kind in ((-1, "c2c_fwd"), (1, "c2c_inv")):
+        ref = O.fft2(x, "c2c", direction)
+        got = H.fft2(x, kind, double=double)
+        assert _rel(got, ref) < _bound(n0 * n1, double), (kind, _rel(got, ref))
+
+
+@pytest.mark.parametrize("n,batch,double", [(1 << 20, 1, False), (1 << 20, 2, True)])
+def test_tma_column_four_step_c2c(n, batch, double):
+    x = O.random_complex(n * batch, O.accuracy_seed(C2C, n, batch), double=True).reshape(batch, n)
+    d = _describe(lambda: H.plan1d(n, Z2Z if double else C2C, batch))
+    assert "tma-columns" in d, d
+    got = H.c2c(x, -1, double)
+    ref = np.stack([O.c2c(r, -1) for r in x])
+    assert _rel(got, ref) < _bound(n, double)
+
+
+# a 1536-point column pass in double precision (the 3 * 2^20 real transform)
+# and a power-of-two real transform, forward and back
+@pytest.mark.parametrize("n,batch,double", [(3 << 19, 2, True), (1 << 21, 1, False)])
+def test_tma_column_real_round_trip(n, batch, double):
+    x = O.random_normal(n * batch, O.accuracy_seed(R2C, n, batch), double=True).reshape(batch, n)
+    spec = H.r2c(x, double)
+    ref = np.stack([O.r2c(r) for r in x])
+    assert _rel(spec, ref) < _bound(n, double)
+    back = H.c2r(ref, n, double)
+    assert _rel(back, x * n) < _bound(n, double)
