@@ -36,6 +36,13 @@ struct PassBase {
   virtual cudaError_t run(const void *in, void *out, void *s0, void *s1, cudaStream_t st) const = 0;
   virtual std::string describe() const = 0;
   virtual int launches() const { return 1; }
+  // A copy of this pass for `to` transforms where it was lowered for `from`
+  // (batch-proportional passes; nullptr for a pass that cannot be re-sized).
+  virtual std::shared_ptr<PassBase> rebatched(long long from, long long to) const {
+    (void)from;
+    (void)to;
+    return nullptr;
+  }
 };
 
 // One direction of one plan: a fixed sequence of passes.

@@ -2,6 +2,7 @@
 // the request server (serve.cpp).
 #pragma once
 
+#include <memory>
 #include <sstream>
 #include <string>
 
@@ -103,6 +104,11 @@ struct RealPass final : PassBase {
     return post ? launch_real_post<T>(sp, dp, batch, sdist, ddist, L, rtw, st)
                 : launch_real_pre<T>(sp, dp, batch, sdist, ddist, L, rtw, st);
   }
+  std::shared_ptr<PassBase> rebatched(long long from, long long to) const override {
+    auto q = std::make_shared<RealPass<T>>(*this);
+    q->batch = batch / from * to;
+    return q;
+  }
   std::string describe() const override {
     std::ostringstream o;
     o << (post ? "real-post" : "real-pre") << " " << (sizeof(T) == 4 ? "f32" : "f64") << " L=" << L
@@ -120,6 +126,11 @@ struct TransposePass final : PassBase {
   cudaError_t run(const void *in, void *out, void *s0, void *s1, cudaStream_t st) const override {
     return launch_transpose<T>(reinterpret_cast<const cpx<T> *>(TilePass<T>::pick(src, in, out, s0, s1)),
                                reinterpret_cast<cpx<T> *>(TilePass<T>::pick(dst, in, out, s0, s1)), batch, R, C, st);
+  }
+  std::shared_ptr<PassBase> rebatched(long long from, long long to) const override {
+    auto q = std::make_shared<TransposePass<T>>(*this);
+    q->batch = batch / from * to;
+    return q;
   }
   std::string describe() const override {
     std::ostringstream o;
@@ -141,6 +152,11 @@ struct ConvertPass final : PassBase {
   cudaError_t run(const void *in, void *out, void *s0, void *s1, cudaStream_t st) const override {
     return launch_real_convert<T>(mode, TilePass<T>::pick(src, in, out, s0, s1),
                                   TilePass<T>::pick(dst, in, out, s0, s1), batch, sdist, ddist, n, st);
+  }
+  std::shared_ptr<PassBase> rebatched(long long from, long long to) const override {
+    auto q = std::make_shared<ConvertPass<T>>(*this);
+    q->batch = batch / from * to;
+    return q;
   }
   std::string describe() const override {
     static const char *names[4] = {"real-widen", "half-take", "hermitian-expand", "real-take"};

@@ -286,7 +286,7 @@ class Server {
     NodePtr root = build_raw_root(*pl->second, n, nullptr, nullptr);
     if (!raw_supported(root)) return nullptr;
     Layout lay;
-    lay.batch = 2;
+    lay.batch = kTemplateBatch;
     int64_t ib = 0, ob = 0;
     io_elems(type, n, &ib, &ob);
     const int64_t esz_in = type == FLAGFFT_R2C ? 4 : type == FLAGFFT_D2Z ? 8 : dbl ? 16 : 8;
@@ -295,17 +295,29 @@ class Server {
     lay.odist = ob / esz_out;
     auto t = std::make_unique<Template>();
     t->prog = lower(root, *pl->second, dbl, tr, inv, n, lay, false);
-    t->ws0_per = t->prog->scratch0 ? t->prog->scratch0->bytes / 2 : 0;
-    t->ws1_per = t->prog->scratch1 ? t->prog->scratch1->bytes / 2 : 0;
+    if (!servable(*t->prog)) return nullptr;
+    t->ws0_per = t->prog->scratch0 ? t->prog->scratch0->bytes / kTemplateBatch : 0;
+    t->ws1_per = t->prog->scratch1 ? t->prog->scratch1->bytes / kTemplateBatch : 0;
     const Template *raw = t.get();
     tpls_.emplace(key, std::move(t));
     return raw;
   }
 
+  // Every pass of a template is a tile pass or re-sizes to a request's batch.
+  static bool servable(const Program &prog) {
+    for (const auto &pb : prog.passes)
+      if (!dynamic_cast<const TilePass<float> *>(pb.get()) && !dynamic_cast<const TilePass<double> *>(pb.get()) &&
+          !pb->rebatched(kTemplateBatch, kTemplateBatch))
+        return false;
+    return true;
+  }
+
   // ---- tick assembly for one precision
+  // (a template's tile passes carry its batch as the outer batch, or, for
+  // single-pass lowerings, as the transform count per outer batch)
   template <typename T>
   static void retarget(TileArgs<T> &a, int64_t b) {
-    if (a.nbatch == 2)
+    if (a.nbatch == kTemplateBatch)
       a.nbatch = b;
     else
       a.G = (int)b;
@@ -364,12 +376,13 @@ class Server {
         w.arg_phase.push_back((int)p);
         w.arg_cls.push_back(cls);
         // items are numbered after all requests are in (tile counts need the class width)
-      } else if (auto *rp = dynamic_cast<const RealPass<T> *>(pb)) {
-        RealPass<T> q = *rp;
-        q.batch = r.batch;
+      } else {
+        // every other pass (Hermitian post / pre, widen / take, transposes)
+        // at the request's batch; templates hold no other kind (servable())
+        std::shared_ptr<PassBase> q = pb->rebatched(kTemplateBatch, r.batch);
         const void *in = r.in;
         void *out = r.out, *s0 = r.ws0, *s1 = r.ws1;
-        own[p].push_back([q, in, out, s0, s1](cudaStream_t st) { return q.run(in, out, s0, s1, st); });
+        own[p].push_back([q, in, out, s0, s1](cudaStream_t st) { return q->run(in, out, s0, s1, st); });
       }
     }
   }
@@ -601,6 +614,7 @@ class Server {
   }
 
   static constexpr size_t kMaxPerTick = 4096;
+  static constexpr int64_t kTemplateBatch = 2;  // transforms a template program is lowered for
   static constexpr size_t kCoalesceMin = 16;
   static constexpr double kCoalesceWait = 50e-6;  // seconds
 

@@ -13,7 +13,10 @@ pytestmark = pytest.mark.gpu
 # (type name, n, batch, direction)
 MIX = [("C2C", 1009, 3, -1), ("Z2Z", 64, 5, 1), ("R2C", 4096, 2, -1), ("C2C", 10007, 2, 1), ("C2C", 16, 7, -1),
        ("D2Z", 999, 3, -1), ("C2C", 61423, 1, -1), ("C2R", 1000, 2, 1), ("Z2Z", 1701, 4, -1), ("C2C", 4096, 64, 1),
-       ("C2C", 16384, 2, -1), ("C2C", 131072, 1, 1)]
+       ("C2C", 16384, 2, -1), ("C2C", 131072, 1, 1),
+       # real lengths without an on-chip core: widened to complex (odd n) or a
+       # multi-pass half-length transform with a Hermitian pre pass (2 x prime)
+       ("R2C", 30011, 2, -1), ("C2R", 60022, 2, 1), ("D2Z", 20011, 1, -1)]
 
 
 def _inputs(ffb, torch, seed):

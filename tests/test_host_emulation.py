@@ -67,3 +67,52 @@ def test_tma_column_real_round_trip(n, batch, double):
     assert _rel(spec, ref) < _bound(n, double)
     back = H.c2r(ref, n, double)
     assert _rel(back, x * n) < _bound(n, double)
+
+
+def _server_run(reqs):
+    """Submits every (type code, n, batch, direction, input) to one server of
+    the host-emulation build and returns the outputs."""
+    import ctypes
+    L = H.lib()
+    vp, i = ctypes.c_void_p, ctypes.c_int
+    L.flagfftB200ServerCreate.argtypes = [ctypes.POINTER(vp), ctypes.c_longlong, i]
+    L.flagfftB200ServerSubmit.argtypes = [vp, i, i, i, i, vp, vp, ctypes.POINTER(ctypes.c_longlong)]
+    L.flagfftB200ServerWait.argtypes = [vp, ctypes.c_longlong, ctypes.POINTER(ctypes.c_double)]
+    L.flagfftB200ServerDestroy.argtypes = [vp]
+    srv = vp()
+    assert L.flagfftB200ServerCreate(ctypes.byref(srv), 1 << 30, 2) == 0
+    outs, tickets = [], []
+    try:
+        for code, n, b, d, x in reqs:
+            dbl = code in (Z2Z, D2Z, Z2D)
+            if code in (R2C, D2Z):
+                y = np.empty((b, n // 2 + 1), np.complex128 if dbl else np.complex64)
+            elif code in (C2R, Z2D):
+                y = np.empty((b, n), np.float64 if dbl else np.float32)
+            else:
+                y = np.empty((b, n), np.complex128 if dbl else np.complex64)
+            tk = ctypes.c_longlong()
+            assert L.flagfftB200ServerSubmit(srv, code, n, b, d, H._p(x), H._p(y), ctypes.byref(tk)) == 0
+            outs.append(y)
+            tickets.append(tk.value)
+        for tk in tickets:
+            lat = ctypes.c_double()
+            assert L.flagfftB200ServerWait(srv, tk, ctypes.byref(lat)) == 0
+    finally:
+        L.flagfftB200ServerDestroy(srv)
+    return outs
+
+
+def test_server_real_lengths_without_an_on_chip_core():
+    """Real requests whose lowering has widen / take or Hermitian pre / post
+    passes around a multi-pass complex transform: every pass runs at the
+    request's batch."""
+    n_odd, n_even, n_dbl = 30011, 60022, 20011
+    x1 = O.random_real(2 * n_odd, 11).reshape(2, n_odd).astype(np.float32)
+    x2 = np.fft.rfft(O.random_real(3 * n_even, 12).reshape(3, n_even).astype(np.float64), axis=-1).astype(np.complex64)
+    x3 = O.random_real(n_dbl, 13, True).reshape(1, n_dbl).astype(np.float64)
+    outs = _server_run([(R2C, n_odd, 2, -1, x1), (C2R, n_even, 3, 1, x2), (D2Z, n_dbl, 1, -1, x3)])
+    assert _rel(outs[0], np.stack([O.r2c(r.astype(np.float64)) for r in x1])) < _bound(n_odd, False)
+    ref2 = np.stack([O.c2r(r.astype(np.complex128), n_even) for r in x2])
+    assert _rel(outs[1], ref2) < _bound(n_even, False)
+    assert _rel(outs[2], np.stack([O.r2c(r) for r in x3])) < _bound(n_dbl, True)
