@@ -29,28 +29,33 @@ cudaError_t launch_rows_any(const TileArgs<T> &a, size_t smem, cudaStream_t s);
 
 namespace {
 
-// One thread per pair (k, L-k), k = 0..L/2: reads both Z values, writes both
-// X values, so z and x may alias.
+// Pair (k, L-k), k = 0..L/2, of the Hermitian post-processing: from both Z
+// values, both X values (k = 0: X_0 and X_L from Z_0).
 template <typename T>
-FFB_HD void real_post_pair(const cpx<T> *z, cpx<T> *x, int L, int k, const RealTw<T> &rtw) {
-  auto post = [&](cpx<T> zk, cpx<T> zm, int kk) {
-    cpx<T> ev = mk((zk.x + zm.x) * (T)0.5, (zk.y - zm.y) * (T)0.5);
-    cpx<T> od = mk((zk.y + zm.y) * (T)0.5, (zm.x - zk.x) * (T)0.5);
+FFB_HD void real_post_vals(cpx<T> zk, cpx<T> zm, int L, int k, const RealTw<T> &rtw, cpx<T> &xk, cpx<T> &xm) {
+  auto post = [&](cpx<T> a, cpx<T> b, int kk) {
+    cpx<T> ev = mk((a.x + b.x) * (T)0.5, (a.y - b.y) * (T)0.5);
+    cpx<T> od = mk((a.y + b.y) * (T)0.5, (b.x - a.x) * (T)0.5);
     return ev + cmul(real_tw(rtw, (uint32_t)kk), od);
   };
+  xk = post(zk, zm, k);
+  xm = post(zm, zk, L - k);
+}
+// One thread per pair: reads both Z values, writes both X values, so z and
+// x may alias.
+template <typename T>
+FFB_HD void real_post_pair(const cpx<T> *z, cpx<T> *x, int L, int k, const RealTw<T> &rtw) {
   const int m = L - k;
-  cpx<T> zk = z[k == 0 ? 0 : k];
-  cpx<T> zm = z[k == 0 ? 0 : m];
-  cpx<T> xk = post(zk, zm, k);
-  cpx<T> xm = post(zm, zk, m);  // k = 0: X_L from Z_0
+  cpx<T> xk, xm;
+  real_post_vals<T>(z[k], z[k == 0 ? 0 : m], L, k, rtw, xk, xm);
   x[k] = xk;
   if (m != k) x[m] = xm;
 }
 
-// One thread per pair (k, L-k), k = 0..L/2: reads X_k and X_{L-k} once and
-// writes Z_k and Z_{L-k} (Z_0 from X_0 and X_L; Im X_0 and Im X_L ignored).
+// Pair (k, L-k) of the Hermitian pre-processing: Z_k and Z_{L-k} from X_k
+// and X_{L-k} (Z_0 from X_0 and X_L; Im X_0 and Im X_L ignored).
 template <typename T>
-FFB_HD void real_pre_pair(const cpx<T> *x, cpx<T> *z, int L, int k, const RealTw<T> &rtw) {
+FFB_HD void real_pre_vals(cpx<T> xk, cpx<T> xm, int L, int k, const RealTw<T> &rtw, cpx<T> &zk, cpx<T> &zm) {
   auto pre = [&](cpx<T> a, cpx<T> b, int kk) {  // a = X_kk, b = X_{L-kk}
     const cpx<T> s = mk(a.x + b.x, a.y - b.y);
     const cpx<T> d = mk(a.x - b.x, a.y + b.y);
@@ -58,32 +63,92 @@ FFB_HD void real_pre_pair(const cpx<T> *x, cpx<T> *z, int L, int k, const RealTw
     const cpx<T> dw = mk(d.x * w.x + d.y * w.y, d.y * w.x - d.x * w.y);
     return mk(s.x - dw.y, s.y + dw.x);
   };
-  const int m = L - k;
-  cpx<T> xk = x[k], xm = x[m];
   if (k == 0) {
     xk.y = (T)0;
     xm.y = (T)0;
   }
-  z[k] = pre(xk, xm, k);
-  if (m != k && m < L) z[m] = pre(xm, xk, m);
+  zk = pre(xk, xm, k);
+  zm = pre(xm, xk, L - k);
+}
+template <typename T>
+FFB_HD void real_pre_pair(const cpx<T> *x, cpx<T> *z, int L, int k, const RealTw<T> &rtw) {
+  const int m = L - k;
+  cpx<T> zk, zm;
+  real_pre_vals<T>(x[k], x[m], L, k, rtw, zk, zm);
+  z[k] = zk;
+  if (m != k && m < L) z[m] = zm;
+}
+
+#ifndef FFB_HOST_EMULATION
+
+constexpr int kRealThreads = 256, kRealUnroll = 4;
+
+// U pairs per thread, k = k0 + u * stride: every load of the U pairs issued
+// before the first store (bytes in flight), pairs of one thread disjoint
+// from every other thread's, so the passes may run in place.
+template <typename T>
+__global__ void __launch_bounds__(kRealThreads) k_real_post(const cpx<T> *z, cpx<T> *x, long long zdist,
+                                                            long long xdist, int L, const RealTw<T> rtw) {
+  pdl_entry();
+  const long long b = blockIdx.y;
+  z += b * zdist;
+  x += b * xdist;
+  const int stride = gridDim.x * blockDim.x, half = L / 2;
+  for (int k0 = blockIdx.x * blockDim.x + threadIdx.x; k0 <= half; k0 += kRealUnroll * stride) {
+    cpx<T> a[kRealUnroll], c[kRealUnroll];
+#pragma unroll
+    for (int u = 0; u < kRealUnroll; ++u) {
+      const int k = k0 + u * stride;
+      if (k <= half) {
+        a[u] = z[k];
+        c[u] = z[k == 0 ? 0 : L - k];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < kRealUnroll; ++u) {
+      const int k = k0 + u * stride;
+      if (k <= half) {
+        cpx<T> xk, xm;
+        real_post_vals<T>(a[u], c[u], L, k, rtw, xk, xm);
+        x[k] = xk;
+        if (L - k != k) x[L - k] = xm;
+      }
+    }
+  }
 }
 
 template <typename T>
-__global__ void k_real_post(const cpx<T> *z, cpx<T> *x, long long zdist, long long xdist, int L,
-                            const RealTw<T> rtw) {
+__global__ void __launch_bounds__(kRealThreads) k_real_pre(const cpx<T> *x, cpx<T> *z, long long xdist,
+                                                           long long zdist, int L, const RealTw<T> rtw) {
   pdl_entry();
   const long long b = blockIdx.y;
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k <= L / 2; k += gridDim.x * blockDim.x)
-    real_post_pair<T>(z + b * zdist, x + b * xdist, L, k, rtw);
+  x += b * xdist;
+  z += b * zdist;
+  const int stride = gridDim.x * blockDim.x, half = L / 2;
+  for (int k0 = blockIdx.x * blockDim.x + threadIdx.x; k0 <= half; k0 += kRealUnroll * stride) {
+    cpx<T> a[kRealUnroll], c[kRealUnroll];
+#pragma unroll
+    for (int u = 0; u < kRealUnroll; ++u) {
+      const int k = k0 + u * stride;
+      if (k <= half) {
+        a[u] = x[k];
+        c[u] = x[L - k];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < kRealUnroll; ++u) {
+      const int k = k0 + u * stride;
+      if (k <= half) {
+        cpx<T> zk, zm;
+        real_pre_vals<T>(a[u], c[u], L, k, rtw, zk, zm);
+        z[k] = zk;
+        if (L - k != k && L - k < L) z[L - k] = zm;
+      }
+    }
+  }
 }
 
-template <typename T>
-__global__ void k_real_pre(const cpx<T> *x, cpx<T> *z, long long xdist, long long zdist, int L, const RealTw<T> rtw) {
-  pdl_entry();
-  const long long b = blockIdx.y;
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k <= L / 2; k += gridDim.x * blockDim.x)
-    real_pre_pair<T>(x + b * xdist, z + b * zdist, L, k, rtw);
-}
+#endif  // !FFB_HOST_EMULATION
 
 template <typename T>
 __global__ void __launch_bounds__(256) k_transpose(const cpx<T> *in, cpx<T> *out, long long R, long long C) {
@@ -134,9 +199,10 @@ template <typename T>
 cudaError_t launch_real_post(const cpx<T> *z, cpx<T> *x, long long batch, long long zdist, long long xdist, int L,
                              const RealTw<T> &rtw, cudaStream_t s) {
 #ifndef FFB_HOST_EMULATION
-  const int threads = 256;
-  const int blocks = (int)std::min<long long>((L / 2 + threads) / threads, 1024);
-  return launch_pdl(k_real_post<T>, dim3(blocks, (unsigned)batch), dim3(threads), 0, s, z, x, zdist, xdist, L, rtw);
+  const int per = kRealThreads * kRealUnroll;
+  const int blocks = (int)std::min<long long>((L / 2 + per) / per, 2048);
+  return launch_pdl(k_real_post<T>, dim3(blocks, (unsigned)batch), dim3(kRealThreads), 0, s, z, x, zdist, xdist, L,
+                    rtw);
 #else
   for (long long b = 0; b < batch; ++b)
     for (int k = 0; k <= L / 2; ++k) real_post_pair<T>(z + b * zdist, x + b * xdist, L, k, rtw);
@@ -148,9 +214,10 @@ template <typename T>
 cudaError_t launch_real_pre(const cpx<T> *x, cpx<T> *z, long long batch, long long xdist, long long zdist, int L,
                             const RealTw<T> &rtw, cudaStream_t s) {
 #ifndef FFB_HOST_EMULATION
-  const int threads = 256;
-  const int blocks = (int)std::min<long long>((L / 2 + threads) / threads, 1024);
-  return launch_pdl(k_real_pre<T>, dim3(blocks, (unsigned)batch), dim3(threads), 0, s, x, z, xdist, zdist, L, rtw);
+  const int per = kRealThreads * kRealUnroll;
+  const int blocks = (int)std::min<long long>((L / 2 + per) / per, 2048);
+  return launch_pdl(k_real_pre<T>, dim3(blocks, (unsigned)batch), dim3(kRealThreads), 0, s, x, z, xdist, zdist, L,
+                    rtw);
 #else
   for (long long b = 0; b < batch; ++b)
     for (int k = 0; k <= L / 2; ++k) real_pre_pair<T>(x + b * xdist, z + b * zdist, L, k, rtw);

@@ -355,8 +355,28 @@ struct StageRegs {
   cpx<T> x[V][R];
 };
 
-template <typename T, bool INV, int L, int TPT, int Ns, int R, class Rd>
+// 16 bytes from shared memory (a 16-byte aligned address) into w[0..3].
+FFB_HD void lds_f4(const void *p, float (&w)[4]) {
+#ifdef __CUDA_ARCH__
+  asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];"
+               : "=f"(w[0]), "=f"(w[1]), "=f"(w[2]), "=f"(w[3])
+               : "r"((uint32_t)__cvta_generic_to_shared(p)));
+#else
+  const float *f = static_cast<const float *>(p);
+  for (int i = 0; i < 4; ++i) w[i] = f[i];
+#endif
+}
+
+// Where the stage twiddles are: TW_GLOBAL the host's block (R - 1 rows of Ns
+// entries) in global memory; TW_SHARED the same block in shared memory;
+// TW_PAIRS (single precision, shared memory) rows r, r + 1 interleaved, so
+// one 16-byte load brings W^{r k} and W^{(r+1) k}: entry (m, k) of the
+// block holds rows 2m + 1 and 2m + 2 (the second one unused past R - 1).
+enum : int { TW_GLOBAL = 0, TW_SHARED = 1, TW_PAIRS = 2 };
+
+template <typename T, bool INV, int L, int TPT, int Ns, int R, int TWS = TW_GLOBAL, class Rd>
 FFB_HD StageRegs<T, L, TPT, R> stage_read(int t, const cpx<T> *__restrict__ blk, const Rd &rd) {
+  static_assert(TWS != TW_PAIRS || sizeof(T) == 4, "twiddle pairs are single precision");
   constexpr int nb = L / R;
   StageRegs<T, L, TPT, R> st;
 #pragma unroll
@@ -365,10 +385,20 @@ FFB_HD StageRegs<T, L, TPT, R> stage_read(int t, const cpx<T> *__restrict__ blk,
     if (nb % TPT == 0 || j < nb) {
       const int k = Ns == 1 ? 0 : j % Ns;
       rd.template get<nb, R>(j, st.x[v]);
-      if constexpr (Ns > 1) {
+      if constexpr (Ns > 1 && TWS == TW_PAIRS) {
+        const cpx<T> *row = blk + 2 * k;
+#pragma unroll
+        for (int r = 1; r < R; r += 2) {
+          float w[4];
+          lds_f4(row + (r - 1) * Ns, w);
+          st.x[v][r] = cmul(st.x[v][r], mk((T)w[0], (T)w[1]));
+          if (r + 1 < R) st.x[v][r + 1] = cmul(st.x[v][r + 1], mk((T)w[2], (T)w[3]));
+        }
+      } else if constexpr (Ns > 1) {
         const cpx<T> *row = blk + k;
 #pragma unroll
-        for (int r = 1; r < R; ++r) st.x[v][r] = cmul(st.x[v][r], ldg_c(row + (r - 1) * Ns));
+        for (int r = 1; r < R; ++r)
+          st.x[v][r] = cmul(st.x[v][r], TWS == TW_SHARED ? row[(r - 1) * Ns] : ldg_c(row + (r - 1) * Ns));
       }
       dft_fixed<R, INV, T>(st.x[v]);
     }

@@ -47,17 +47,19 @@ bool make_view(const void *base, long long nbatch, long long G, long long b_stri
     v->box[2] = GC;
     v->box[3] = 1;
   } else if (g_stride == 1 && e_stride >= G) {
+    // element i = i_hi * RB + i_lo: the whole GC x L tile is one box
+    // (boxes are at most 256 per dimension), laid out [i_hi][i_lo][c]
     *is_rows = 0;
     v->dims[0] = 2 * (unsigned long long)G;
-    v->dims[1] = L;
-    v->dims[2] = (unsigned long long)nbatch;
-    v->dims[3] = 1;
+    v->dims[1] = RB;
+    v->dims[2] = L / RB;
+    v->dims[3] = (unsigned long long)nbatch;
     v->strides[0] = (unsigned long long)e_stride * es;
-    v->strides[1] = nbatch > 1 ? (unsigned long long)b_stride * es : v->strides[0] * L;
-    v->strides[2] = v->strides[1] * v->dims[2];
+    v->strides[1] = v->strides[0] * RB;
+    v->strides[2] = nbatch > 1 ? (unsigned long long)b_stride * es : v->strides[1] * (L / RB);
     v->box[0] = 2 * GC;
     v->box[1] = RB;
-    v->box[2] = 1;
+    v->box[2] = L / RB;
     v->box[3] = 1;
   } else {
     return false;
@@ -134,7 +136,7 @@ cudaError_t launch_seq(const TileArgs<T> &a, cudaStream_t s) {
   {                                                                                      \
     auto k = k_tcols<T, INV, L, IR, OR, Rs...>;                                          \
     if ((e = set_smem_limit_once<k_tcols<T, INV, L, IR, OR, Rs...>>((int)Sh::smem)) != cudaSuccess) return e; \
-    if ((e = launch_pdl(k, dim3((unsigned)ctas), dim3(Sh::NT + 32), Sh::smem, s, p)) != cudaSuccess) return e; \
+    if ((e = launch_pdl(k, dim3((unsigned)ctas), dim3(Sh::NT), Sh::smem, s, p)) != cudaSuccess) return e; \
   }
   if (p.in_rows)
     FFB_TCOLS_GO(true, false)
@@ -157,6 +159,12 @@ void emulate(const Args<T> &p) {
   std::vector<unsigned char> image(Sh::smem + 1024);
   unsigned char *base = image.data() + (1024 - (reinterpret_cast<uintptr_t>(image.data()) & 1023));
   cpx<T> *const ring = reinterpret_cast<cpx<T> *>(base + Sh::head);
+  const cpx<T> *tw = p.a.tw;
+  if constexpr (Sh::TWS != rows::TW_GLOBAL) {  // the kernel's shared-memory table, filled as its threads do
+    cpx<T> *tws = reinterpret_cast<cpx<T> *>(base + Sh::tw_at);
+    for (int t = 0; t < Sh::NT; ++t) fill_twiddles<T, Sh, Q>(tws, p.a.tw, t);
+    tw = tws;
+  }
   for (long long q = 0; q < p.total_groups; ++q) {
     const Group gr = group_of<Sh::GC>(q, p.groups_per_batch);
     cpx<T> *const raw = ring + (size_t)(q % Sh::NBUF) * Sh::buf_elems;
@@ -164,15 +172,12 @@ void emulate(const Args<T> &p) {
     if (IR)
       tma::emulate_box(p.in_view, 0, 0, (int)gr.g0, (int)gr.b, raw, true);
     else
-      for (int k = 0; k < L / Sh::RB; ++k)
-        tma::emulate_box(p.in_view, (int)(2 * gr.g0), k * Sh::RB, (int)gr.b, 0, raw + k * Sh::RB * Sh::GC, true);
-    run_stages<T, INV, L, Sh, Q, 0, IR, OR>(rows::HostT{}, p.a, raw, gr.g0);
+      tma::emulate_box(p.in_view, (int)(2 * gr.g0), 0, 0, (int)gr.b, raw, true);
+    run_stages<T, INV, L, Sh, Q, 0, IR, OR, Sh::TWS>(rows::HostT{}, p.a, tw, raw, gr.g0, [] {});
     if (OR)
       tma::emulate_box(p.out_view, 0, 0, (int)gr.g0, (int)gr.b, raw, false);
     else
-      for (int k = 0; k < L / Sh::RB; ++k)
-        tma::emulate_box(p.out_view, (int)(2 * gr.g0), k * Sh::RB, (int)gr.b, 0, raw + k * Sh::RB * Sh::GC,
-                         false);
+      tma::emulate_box(p.out_view, (int)(2 * gr.g0), 0, 0, (int)gr.b, raw, false);
   }
 }
 
