@@ -197,13 +197,11 @@ struct TwiddledOut {
 // tile in the input's layout, the last writes it in the output's layout, the
 // ones between use the swizzled working layout.  Every stage reads, crosses a
 // barrier (its values wait in registers) and writes; a barrier separates
-// consecutive stages and none follows the last.  mid() runs in every thread
-// after the barrier that follows stage 0.
+// consecutive stages and none follows the last.
 // tw: the host's twiddle block in global memory (TWS = rows::TW_GLOBAL) or
 // the shared-memory table (tw_table_off layout).
-template <typename T, bool INV, int L, class Sh, class Q, int S, bool IN_ROWS, bool OUT_ROWS, int TWS, class X,
-          class M>
-FFB_HD void run_stages(const X &x, const TileArgs<T> &a, const cpx<T> *tw, cpx<T> *raw, long long g0, const M &mid) {
+template <typename T, bool INV, int L, class Sh, class Q, int S, bool IN_ROWS, bool OUT_ROWS, int TWS, class X>
+FFB_HD void run_stages(const X &x, const TileArgs<T> &a, const cpx<T> *tw, cpx<T> *raw, long long g0) {
   static_assert(Q::n >= 2, "the tile is read by the first stage and written by the last");
   constexpr int R = Q::r(S), Ns = Q::span(S);
   constexpr int TwOff = TWS == rows::TW_GLOBAL ? Q::twoff(S) : tw_off_of<Q, TWS == rows::TW_PAIRS>(S);
@@ -238,8 +236,7 @@ FFB_HD void run_stages(const X &x, const TileArgs<T> &a, const cpx<T> *tw, cpx<T
   x.each2(NT, rd, wr);
   if constexpr (!last) {
     x.sync();
-    if constexpr (S == 0) mid();
-    run_stages<T, INV, L, Sh, Q, S + 1, IN_ROWS, OUT_ROWS, TWS>(x, a, tw, raw, g0, mid);
+    run_stages<T, INV, L, Sh, Q, S + 1, IN_ROWS, OUT_ROWS, TWS>(x, a, tw, raw, g0);
   }
 }
 
@@ -353,9 +350,13 @@ struct ComputeThreads {
 // group i - 1, waits until its store of group i - 2 has read its slot out --
 // issued a group of compute earlier, so in practice no wait -- and loads
 // group i + 1 into that slot: a load has a group of compute to land.
-// full[s] counts a load's bytes.  Every wait is bounded; a wait that gives
-// up is counted in g_tcols_wait_failures, the threads leave the loop
-// together and thread 0 lets the load in flight land before the CTA ends.
+// (Loading group i + 2 late in group i instead, once the store of group
+// i - 1 has drained, measured 8-26% slower on the 2^24-point real
+// transforms: thread 0's wait for that store held every warp at the next
+// barrier.)  full[s] counts a load's bytes.  Every wait is bounded; a wait
+// that gives up is counted in g_tcols_wait_failures, the threads leave the
+// loop together and thread 0 lets the load in flight land before the CTA
+// ends.
 template <typename T, bool INV, int L, bool IN_ROWS, bool OUT_ROWS, int... Rs>
 __global__ void __launch_bounds__(Shape<T, L, Rs...>::NT, 1) k_tcols(const __grid_constant__ Args<T> p) {
   pdl_entry();
@@ -376,8 +377,7 @@ __global__ void __launch_bounds__(Shape<T, L, Rs...>::NT, 1) k_tcols(const __gri
     tma::fence_mbar_init();
   }
   __syncwarp();
-  if (issuer && group(0) < p.total_groups)
-    issue_load<T, L, Sh::GC, Sh::RB>(p, &p.in_map, group(0), slot(0), &full[0]);
+  if (issuer && group(0) < p.total_groups) issue_load<T, L, Sh::GC, Sh::RB>(p, &p.in_map, group(0), slot(0), &full[0]);
   const ComputeThreads x{Sh::NT};
   const cpx<T> *tw = p.a.tw;
   if constexpr (Sh::TWS != rows::TW_GLOBAL) {
@@ -402,7 +402,7 @@ __global__ void __launch_bounds__(Shape<T, L, Rs...>::NT, 1) k_tcols(const __gri
       }
     }
     const Group gr = group_of<Sh::GC>(group(i), p.groups_per_batch);
-    run_stages<T, INV, L, Sh, Q, 0, IN_ROWS, OUT_ROWS, Sh::TWS>(x, p.a, tw, slot(i), gr.g0, [] {});
+    run_stages<T, INV, L, Sh, Q, 0, IN_ROWS, OUT_ROWS, Sh::TWS>(x, p.a, tw, slot(i), gr.g0);
     tma::fence_async_smem();  // this thread's writes, before thread 0's TMA store reads them
   }
   x.sync();  // the last group is written (or the threads left together)

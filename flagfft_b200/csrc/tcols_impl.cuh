@@ -173,7 +173,7 @@ void emulate(const Args<T> &p) {
       tma::emulate_box(p.in_view, 0, 0, (int)gr.g0, (int)gr.b, raw, true);
     else
       tma::emulate_box(p.in_view, (int)(2 * gr.g0), 0, 0, (int)gr.b, raw, true);
-    run_stages<T, INV, L, Sh, Q, 0, IR, OR, Sh::TWS>(rows::HostT{}, p.a, tw, raw, gr.g0, [] {});
+    run_stages<T, INV, L, Sh, Q, 0, IR, OR, Sh::TWS>(rows::HostT{}, p.a, tw, raw, gr.g0);
     if (OR)
       tma::emulate_box(p.out_view, 0, 0, (int)gr.g0, (int)gr.b, raw, false);
     else
