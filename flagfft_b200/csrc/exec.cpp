@@ -788,6 +788,49 @@ class Builder {
     a.ptw_div = make_fastdiv((uint32_t)split);
   }
 
+  // The same split tables as a transpose's twiddle W_N^{r c}.
+  SplitTw<T> split_tw(int64_t N, bool inverse) {
+    TileArgs<T> a{};
+    set_post_twiddle(a, N);
+    SplitTw<T> t;
+    t.lo = a.ptw_lo;
+    t.hi = a.ptw_hi;
+    t.split = a.ptw_div;
+    t.inv = inverse;
+    return t;
+  }
+
+  // Tables of a multi-pass Rader chain for prime p (generator g): the
+  // gather q -> g^-q, the scatter q -> g^q and FFT_m(b) / m in natural order,
+  // b_q = W_p^{sign g^q} (src/plan/rader_utils.cpp:55-90,
+  // src/codegen/tables.cpp:218-258).
+  struct RaderChain {
+    const int *perm_in, *perm_out;
+    const cpx<T> *kern;
+  };
+  RaderChain rader_chain(int64_t p, int64_t g, bool inverse) {
+    const int64_t m = p - 1;
+    const std::string pk = std::to_string(p) + "|g" + std::to_string(g);
+    const auto idx = rader_index_table(p, g);
+    RaderChain r;
+    r.perm_in = cached<int>("rcin|" + pk, [&]() {
+      std::vector<int> v((size_t)m);
+      for (int64_t q = 0; q < m; ++q) v[(size_t)q] = (int)idx[(size_t)(q == 0 ? 0 : m - q)];
+      return v;
+    });
+    r.perm_out = cached<int>("rpout|" + pk, [&]() {
+      std::vector<int> v((size_t)m);
+      for (int64_t q = 0; q < m; ++q) v[(size_t)q] = (int)idx[(size_t)q];
+      return v;
+    });
+    r.kern = cached<cpx<T>>("rchain|" + pk + (inverse ? "|inv" : "|fwd"), [&]() {
+      std::vector<cld> b((size_t)m);
+      for (int64_t q = 0; q < m; ++q) b[(size_t)q] = unit_root(idx[(size_t)q], p, inverse ? 1 : -1);
+      return kernel_spectrum(b, true, {});
+    });
+    return r;
+  }
+
  private:
   // Chirp, kernel spectrum and permutation tables of a Bluestein / Rader core.
   void fill_convolution(TileArgs<T> &a, const CoreSpec &spec, bool inverse) {
@@ -876,9 +919,106 @@ static int onchip_policy() {
   return s == "inplace" ? 1 : s == "multipass" ? 2 : 0;
 }
 
+// Plan-tree lowering ($FLAGFFT_TREE_LOWERING=1): a four-step whose child
+// needs more than one pass, and a Rader prime whose p - 1 transform needs
+// more than one pass, run as the tree says -- the reference's generic
+// four-step (src/exec/raw_nodes.cpp:340-394: reshape, row child, twiddle
+// reshape, column child, pack) and Rader chain (raw_nodes.cpp:252-305:
+// gather, child FFT, kernel product, child FFT, scatter) around the
+// children's own lowerings -- instead of the executor's own split or a
+// Bluestein chain of the whole length (fewer HBM round trips, the default).
+// A tree lowering keeps its working rows in workspace 1; a child that would
+// need workspace 1 itself runs the executor's way.
+static bool tree_lowering() {
+  const char *v = std::getenv("FLAGFFT_TREE_LOWERING");
+  return v && v[0] == '1';
+}
+
+template <typename T>
+void lower_c2c(Builder<T> &bld, Program &prog, const NodePtr &root, bool inverse, int64_t n, int64_t batch,
+               long long idist, long long odist, Buf src, Buf dst);
+
+// True when node's lowering under the current policy is a tree lowering
+// (it would use workspace 1).
+template <typename T>
+bool needs_tree_lowering(Builder<T> &bld, const NodePtr &node) {
+  if (!tree_lowering() || !node) return false;
+  CoreSpec a, b;
+  if (node->kind == NodeKind::FourStep)
+    return !(bld.core_for(node->row, a) && bld.core_for(node->col, b)) && !bld.core_for(node, a);
+  if (node->kind == NodeKind::Rader) return !bld.core_for(node, a) || a.kind != CoreKind::Rader;
+  return false;
+}
+
+// The plan tree's four-step over children of any lowering: x viewed as
+// n1 x n2 (x[j1 n2 + j2]) is transposed to n2 rows of n1, the n1-point
+// child runs on them, a twiddled transpose (W_N^{j2 k1}) gives n1 rows of
+// n2, the n2-point child runs on those into workspace 1, and a last
+// transpose gives X[k1 + n1 k2].  Workspace 1 holds the working rows; the
+// children use workspace 0.
+template <typename T>
+bool lower_tree_four_step(Builder<T> &bld, Program &prog, const NodePtr &root, bool inverse, int64_t n,
+                          int64_t batch, long long idist, long long odist, Buf src, Buf dst) {
+  if (needs_tree_lowering(bld, root->row) || needs_tree_lowering(bld, root->col)) return false;
+  if (src == Buf::Scratch1 || dst == Buf::Scratch1) return false;
+  const int64_t n1 = root->n1, n2 = root->n2;
+  // (the n2-point rows are formed in the output, so its rows are contiguous;
+  // the children's multi-pass lowerings take at most 65535 rows)
+  if (n1 * n2 != n || odist != n || batch * std::max(n1, n2) > 65535) return false;
+  ensure_scratch(prog.scratch1, (size_t)(batch * n) * sizeof(cpx<T>));
+  auto t1 = std::make_unique<TransposePass<T>>(src, Buf::Scratch1, batch, n1, n2);
+  t1->sdist = idist;
+  t1->ddist = n;
+  prog.passes.push_back(std::move(t1));
+  lower_c2c<T>(bld, prog, root->row, inverse, n1, batch * n2, n1, n1, Buf::Scratch1, Buf::Scratch1);
+  auto t2 = std::make_unique<TransposePass<T>>(Buf::Scratch1, dst, batch, n2, n1);
+  t2->sdist = n;
+  t2->ddist = odist;
+  t2->tw = bld.split_tw(n, inverse);
+  prog.passes.push_back(std::move(t2));
+  lower_c2c<T>(bld, prog, root->col, inverse, n2, batch * n1, n2, n2, dst, Buf::Scratch1);
+  auto t3 = std::make_unique<TransposePass<T>>(Buf::Scratch1, dst, batch, n1, n2);
+  t3->sdist = n;
+  t3->ddist = odist;
+  prog.passes.push_back(std::move(t3));
+  return true;
+}
+
+// The plan tree's Rader chain over a multi-pass p - 1 transform: gather into
+// workspace 1, the child forward, the kernel product (conjugated), the child
+// forward again, scatter with x_0 added (the reference's conj(FFT(conj(.)))
+// form of the inverse).  Workspace 1: batch rows of p - 1 plus 2 * batch.
+template <typename T>
+bool lower_tree_rader(Builder<T> &bld, Program &prog, const NodePtr &root, bool inverse, int64_t batch,
+                      long long idist, long long odist, Buf src, Buf dst) {
+  const NodePtr child = root->child;
+  if (!child || needs_tree_lowering(bld, child)) return false;
+  if (src == Buf::Scratch1 || dst == Buf::Scratch1) return false;
+  const int64_t p = root->length, m = p - 1;
+  if (batch > 65535) return false;
+  ensure_scratch(prog.scratch1, (size_t)(batch * m + 2 * batch) * sizeof(cpx<T>));
+  const auto r = bld.rader_chain(p, root->root, inverse);
+  prog.passes.push_back(std::make_unique<RaderStepPass<T>>(0, src, Buf::Scratch1, dst, batch, p, idist, odist,
+                                                           r.perm_in, r.kern));
+  lower_c2c<T>(bld, prog, child, false, m, batch, m, m, Buf::Scratch1, Buf::Scratch1);
+  prog.passes.push_back(std::make_unique<RaderStepPass<T>>(1, src, Buf::Scratch1, dst, batch, p, idist, odist,
+                                                           r.perm_in, r.kern));
+  lower_c2c<T>(bld, prog, child, false, m, batch, m, m, Buf::Scratch1, Buf::Scratch1);
+  prog.passes.push_back(std::make_unique<RaderStepPass<T>>(2, src, Buf::Scratch1, dst, batch, p, idist, odist,
+                                                           r.perm_out, r.kern));
+  return true;
+}
+
 template <typename T>
 void lower_c2c(Builder<T> &bld, Program &prog, const NodePtr &root, bool inverse, int64_t n, int64_t batch,
                long long idist, long long odist, Buf src, Buf dst) {
+  if (needs_tree_lowering(bld, root)) {
+    if (root->kind == NodeKind::FourStep &&
+        lower_tree_four_step<T>(bld, prog, root, inverse, n, batch, idist, odist, src, dst))
+      return;
+    if (root->kind == NodeKind::Rader && lower_tree_rader<T>(bld, prog, root, inverse, batch, idist, odist, src, dst))
+      return;
+  }
   CoreSpec spec;
   const bool onchip = bld.core_for(root, spec);
   CoreSpec ca, cb;

@@ -117,15 +117,19 @@ struct RealPass final : PassBase {
   }
 };
 
-// Axis exchange between passes: (batch, R, C) -> (batch, C, R).
+// Axis exchange between passes: (batch, R, C) -> (batch, C, R), matrix b at
+// b * sdist / b * ddist (0: R * C), with the optional four-step twiddle
+// W_N^{r c} (tw.lo set).
 template <typename T>
 struct TransposePass final : PassBase {
   Buf src, dst;
-  long long batch, R, C;
+  long long batch, R, C, sdist = 0, ddist = 0;
+  SplitTw<T> tw{};
   TransposePass(Buf s, Buf d, long long b, long long r, long long c) : src(s), dst(d), batch(b), R(r), C(c) {}
   cudaError_t run(const void *in, void *out, void *s0, void *s1, cudaStream_t st) const override {
     return launch_transpose<T>(reinterpret_cast<const cpx<T> *>(TilePass<T>::pick(src, in, out, s0, s1)),
-                               reinterpret_cast<cpx<T> *>(TilePass<T>::pick(dst, in, out, s0, s1)), batch, R, C, st);
+                               reinterpret_cast<cpx<T> *>(TilePass<T>::pick(dst, in, out, s0, s1)), batch, R, C, st,
+                               sdist, ddist, tw);
   }
   std::shared_ptr<PassBase> rebatched(long long from, long long to) const override {
     auto q = std::make_shared<TransposePass<T>>(*this);
@@ -135,7 +139,39 @@ struct TransposePass final : PassBase {
   std::string describe() const override {
     std::ostringstream o;
     o << "transpose " << (sizeof(T) == 4 ? "f32" : "f64") << " " << R << "x" << C << " transforms=" << batch << " "
-      << buf_name(src) << "->" << buf_name(dst);
+      << buf_name(src) << "->" << buf_name(dst) << (tw.lo ? " +twiddle" : "");
+    return o.str();
+  }
+};
+
+// One elementwise step of a multi-pass Rader chain (launch_rader_step); the
+// working rows and the saved x_0 / A_0 live in `ws`.
+template <typename T>
+struct RaderStepPass final : PassBase {
+  int mode;
+  Buf src, ws, dst;
+  long long batch, p, xdist, ydist;
+  const int *perm;
+  const cpx<T> *kern;
+  RaderStepPass(int m, Buf s, Buf w, Buf d, long long b, long long p_, long long xd, long long yd, const int *pm,
+                const cpx<T> *k)
+      : mode(m), src(s), ws(w), dst(d), batch(b), p(p_), xdist(xd), ydist(yd), perm(pm), kern(k) {}
+  cudaError_t run(const void *in, void *out, void *s0, void *s1, cudaStream_t st) const override {
+    return launch_rader_step<T>(mode, reinterpret_cast<const cpx<T> *>(TilePass<T>::pick(src, in, out, s0, s1)),
+                                reinterpret_cast<cpx<T> *>(TilePass<T>::pick(ws, in, out, s0, s1)),
+                                reinterpret_cast<cpx<T> *>(TilePass<T>::pick(dst, in, out, s0, s1)), batch, p, xdist,
+                                ydist, perm, kern, st);
+  }
+  std::shared_ptr<PassBase> rebatched(long long from, long long to) const override {
+    auto q = std::make_shared<RaderStepPass<T>>(*this);
+    q->batch = batch / from * to;
+    return q;
+  }
+  std::string describe() const override {
+    static const char *names[3] = {"rader-gather", "rader-kernel-product", "rader-scatter"};
+    std::ostringstream o;
+    o << names[mode] << " " << (sizeof(T) == 4 ? "f32" : "f64") << " p=" << p << " transforms=" << batch << " "
+      << buf_name(mode == 0 ? src : ws) << "->" << buf_name(mode == 2 ? dst : ws);
     return o.str();
   }
 };

@@ -151,17 +151,27 @@ __global__ void __launch_bounds__(kRealThreads) k_real_pre(const cpx<T> *x, cpx<
 #endif  // !FFB_HOST_EMULATION
 
 template <typename T>
-__global__ void __launch_bounds__(256) k_transpose(const cpx<T> *in, cpx<T> *out, long long R, long long C) {
+__global__ void __launch_bounds__(256) k_transpose(const cpx<T> *in, cpx<T> *out, long long R, long long C,
+                                                   long long sdist, long long ddist, const SplitTw<T> tw) {
   pdl_entry();
   __shared__ cpx<T> tile[32][33];
   const long long b = blockIdx.z;
   const long long r0 = (long long)blockIdx.y * 32, c0 = (long long)blockIdx.x * 32;
-  in += b * R * C;
-  out += b * R * C;
+  in += b * sdist;
+  out += b * ddist;
 #pragma unroll
   for (int i = threadIdx.y; i < 32; i += 8) {
     const long long r = r0 + i, c = c0 + threadIdx.x;
-    if (r < R && c < C) tile[i][threadIdx.x] = in[r * C + c];
+    if (r < R && c < C) {
+      cpx<T> v = in[r * C + c];
+      if (tw.lo) {
+        const uint32_t m = (uint32_t)(r * c), hi = fdiv(m, tw.split);
+        cpx<T> w = cmul(ldg_c(tw.hi + hi), ldg_c(tw.lo + (m - hi * tw.split.d)));
+        if (tw.inv) w.y = -w.y;
+        v = cmul(v, w);
+      }
+      tile[i][threadIdx.x] = v;
+    }
   }
   __syncthreads();
 #pragma unroll
@@ -171,29 +181,100 @@ __global__ void __launch_bounds__(256) k_transpose(const cpx<T> *in, cpx<T> *out
   }
 }
 
+// One Rader chain step for element q of row b (see launch_rader_step).
+template <typename T>
+FFB_HD void rader_step_one(int mode, const cpx<T> *x, cpx<T> *ws, cpx<T> *y, long long batch, long long p,
+                           long long xdist, long long ydist, const int *perm, const cpx<T> *kern, long long b,
+                           long long q) {
+  const long long m = p - 1;
+  cpx<T> *w = ws + b * m;
+  cpx<T> *x0 = ws + batch * m + b, *a0 = ws + batch * m + batch + b;
+  if (mode == 0) {
+    w[q] = x[b * xdist + perm[q]];
+    if (q == 0) *x0 = x[b * xdist];
+  } else if (mode == 1) {
+    const cpx<T> v = w[q];
+    if (q == 0) *a0 = v;
+    const cpx<T> t = cmul(v, ldg_c(kern + q));
+    w[q] = mk(t.x, -t.y);
+  } else {
+    const cpx<T> base = *x0, v = w[q];
+    y[b * ydist + perm[q]] = mk(base.x + v.x, base.y - v.y);
+    if (q == 0) y[b * ydist] = base + *a0;
+  }
+}
+
+#ifndef FFB_HOST_EMULATION
+template <typename T>
+__global__ void __launch_bounds__(256) k_rader_step(int mode, const cpx<T> *x, cpx<T> *ws, cpx<T> *y,
+                                                    long long batch, long long p, long long xdist, long long ydist,
+                                                    const int *perm, const cpx<T> *kern) {
+  pdl_entry();
+  const long long b = blockIdx.y;
+  for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < p - 1; q += (long long)gridDim.x * blockDim.x)
+    rader_step_one<T>(mode, x, ws, y, batch, p, xdist, ydist, perm, kern, b, q);
+}
+#endif
+
 }  // namespace
 
 template <typename T>
 cudaError_t launch_transpose(const cpx<T> *in, cpx<T> *out, long long batch, long long R, long long C,
-                             cudaStream_t s) {
+                             cudaStream_t s, long long sdist, long long ddist, const SplitTw<T> &tw) {
   if (batch <= 0 || R <= 0 || C <= 0) return cudaSuccess;
   if ((R + 31) / 32 > 65535 || batch > 65535) return cudaErrorInvalidValue;
+  if (sdist == 0) sdist = R * C;
+  if (ddist == 0) ddist = R * C;
 #ifndef FFB_HOST_EMULATION
   return launch_pdl(k_transpose<T>, dim3((unsigned)((C + 31) / 32), (unsigned)((R + 31) / 32), (unsigned)batch),
-                    dim3(32, 8), 0, s, in, out, R, C);
+                    dim3(32, 8), 0, s, in, out, R, C, sdist, ddist, tw);
 #else
   (void)s;
   for (long long b = 0; b < batch; ++b)
     for (long long r = 0; r < R; ++r)
-      for (long long c = 0; c < C; ++c) out[b * R * C + c * R + r] = in[b * R * C + r * C + c];
+      for (long long c = 0; c < C; ++c) {
+        cpx<T> v = in[b * sdist + r * C + c];
+        if (tw.lo) {
+          const uint32_t m = (uint32_t)(r * c), hi = fdiv(m, tw.split);
+          cpx<T> w = cmul(tw.hi[hi], tw.lo[m - hi * tw.split.d]);
+          if (tw.inv) w.y = -w.y;
+          v = cmul(v, w);
+        }
+        out[b * ddist + c * R + r] = v;
+      }
   return cudaSuccess;
 #endif
 }
 
-template cudaError_t launch_transpose<float>(const cpx<float> *, cpx<float> *, long long, long long, long long,
-                                             cudaStream_t);
-template cudaError_t launch_transpose<double>(const cpx<double> *, cpx<double> *, long long, long long, long long,
+template <typename T>
+cudaError_t launch_rader_step(int mode, const cpx<T> *x, cpx<T> *ws, cpx<T> *y, long long batch, long long p,
+                              long long xdist, long long ydist, const int *perm, const cpx<T> *kern,
+                              cudaStream_t s) {
+  if (batch <= 0 || p < 3) return cudaSuccess;
+  if (batch > 65535) return cudaErrorInvalidValue;
+#ifndef FFB_HOST_EMULATION
+  const unsigned blocks = (unsigned)std::min<long long>((p - 1 + 255) / 256, 4096);
+  return launch_pdl(k_rader_step<T>, dim3(blocks, (unsigned)batch), dim3(256), 0, s, mode, x, ws, y, batch, p, xdist,
+                    ydist, perm, kern);
+#else
+  (void)s;
+  for (long long b = 0; b < batch; ++b)
+    for (long long q = 0; q < p - 1; ++q) rader_step_one<T>(mode, x, ws, y, batch, p, xdist, ydist, perm, kern, b, q);
+  return cudaSuccess;
+#endif
+}
+
+template cudaError_t launch_rader_step<float>(int, const cpx<float> *, cpx<float> *, cpx<float> *, long long,
+                                              long long, long long, long long, const int *, const cpx<float> *,
                                               cudaStream_t);
+template cudaError_t launch_rader_step<double>(int, const cpx<double> *, cpx<double> *, cpx<double> *, long long,
+                                               long long, long long, long long, const int *, const cpx<double> *,
+                                               cudaStream_t);
+
+template cudaError_t launch_transpose<float>(const cpx<float> *, cpx<float> *, long long, long long, long long,
+                                             cudaStream_t, long long, long long, const SplitTw<float> &);
+template cudaError_t launch_transpose<double>(const cpx<double> *, cpx<double> *, long long, long long, long long,
+                                              cudaStream_t, long long, long long, const SplitTw<double> &);
 
 template <typename T>
 cudaError_t launch_real_post(const cpx<T> *z, cpx<T> *x, long long batch, long long zdist, long long xdist, int L,

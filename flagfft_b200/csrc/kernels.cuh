@@ -150,13 +150,41 @@ template <typename T>
 cudaError_t launch_real_convert(int mode, const void *src, void *dst, long long batch, long long sdist,
                                 long long ddist, long long n, cudaStream_t stream);
 
+// Four-step twiddle W_N^m from two split tables (m < N): W_N^m =
+// hi[m / split] * lo[m % split], conjugated for the inverse.
+template <typename T>
+struct SplitTw {
+  const cpx<T> *lo = nullptr;
+  const cpx<T> *hi = nullptr;
+  FastDiv split{};
+  bool inv = false;
+};
+
 // Batched out-of-place transpose of complex matrices: in (batch, R, C)
-// row-major -> out (batch, C, R), through 32 x 32 shared-memory tiles (both
-// sides coalesced).  Used by the lowerings that exchange axes between
-// passes (2-D transforms with an axis too long for one CTA).
+// row-major -> out (batch, C, R), matrix b of the input at b * sdist and of
+// the output at b * ddist (0: R * C), through 32 x 32 shared-memory tiles
+// (both sides coalesced); with tw.lo, element (r, c) is multiplied by
+// W_N^{r c} on the way.  Used by the lowerings that exchange axes between
+// passes (2-D transforms with an axis too long for one CTA, the plan tree's
+// four-step over a multi-pass child).
 template <typename T>
 cudaError_t launch_transpose(const cpx<T> *in, cpx<T> *out, long long batch, long long R, long long C,
-                             cudaStream_t stream);
+                             cudaStream_t stream, long long sdist = 0, long long ddist = 0,
+                             const SplitTw<T> &tw = SplitTw<T>{});
+
+// The elementwise steps of a Rader chain over a multi-pass length-m
+// (m = p - 1) transform (src/exec/raw_nodes.cpp:252-305): rows of p inputs
+// x (distance xdist), the working rows w of m elements (distance m) and,
+// after them, x_0 and A_0 per row (ws + batch * m: 2 * batch elements):
+//   mode 0 prepare:   w[q] = x[perm_in[q]], x0 saved;
+//   mode 1 pointwise: A_0 = w[0] saved; w[q] = conj(w[q] * kern[q])
+//                     (kern = FFT_m(b) / m);
+//   mode 2 finalize:  y[perm_out[q]] = x_0 + conj(w[q]); y[0] = x_0 + A_0
+//                     (rows of p outputs, distance ydist).
+template <typename T>
+cudaError_t launch_rader_step(int mode, const cpx<T> *x, cpx<T> *ws, cpx<T> *y, long long batch, long long p,
+                              long long xdist, long long ydist, const int *perm, const cpx<T> *kern,
+                              cudaStream_t stream);
 
 // Real-transform twiddles W_n^k, k <= n/2, as two short tables:
 // W_n^k = hi[k / split] * lo[k % split] (lo: split entries, hi: n/2/split + 1),

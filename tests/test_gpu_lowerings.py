@@ -80,3 +80,28 @@ def test_long_bluestein_and_nested_trees(ffb, torch_cuda, n, batch, double):
             p.execute(xd, yd, d)
             torch.cuda.synchronize()
             _bounds(O.error_stats(yd.cpu().numpy(), O.c2c(x.astype(np.complex128), d)), ftype, n)
+
+
+# The plan tree's own lowerings (FLAGFFT_TREE_LOWERING=1, read at plan time):
+# the reference's generic four-step over a multi-pass child (60022 = 2 x
+# Bluestein(30011), M = 60021 = 19 x 3159) and its Rader chain over a
+# multi-pass p - 1 transform (65537: 256 x 256; 40961: 128 x 320), in place
+# and out of place.
+@pytest.mark.parametrize("n,batch,double,marker", [(60022, 3, False, "transpose"), (65537, 2, False, "rader-gather"),
+                                                   (40961, 2, True, "rader-gather"), (65537, 1, True, "rader-gather")])
+def test_tree_lowering(ffb, torch_cuda, monkeypatch, n, batch, double, marker):
+    monkeypatch.setenv("FLAGFFT_TREE_LOWERING", "1")
+    torch = torch_cuda
+    ftype = O.Z2Z if double else O.C2C
+    x = O.random_complex(n * batch, O.accuracy_seed(ftype, n, batch, 3), double).reshape(batch, n)
+    with ffb.plan1d(n, ffb.Z2Z if double else ffb.C2C, batch) as p:
+        assert marker in p.description(), p.description()
+        for d in (ffb.FORWARD, ffb.INVERSE):
+            ref = np.stack([O.c2c(r, d) for r in x.astype(np.complex128)])
+            xd = torch.from_numpy(x).cuda()
+            yd = torch.empty_like(xd)
+            p.execute(xd, yd, d)
+            p.execute(xd, xd, d)  # in place
+            torch.cuda.synchronize()
+            _bounds(O.error_stats(yd.cpu().numpy(), ref), ftype, n)
+            np.testing.assert_array_equal(xd.cpu().numpy(), yd.cpu().numpy())

@@ -116,3 +116,19 @@ def test_server_real_lengths_without_an_on_chip_core():
     ref2 = np.stack([O.c2r(r.astype(np.complex128), n_even) for r in x2])
     assert _rel(outs[1], ref2) < _bound(n_even, False)
     assert _rel(outs[2], np.stack([O.r2c(r) for r in x3])) < _bound(n_dbl, True)
+
+
+# The plan tree's own lowerings (FLAGFFT_TREE_LOWERING=1): a four-step over a
+# multi-pass Bluestein child (60022 = 2 x 30011) and Rader chains over
+# multi-pass p - 1 transforms (65537: 256 x 256; 40961: 128 x 320).
+@pytest.mark.parametrize("n,batch,double,marker", [(60022, 2, False, "transpose"), (65537, 2, False, "rader-gather"),
+                                                   (40961, 1, True, "rader-gather")])
+def test_tree_lowering(monkeypatch, n, batch, double, marker):
+    monkeypatch.setenv("FLAGFFT_TREE_LOWERING", "1")
+    x = O.random_complex(n * batch, O.accuracy_seed(C2C, n, batch), double=True).reshape(batch, n)
+    d = _describe(lambda: H.plan1d(n, Z2Z if double else C2C, batch))
+    assert marker in d, d
+    for direction in (-1, 1):
+        got = H.c2c(x, direction, double)
+        ref = np.stack([O.c2c(r, direction) for r in x])
+        assert _rel(got, ref) < _bound(n, double), (direction, _rel(got, ref))
