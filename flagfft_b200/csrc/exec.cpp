@@ -963,8 +963,11 @@ bool lower_tree_four_step(Builder<T> &bld, Program &prog, const NodePtr &root, b
   if (src == Buf::Scratch1 || dst == Buf::Scratch1) return false;
   const int64_t n1 = root->n1, n2 = root->n2;
   // (the n2-point rows are formed in the output, so its rows are contiguous;
-  // the children's multi-pass lowerings take at most 65535 rows)
-  if (n1 * n2 != n || odist != n || batch * std::max(n1, n2) > 65535) return false;
+  // a child's multi-pass lowering takes at most 65535 rows)
+  CoreSpec c1, c2;
+  if (n1 * n2 != n || odist != n) return false;
+  if ((!bld.core_for(root->row, c1) && batch * n2 > 65535) || (!bld.core_for(root->col, c2) && batch * n1 > 65535))
+    return false;
   ensure_scratch(prog.scratch1, (size_t)(batch * n) * sizeof(cpx<T>));
   auto t1 = std::make_unique<TransposePass<T>>(src, Buf::Scratch1, batch, n1, n2);
   t1->sdist = idist;

@@ -121,7 +121,7 @@ def test_server_real_lengths_without_an_on_chip_core():
 # The plan tree's own lowerings (FLAGFFT_TREE_LOWERING=1): a four-step over a
 # multi-pass Bluestein child (60022 = 2 x 30011) and Rader chains over
 # multi-pass p - 1 transforms (65537: 256 x 256; 40961: 128 x 320).
-@pytest.mark.parametrize("n,batch,double,marker", [(60022, 2, False, "transpose"), (65537, 2, False, "rader-gather"),
+@pytest.mark.parametrize("n,batch,double,marker", [(60022, 3, False, "transpose"), (65537, 2, False, "rader-gather"),
                                                    (40961, 1, True, "rader-gather")])
 def test_tree_lowering(monkeypatch, n, batch, double, marker):
     monkeypatch.setenv("FLAGFFT_TREE_LOWERING", "1")
