@@ -171,7 +171,19 @@ template <typename T, int N1, int L2, int... Rs>
 __global__ void __launch_bounds__(Shape<N1, L2, Rs...>::NT) k_blue4(const __grid_constant__ TileArgs<T> a) {
   pdl_entry();
   extern __shared__ __align__(16) unsigned char smraw[];
-  blue4_body<T, N1, L2, rows::DevT, Rs...>(a, (long long)blockIdx.x, reinterpret_cast<cpx<T> *>(smraw), rows::DevT{});
+  for (long long by = blockIdx.x; by < a.nbatch; by += gridDim.x) {
+    const long long nx = by + gridDim.x;
+    if (threadIdx.x == 0 && nx < a.nbatch) {
+      // the next transform's input into L2 while this one computes
+      const char *row = reinterpret_cast<const char *>(reinterpret_cast<const cpx<T> *>(a.in) + nx * a.ib);
+      const uintptr_t b0 = (reinterpret_cast<uintptr_t>(row) + 15) & ~(uintptr_t)15;
+      const uintptr_t b1 = (reinterpret_cast<uintptr_t>(row) + (size_t)a.n * sizeof(cpx<T>)) & ~(uintptr_t)15;
+      if (b1 > b0)
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(b0), "r"((uint32_t)(b1 - b0)) : "memory");
+    }
+    blue4_body<T, N1, L2, rows::DevT, Rs...>(a, by, reinterpret_cast<cpx<T> *>(smraw), rows::DevT{});
+    __syncthreads();  // the next transform's first phase rewrites the rows
+  }
 }
 
 template <typename T, int N1, int L2>
@@ -186,7 +198,11 @@ cudaError_t launch(const TileArgs<T> &a, cudaStream_t s) {
     cudaError_t e = set_smem_limit_once<k_blue4<T, N1, L2, Rs...>>((int)smem_of<T, N1, L2>());
     if (e != cudaSuccess) return e;
   }
-  return launch_pdl(k_blue4<T, N1, L2, Rs...>, dim3((unsigned)a.nbatch), dim3(Shape<N1, L2, Rs...>::NT), smem_of<T, N1, L2>(), s, a);
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const long long grid = std::min<long long>(a.nbatch, sms);
+  return launch_pdl(k_blue4<T, N1, L2, Rs...>, dim3((unsigned)grid), dim3(Shape<N1, L2, Rs...>::NT), smem_of<T, N1, L2>(), s, a);
 }
 #else
 template <typename T, int N1, int L2, int... Rs>

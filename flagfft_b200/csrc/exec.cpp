@@ -1340,6 +1340,35 @@ std::unique_ptr<Program> lower_2d(const NodePtr &root, Planner &planner, bool is
                    : lower_2d_t<float>(root, planner, t, inverse, n0, n1, batch);
 }
 
+std::unique_ptr<Program> lower_batchable(const NodePtr &root, Planner &planner, bool is_double, Transform t,
+                                         bool inverse, int64_t n, const Layout &layout) {
+  struct Scope {  // the thread's lowering switches, restored on every exit
+    bool one = t_no_one_pass;
+    int pol = t_policy_override;
+    ~Scope() {
+      t_no_one_pass = one;
+      t_policy_override = pol;
+    }
+  } scope;
+  t_no_one_pass = true;
+  auto prog = lower(root, planner, is_double, t, inverse, n, layout, false);
+  bool in_place = false;
+  for (const auto &ps : prog->passes) {
+    if (is_double) {
+      auto *tp = dynamic_cast<const TilePass<double> *>(ps.get());
+      if (tp && !tp->a.pp && !tp->a.regcol) in_place = true;
+    } else {
+      auto *tp = dynamic_cast<const TilePass<float> *>(ps.get());
+      if (tp && !tp->a.pp && !tp->a.regcol) in_place = true;
+    }
+  }
+  if (in_place) {
+    t_policy_override = 2;
+    prog = lower(root, planner, is_double, t, inverse, n, layout, false);
+  }
+  return prog;
+}
+
 // ---------------------------------------------------------------------------
 // Batch programs
 // ---------------------------------------------------------------------------

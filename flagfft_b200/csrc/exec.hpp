@@ -70,6 +70,14 @@ std::unique_ptr<Program> lower(const NodePtr &root, Planner &planner, bool is_do
 std::unique_ptr<Program> lower_2d(const NodePtr &root, Planner &planner, bool is_double, Transform t, bool inverse,
                                   int64_t n0, int64_t n1, int64_t batch);
 
+// The same 1-D lowering with every tile pass in a form the persistent
+// work-queue kernel takes (no strided tile / TMA column kernels, no one-pass
+// four-step Bluestein, a multi-pass chain instead of an in-place pass), as
+// batch plans and server templates use it: their requests' passes then join
+// one launch per phase instead of launching one by one.
+std::unique_ptr<Program> lower_batchable(const NodePtr &root, Planner &planner, bool is_double, Transform t,
+                                         bool inverse, int64_t n, const Layout &layout);
+
 // Largest core length one CTA can hold.
 int64_t max_onchip_length(bool is_double);
 

@@ -183,13 +183,37 @@ class Server {
   flagfftResult prepare(flagfftType type, int64_t n, int dir) {
     try {
       std::lock_guard<std::mutex> lock(tpl_mu_);
-      return template_for(type, n, dir) ? FLAGFFT_SUCCESS : FLAGFFT_SETUP_FAILED;
+      if (!template_for(type, n, dir)) return FLAGFFT_SETUP_FAILED;
     } catch (const std::bad_alloc &) {
       return FLAGFFT_ALLOC_FAILED;
     } catch (const std::exception &e) {
       std::fprintf(stderr, "[flagfft] server prepare failed: %s\n", e.what());
       return FLAGFFT_SETUP_FAILED;
     }
+#ifndef FFB_HOST_EMULATION
+    // One transform of the template through the tick path: the first launch
+    // of each kernel it takes loads that kernel (lazy module loading), a
+    // stall of the scheduler thread of up to milliseconds that, under load,
+    // would land on the requests queued behind it.
+    int64_t ib = 0, ob = 0;
+    io_elems(type, n, &ib, &ob);
+    void *in = nullptr, *out = nullptr;
+    if (cudaMalloc(&in, (size_t)ib) != cudaSuccess || cudaMalloc(&out, (size_t)ob) != cudaSuccess) {
+      cudaGetLastError();
+      if (in) cudaFree(in);
+      return FLAGFFT_ALLOC_FAILED;
+    }
+    cudaMemsetAsync(in, 0, (size_t)ib, cudaStreamPerThread);
+    cudaStreamSynchronize(cudaStreamPerThread);
+    int64_t id = 0;
+    flagfftResult st = submit(type, n, 1, dir, in, out, &id);
+    if (st == FLAGFFT_SUCCESS) st = wait(id, nullptr);
+    cudaFree(in);
+    cudaFree(out);
+    return st;
+#else
+    return FLAGFFT_SUCCESS;
+#endif
   }
 
   flagfftResult submit(flagfftType type, int64_t n, int64_t batch, int dir, const void *in, void *out, int64_t *id) {
@@ -295,7 +319,7 @@ class Server {
     lay.idist = ib / esz_in;
     lay.odist = ob / esz_out;
     auto t = std::make_unique<Template>();
-    t->prog = lower(root, *pl->second, dbl, tr, inv, n, lay, false);
+    t->prog = lower_batchable(root, *pl->second, dbl, tr, inv, n, lay);
     if (!servable(*t->prog)) return nullptr;
     t->ws0_per = t->prog->scratch0 ? t->prog->scratch0->bytes / kTemplateBatch : 0;
     t->ws1_per = t->prog->scratch1 ? t->prog->scratch1->bytes / kTemplateBatch : 0;

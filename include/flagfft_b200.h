@@ -93,7 +93,8 @@ FLAGFFT_API int flagfftB200TuneCandidates(int n, int is_double, char *buf, int b
  * overlap on the device.  A request's result does not depend on which
  * requests share its tick.  Programs and tables of every (type, n,
  * direction) seen stay resident; Prepare builds one ahead of the first
- * request.  Wait blocks until the request finished and gives its latency
+ * request and runs one transform of it on scratch buffers it allocates, so
+ * the kernels the template takes are loaded before requests arrive.  Wait blocks until the request finished and gives its latency
  * from Submit to completion as seen by the scheduler (the caller's buffers
  * may then be reused).  Submit from any thread; a request larger than the
  * budget returns FLAGFFT_INVALID_SIZE. */

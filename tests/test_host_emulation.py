@@ -132,3 +132,19 @@ def test_tree_lowering(monkeypatch, n, batch, double, marker):
         got = H.c2c(x, direction, double)
         ref = np.stack([O.c2c(r, direction) for r in x])
         assert _rel(got, ref) < _bound(n, double), (direction, _rel(got, ref))
+
+
+def test_server_multi_pass_lengths():
+    """Server templates lower their four-step and Bluestein-chain passes in
+    the persistent kernel's form (no strided tile / TMA column kernels):
+    complex lengths above one CTA, both precisions."""
+    reqs = []
+    for code, n, b, d, seed in [(C2C, 65536, 2, -1, 21), (C2C, 131072, 1, 1, 22), (Z2Z, 20011, 1, -1, 23),
+                                (Z2Z, 32768, 2, 1, 24)]:
+        dbl = code == Z2Z
+        x = O.random_complex(n * b, seed, double=True).reshape(b, n).astype(np.complex128 if dbl else np.complex64)
+        reqs.append((code, n, b, d, x))
+    outs = _server_run(reqs)
+    for (code, n, b, d, x), y in zip(reqs, outs):
+        ref = np.stack([O.c2c(r.astype(np.complex128), d) for r in x])
+        assert _rel(y, ref) < _bound(n, code == Z2Z), (code, n, _rel(y, ref))
