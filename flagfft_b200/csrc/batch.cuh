@@ -19,7 +19,15 @@
 
 namespace ffb {
 
-enum BatchKind : int { kBatchPpDit = 0, kBatchPpBluestein = 1, kBatchPpRader = 2, kBatchPpConv = 3, kBatchRegcol = 8 };
+enum BatchKind : int {
+  kBatchPpDit = 0,
+  kBatchPpBluestein = 1,
+  kBatchPpRader = 2,
+  kBatchPpConv = 3,
+  kBatchR2C = 4,  // an on-chip Dit core with the real pack / Hermitian post on its load / store (in-place tile)
+  kBatchC2R = 5,  // the same with the Hermitian pre / unpack
+  kBatchRegcol = 8
+};
 
 struct BatchItem {
   int args;
@@ -97,7 +105,11 @@ FFB_HD void run_item(const TileArgs<T> &a, int kind, int tile, cpx<T> *sm, const
   }
   const int tiles = (a.G + a.W - 1) / a.W;
   const int by = tile / tiles, bx = tile - by * tiles;
-  if (kind == kBatchPpDit) {
+  if (kind == kBatchR2C) {
+    tile::tile_body<T, 0, (int)IoKind::R2C>(a, bx, by, sm, x);
+  } else if (kind == kBatchC2R) {
+    tile::tile_body<T, 0, (int)IoKind::C2R>(a, bx, by, sm, x);
+  } else if (kind == kBatchPpDit) {
     if (a.inv)
       tile::tile_body_pp<T, 0, true>(a, bx, by, sm, x);
     else

@@ -125,6 +125,7 @@ struct Slot {
   TickWork<float> wf;
   TickWork<double> wd;
   void *ws = nullptr;  // the tick's workspaces, one allocation carved per request
+  cudaEvent_t start = nullptr;  // ($FLAGFFT_SERVE_TRACE) the tick's first launch
 };
 
 template <typename T>
@@ -147,11 +148,14 @@ void upload_grow(DevPtr &d, size_t &cap, const void *host, size_t bytes, cudaStr
 class Server {
  public:
   Server(int64_t budget, int max_ticks) : budget_(budget), slots_(std::max(1, max_ticks)) {
+    const char *tr = std::getenv("FLAGFFT_SERVE_TRACE");
+    trace_ = tr && tr[0] == '1';
 #ifndef FFB_HOST_EMULATION
     cudaGetDevice(&device_);
     for (Slot &s : slots_) {
       cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking);
-      cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming);
+      cudaEventCreateWithFlags(&s.done, trace_ ? cudaEventDefault : cudaEventDisableTiming);
+      if (trace_) cudaEventCreate(&s.start);
     }
     // keep freed workspace in the stream-ordered pool between ticks
     cudaMemPool_t pool;
@@ -171,11 +175,18 @@ class Server {
     }
     cv_.notify_all();
     worker_.join();
+    if (trace_)
+      std::fprintf(stderr,
+                   "[flagfft] server trace: ticks %lld, requests %lld, largest tick %lld requests, host time in tick "
+                   "assembly and launch %.1f ms, device time of ticks %.1f ms\n",
+                   (long long)ticks_, (long long)completed_, (long long)max_tick_reqs_, host_launch_s_ * 1e3,
+                   device_tick_ms_);
 #ifndef FFB_HOST_EMULATION
     for (Slot &s : slots_) {
       if (s.stream) cudaStreamSynchronize(s.stream);
       if (s.stream) cudaStreamDestroy(s.stream);
       if (s.done) cudaEventDestroy(s.done);
+      if (s.start) cudaEventDestroy(s.start);
     }
 #endif
   }
@@ -366,6 +377,12 @@ class Server {
         int kind = -1;
         if (a.regcol) {
           kind = kBatchRegcol;
+        } else if (!a.pp && !a.blue_cols && !a.tiles && tp->kind == CoreKind::Dit &&
+                   (tp->io == IoKind::R2C || tp->io == IoKind::C2R)) {
+          // a real request's on-chip core: the in-place tile body with the
+          // pack / unpack, at the template's tile width
+          kind = tp->io == IoKind::R2C ? kBatchR2C : kBatchC2R;
+          if (smem + kBatchSmemHeader > 232448) kind = -1;
         } else if (a.pp && !a.blue_cols && !a.tiles && !a.rows_only && tp->io == IoKind::C2C) {
           kind = tp->kind == CoreKind::Dit         ? kBatchPpDit
                  : tp->kind == CoreKind::Bluestein ? kBatchPpBluestein
@@ -546,6 +563,13 @@ class Server {
   }
 
   void retire(Slot &s, bool ok) {
+#ifndef FFB_HOST_EMULATION
+    if (trace_ && ok && s.start) {
+      float ms = 0;
+      if (cudaEventElapsedTime(&ms, s.start, s.done) == cudaSuccess) device_tick_ms_ += ms;
+      cudaGetLastError();
+    }
+#endif
     const double t = now_s();
     for (auto &rp : s.reqs) {
       rp->t_done = t;
@@ -614,7 +638,13 @@ class Server {
 #ifndef FFB_HOST_EMULATION
           cudaSetDevice(device_);
 #endif
+          max_tick_reqs_ = std::max<int64_t>(max_tick_reqs_, (int64_t)free_slot->reqs.size());
+          const double th0 = trace_ ? now_s() : 0.0;
+#ifndef FFB_HOST_EMULATION
+          if (trace_ && free_slot->start) cudaEventRecord(free_slot->start, free_slot->stream);
+#endif
           cudaError_t e = launch_tick(*free_slot);
+          if (trace_) host_launch_s_ += now_s() - th0;
           lock.lock();
           if (e != cudaSuccess) {
             std::fprintf(stderr, "[flagfft] server tick failed: %s\n", cudaGetErrorString(e));
@@ -662,6 +692,9 @@ class Server {
   std::unordered_map<int64_t, std::shared_ptr<Request>> all_;
   int64_t next_id_ = 0, completed_ = 0, ticks_ = 0, in_use_ = 0;
   int64_t max_in_flight_ = 0, admitted_while_busy_ = 0;
+  bool trace_ = false;  // $FLAGFFT_SERVE_TRACE=1: tick timing, printed at destruction
+  int64_t max_tick_reqs_ = 0;
+  double host_launch_s_ = 0.0, device_tick_ms_ = 0.0;
   std::map<std::tuple<int, int64_t, bool>, std::unique_ptr<Template>> tpls_;
   std::map<bool, std::unique_ptr<Planner>> planners_;
 };

@@ -148,3 +148,18 @@ def test_server_multi_pass_lengths():
     for (code, n, b, d, x), y in zip(reqs, outs):
         ref = np.stack([O.c2c(r.astype(np.complex128), d) for r in x])
         assert _rel(y, ref) < _bound(n, code == Z2Z), (code, n, _rel(y, ref))
+
+
+def test_server_real_on_chip_items():
+    """Real requests whose transform fits one CTA: the persistent launch runs
+    their pack / Hermitian post (R2C) and pre / unpack (C2R) tiles."""
+    n1, n2, n3 = 4096, 1000, 998
+    x1 = O.random_real(3 * n1, 31).reshape(3, n1).astype(np.float32)
+    x2 = np.fft.rfft(O.random_real(2 * n2, 32).reshape(2, n2).astype(np.float64), axis=-1).astype(np.complex64)
+    x3 = O.random_real(4 * n3, 33, True).reshape(4, n3).astype(np.float64)
+    x4 = np.fft.rfft(O.random_real(2 * n3, 34).reshape(2, n3).astype(np.float64), axis=-1).astype(np.complex128)
+    outs = _server_run([(R2C, n1, 3, -1, x1), (C2R, n2, 2, 1, x2), (D2Z, n3, 4, -1, x3), (Z2D, n3, 2, 1, x4)])
+    assert _rel(outs[0], np.stack([O.r2c(r.astype(np.float64)) for r in x1])) < _bound(n1, False)
+    assert _rel(outs[1], np.stack([O.c2r(r.astype(np.complex128), n2) for r in x2])) < _bound(n2, False)
+    assert _rel(outs[2], np.stack([O.r2c(r) for r in x3])) < _bound(n3, True)
+    assert _rel(outs[3], np.stack([O.c2r(r, n3) for r in x4])) < _bound(n3, True)
