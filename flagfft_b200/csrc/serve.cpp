@@ -157,11 +157,19 @@ class Server {
       cudaEventCreateWithFlags(&s.done, trace_ ? cudaEventDefault : cudaEventDisableTiming);
       if (trace_) cudaEventCreate(&s.start);
     }
-    // keep freed workspace in the stream-ordered pool between ticks
+    // keep freed workspace in the stream-ordered pool between ticks, and
+    // grow the pool once now (an eighth of the budget, at most 4 GB) rather
+    // than under load, where mapping new memory stalled a tick
     cudaMemPool_t pool;
     if (cudaDeviceGetDefaultMemPool(&pool, device_) == cudaSuccess) {
       uint64_t keep = ~0ull;
       cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+      const size_t reserve = (size_t)std::min<int64_t>(budget_ / 8, (int64_t)4 << 30);
+      void *p = nullptr;
+      if (reserve && cudaMallocAsync(&p, reserve, slots_[0].stream) == cudaSuccess) {
+        cudaFreeAsync(p, slots_[0].stream);
+        cudaStreamSynchronize(slots_[0].stream);
+      }
     }
     cudaGetLastError();
 #endif
