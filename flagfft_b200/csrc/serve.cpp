@@ -97,22 +97,32 @@ struct TickWork {
   // One device buffer holds the tick's arguments, kinds, items and zeroed
   // work-queue counters (16-byte aligned sections), filled from one pinned
   // host buffer by one copy.  A slot's next tick reuses both only after the
-  // slot's previous tick finished on the device.
-  DevPtr d_all;
+  // slot's previous tick finished on the device.  They grow without any
+  // device-wide synchronisation: the device buffer is stream-ordered
+  // (cudaMallocAsync / cudaFreeAsync on the slot's stream) and outgrown
+  // pinned buffers are kept until the server ends (cudaFree and
+  // cudaFreeHost wait for the whole device: a growth under load once held
+  // the scheduler for half a second).
+  void *d_all = nullptr;
   size_t cap = 0;
   void *h_all = nullptr;
+  std::vector<void *> old_h;
   size_t off_kinds = 0, off_items = 0, off_counters = 0;
-  const TileArgs<T> *dev_args() const { return reinterpret_cast<const TileArgs<T> *>(d_all->ptr); }
-  const int *dev_kinds() const { return reinterpret_cast<const int *>(static_cast<char *>(d_all->ptr) + off_kinds); }
+  const TileArgs<T> *dev_args() const { return reinterpret_cast<const TileArgs<T> *>(d_all); }
+  const int *dev_kinds() const { return reinterpret_cast<const int *>(static_cast<char *>(d_all) + off_kinds); }
   const BatchItem *dev_items() const {
-    return reinterpret_cast<const BatchItem *>(static_cast<char *>(d_all->ptr) + off_items);
+    return reinterpret_cast<const BatchItem *>(static_cast<char *>(d_all) + off_items);
   }
-  int *dev_counters() const { return reinterpret_cast<int *>(static_cast<char *>(d_all->ptr) + off_counters); }
-  ~TickWork() {
+  int *dev_counters() const { return reinterpret_cast<int *>(static_cast<char *>(d_all) + off_counters); }
+  ~TickWork() {  // (the server synchronised the slot's stream before)
+    old_h.push_back(h_all);
 #ifndef FFB_HOST_EMULATION
-    if (h_all) cudaFreeHost(h_all);
+    if (d_all) cudaFree(d_all);
+    for (void *h : old_h)
+      if (h) cudaFreeHost(h);
 #else
-    std::free(h_all);
+    std::free(d_all);
+    for (void *h : old_h) std::free(h);
 #endif
   }
 };
@@ -186,9 +196,11 @@ class Server {
     if (trace_)
       std::fprintf(stderr,
                    "[flagfft] server trace: ticks %lld, requests %lld, largest tick %lld requests, host time in tick "
-                   "assembly and launch %.1f ms, device time of ticks %.1f ms\n",
+                   "assembly and launch %.1f ms (longest %.2f ms, %lld requests), device time of ticks %.1f ms "
+                   "(longest %.2f ms), longest scheduler pass with ticks in flight %.2f ms\n",
                    (long long)ticks_, (long long)completed_, (long long)max_tick_reqs_, host_launch_s_ * 1e3,
-                   device_tick_ms_);
+                   max_host_tick_s_ * 1e3, (long long)max_host_tick_reqs_, device_tick_ms_, max_device_tick_ms_,
+                   max_loop_gap_s_ * 1e3);
 #ifndef FFB_HOST_EMULATION
     for (Slot &s : slots_) {
       if (s.stream) cudaStreamSynchronize(s.stream);
@@ -523,15 +535,21 @@ class Server {
       w.off_counters = w.off_items + al(w.items.size() * sizeof(BatchItem));
       const size_t total = w.off_counters + nc * sizeof(int);
       if (!w.d_all || w.cap < total) {
-        w.cap = std::max(total, 2 * w.cap);
-        w.d_all = std::make_shared<DevMem>(w.cap);
+        const size_t ncap = std::max({total, 2 * w.cap, (size_t)1 << 20});
+        void *nd = nullptr, *nh = nullptr;
 #ifndef FFB_HOST_EMULATION
-        if (w.h_all) cudaFreeHost(w.h_all);
-        if (cudaMallocHost(&w.h_all, w.cap) != cudaSuccess) w.h_all = nullptr;
+        if (cudaMallocAsync(&nd, ncap, s.stream) != cudaSuccess) return false;
+        if (w.d_all) cudaFreeAsync(w.d_all, s.stream);
+        if (cudaMallocHost(&nh, ncap) != cudaSuccess) nh = nullptr;
 #else
-        std::free(w.h_all);
-        w.h_all = std::malloc(w.cap);
+        nd = std::malloc(ncap);
+        std::free(w.d_all);
+        nh = std::malloc(ncap);
 #endif
+        w.d_all = nd;
+        w.old_h.push_back(w.h_all);
+        w.h_all = nh;
+        w.cap = ncap;
       }
       char *h = static_cast<char *>(w.h_all);
       if (h == nullptr) return false;
@@ -540,9 +558,9 @@ class Server {
       std::memcpy(h + w.off_items, w.items.data(), w.items.size() * sizeof(BatchItem));
       std::memset(h + w.off_counters, 0, nc * sizeof(int));  // every work-queue counter starts at zero
 #ifndef FFB_HOST_EMULATION
-      return cudaMemcpyAsync(w.d_all->ptr, h, total, cudaMemcpyHostToDevice, s.stream) == cudaSuccess;
+      return cudaMemcpyAsync(w.d_all, h, total, cudaMemcpyHostToDevice, s.stream) == cudaSuccess;
 #else
-      std::memcpy(w.d_all->ptr, h, total);
+      std::memcpy(w.d_all, h, total);
       return true;
 #endif
     };
@@ -574,7 +592,10 @@ class Server {
 #ifndef FFB_HOST_EMULATION
     if (trace_ && ok && s.start) {
       float ms = 0;
-      if (cudaEventElapsedTime(&ms, s.start, s.done) == cudaSuccess) device_tick_ms_ += ms;
+      if (cudaEventElapsedTime(&ms, s.start, s.done) == cudaSuccess) {
+        device_tick_ms_ += ms;
+        max_device_tick_ms_ = std::max(max_device_tick_ms_, (double)ms);
+      }
       cudaGetLastError();
     }
 #endif
@@ -594,7 +615,15 @@ class Server {
     PdlOff no_pdl;  // this thread feeds several streams at once
 #endif
     std::unique_lock<std::mutex> lock(mu_);
+    double t_iter = now_s();
     while (true) {
+      if (trace_) {  // the longest stretch between two passes of the loop while ticks were in flight
+        const double t = now_s();
+        bool any = false;
+        for (Slot &s : slots_) any = any || s.busy;
+        if (any) max_loop_gap_s_ = std::max(max_loop_gap_s_, t - t_iter);
+        t_iter = t;
+      }
       bool progressed = false;
       // retire finished ticks
       for (Slot &s : slots_) {
@@ -652,7 +681,14 @@ class Server {
           if (trace_ && free_slot->start) cudaEventRecord(free_slot->start, free_slot->stream);
 #endif
           cudaError_t e = launch_tick(*free_slot);
-          if (trace_) host_launch_s_ += now_s() - th0;
+          if (trace_) {
+            const double dt = now_s() - th0;
+            host_launch_s_ += dt;
+            if (dt > max_host_tick_s_) {
+              max_host_tick_s_ = dt;
+              max_host_tick_reqs_ = (int64_t)free_slot->reqs.size();
+            }
+          }
           lock.lock();
           if (e != cudaSuccess) {
             std::fprintf(stderr, "[flagfft] server tick failed: %s\n", cudaGetErrorString(e));
@@ -702,7 +738,9 @@ class Server {
   int64_t max_in_flight_ = 0, admitted_while_busy_ = 0;
   bool trace_ = false;  // $FLAGFFT_SERVE_TRACE=1: tick timing, printed at destruction
   int64_t max_tick_reqs_ = 0;
-  double host_launch_s_ = 0.0, device_tick_ms_ = 0.0;
+  double host_launch_s_ = 0.0, device_tick_ms_ = 0.0, max_host_tick_s_ = 0.0, max_device_tick_ms_ = 0.0;
+  int64_t max_host_tick_reqs_ = 0;
+  double max_loop_gap_s_ = 0.0;
   std::map<std::tuple<int, int64_t, bool>, std::unique_ptr<Template>> tpls_;
   std::map<bool, std::unique_ptr<Planner>> planners_;
 };
