@@ -114,6 +114,27 @@ struct TickWork {
     return reinterpret_cast<const BatchItem *>(static_cast<char *>(d_all) + off_items);
   }
   int *dev_counters() const { return reinterpret_cast<int *>(static_cast<char *>(d_all) + off_counters); }
+  // Room for `bytes` of arguments, kinds, items and counters; outgrown
+  // buffers are released as the class comment says.
+  bool reserve(size_t bytes, cudaStream_t st) {
+    if (d_all && cap >= bytes) return true;
+    void *nd = nullptr, *nh = nullptr;
+#ifndef FFB_HOST_EMULATION
+    if (cudaMallocAsync(&nd, bytes, st) != cudaSuccess) return false;
+    if (d_all) cudaFreeAsync(d_all, st);
+    if (cudaMallocHost(&nh, bytes) != cudaSuccess) nh = nullptr;
+#else
+    (void)st;
+    nd = std::malloc(bytes);
+    std::free(d_all);
+    nh = std::malloc(bytes);
+#endif
+    d_all = nd;
+    old_h.push_back(h_all);
+    h_all = nh;
+    cap = bytes;
+    return nh != nullptr;
+  }
   ~TickWork() {  // (the server synchronised the slot's stream before)
     old_h.push_back(h_all);
 #ifndef FFB_HOST_EMULATION
@@ -164,6 +185,10 @@ class Server {
     cudaGetDevice(&device_);
     for (Slot &s : slots_) {
       cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking);
+      // tick buffers for large ticks up front: growing pinned memory under
+      // load (page-locking megabytes) held the scheduler for a fifth of a second
+      s.wf.reserve(kTickBufferBytes, s.stream);
+      s.wd.reserve(kTickBufferBytes, s.stream);
       cudaEventCreateWithFlags(&s.done, trace_ ? cudaEventDefault : cudaEventDisableTiming);
       if (trace_) cudaEventCreate(&s.start);
     }
@@ -534,23 +559,8 @@ class Server {
       w.off_items = w.off_kinds + al(w.kinds.size() * sizeof(int));
       w.off_counters = w.off_items + al(w.items.size() * sizeof(BatchItem));
       const size_t total = w.off_counters + nc * sizeof(int);
-      if (!w.d_all || w.cap < total) {
-        const size_t ncap = std::max({total, 2 * w.cap, (size_t)1 << 20});
-        void *nd = nullptr, *nh = nullptr;
-#ifndef FFB_HOST_EMULATION
-        if (cudaMallocAsync(&nd, ncap, s.stream) != cudaSuccess) return false;
-        if (w.d_all) cudaFreeAsync(w.d_all, s.stream);
-        if (cudaMallocHost(&nh, ncap) != cudaSuccess) nh = nullptr;
-#else
-        nd = std::malloc(ncap);
-        std::free(w.d_all);
-        nh = std::malloc(ncap);
-#endif
-        w.d_all = nd;
-        w.old_h.push_back(w.h_all);
-        w.h_all = nh;
-        w.cap = ncap;
-      }
+      if ((!w.d_all || w.cap < total) && !w.reserve(std::max({total, 2 * w.cap, (size_t)1 << 20}), s.stream))
+        return false;
       char *h = static_cast<char *>(w.h_all);
       if (h == nullptr) return false;
       std::memcpy(h, w.args.data(), b_args);
@@ -721,6 +731,7 @@ class Server {
   }
 
   static constexpr size_t kMaxPerTick = 4096;
+  static constexpr size_t kTickBufferBytes = 16u << 20;  // per slot and precision, reserved at creation
   static constexpr int64_t kTemplateBatch = 2;  // transforms a template program is lowered for
   static constexpr size_t kCoalesceMin = 32;
   static constexpr double kCoalesceWait = 100e-6;  // seconds
