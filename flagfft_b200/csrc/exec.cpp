@@ -594,12 +594,16 @@ class Builder {
     const size_t per = rows_only ? rows_per
                        : a.pp    ? pp_per
                                  : tile_smem_per_transform<T>((int)L) + Swz<T>::G * sizeof(cpx<T>);
-    // Transforms per CTA: about 256 threads' worth, within a shared-memory
+    // Transforms per CTA: about 128 threads' worth, within a shared-memory
     // budget that leaves room for a second CTA per SM, and no more than keeps
     // ~2 CTAs per SM busy; column tiles take at least 8 transforms so each
-    // row segment they read is 64-128 bytes.
+    // row segment they read is 64-128 bytes.  (Against 256 threads' worth,
+    // measured in one process on B200: C2C 256 x 262144 189 -> 168 us,
+    // 1024 x 65536 175 -> 163, 1009 x 16384 179 -> 166, 256 x 16384 15.5 ->
+    // 13.5, Z2Z 1024 x 32768 178 -> 164; no call slower; 512 threads' worth
+    // was slower everywhere.)
     const size_t budget = std::max<size_t>(per, 110 * 1024);
-    const int64_t w_thr = std::max<int64_t>(1, 256 / tpt);
+    const int64_t w_thr = std::max<int64_t>(1, 128 / tpt);
     const int64_t w_smem = std::max<int64_t>(1, (int64_t)(std::min(budget, limit) / per));
     const int64_t w_par = std::max<int64_t>(1, (nbatch * G) / (2 * kSMs));
     int64_t W = std::min<int64_t>({w_thr, w_smem, w_par, G});
