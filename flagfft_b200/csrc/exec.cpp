@@ -273,6 +273,18 @@ static bool tma_columns_enabled() {
 // passes join the persistent launches.
 thread_local bool t_no_one_pass = false;
 
+// One-pass Bluestein in the pair form ($FLAGFFT_BLUESTEIN_PAIR=1, read at
+// plan time): the N1 convolution rows split over a two-CTA cluster, in both
+// precisions, instead of one CTA (single precision) or the three-pass chain
+// (double precision).  Off by default: on B200 it measured slower at the
+// benchmark lengths (C2C 10007 x 1024: 208.8 us against 176.7 us for one CTA;
+// Z2Z 10007 x 256: 123.2 us against 102 us for three passes) -- a pair CTA
+// runs 12 warps, and its row phase is no more efficient than the chain's.
+bool bluestein_pair() {
+  const char *v = std::getenv("FLAGFFT_BLUESTEIN_PAIR");
+  return v && v[0] == '1';
+}
+
 // The compile-time radix sequence of length L (FFB_FIXED_SEQUENCES), if it
 // has one: such a length runs on a row kernel with every index constant.
 bool fixed_sequence(int64_t L, std::vector<int> *r) {
@@ -313,9 +325,11 @@ int64_t choose_conv_length(int64_t n, int64_t maxL, std::vector<int> *radices) {
 // Four-step convolution M = n1 * n2: n1 one codelet (the column passes), n2
 // on chip (the convolution rows).  Minimises M x chain cost of n2 (the column
 // passes cost about the same for every n1), weighted for compile-time row
-// sequences and, when `one_pass`, for the shapes the one-pass kernel runs.
+// sequences and for the shapes `one_pass` (the one-pass kernel's shape test,
+// or null) accepts.
 constexpr double kOnePassWeight = 0.35;
-int64_t choose_split_conv(int64_t n, int64_t maxL, bool one_pass, int64_t *n1_out, std::vector<int> *row_radices) {
+int64_t choose_split_conv(int64_t n, int64_t maxL, bool (*one_pass)(int, int), int64_t *n1_out,
+                          std::vector<int> *row_radices) {
   std::unordered_map<int64_t, std::pair<double, int>> memo;
   static const int kCols[] = {16, 15, 13, 12, 11, 10, 9, 8};
   int64_t best_m = 0, best_n1 = 0;
@@ -326,7 +340,7 @@ int64_t choose_split_conv(int64_t n, int64_t maxL, bool one_pass, int64_t *n1_ou
       if (m % n1 || m / n1 > maxL) continue;
       const bool fixed = fixed_sequence(m / n1, nullptr);
       const double c = (double)m * chain_cost(m / n1, nullptr, memo) *
-                       (one_pass && fixed && blue4_shape(n1, (int)(m / n1)) ? kOnePassWeight
+                       (one_pass && fixed && one_pass(n1, (int)(m / n1)) ? kOnePassWeight
                                                                              : fixed ? kFixedWeight : 1.0);
       if (c < best) {
         best = c;
@@ -1081,18 +1095,24 @@ void lower_c2c(Builder<T> &bld, Program &prog, const NodePtr &root, bool inverse
     // fused (src/exec/raw_nodes.cpp:153-204 runs the same chain as 7 launches).
     int64_t n1 = 0;
     std::vector<int> row_radices;
-    const bool one_pass_ok = sizeof(T) == 4 && !t_no_one_pass;
-    const int64_t M = choose_split_conv(n, max_onchip_length(sizeof(T) == 8), one_pass_ok, &n1, &row_radices);
+    // the one-pass forms: single precision holds the N1 rows in one CTA;
+    // the pair form (both precisions) splits them over a two-CTA cluster
+    const bool pair = bluestein_pair();
+    bool (*const one_pass)(int, int) = t_no_one_pass ? nullptr
+                                       : pair        ? blue4_pair_shape
+                                       : sizeof(T) == 4 ? blue4_shape
+                                                        : nullptr;
+    const int64_t M = choose_split_conv(n, max_onchip_length(sizeof(T) == 8), one_pass, &n1, &row_radices);
     std::vector<int> seq;
-    if (M && one_pass_ok && blue4_shape((int)n1, (int)(M / n1)) && fixed_sequence(M / n1, &seq) &&
-        seq == row_radices) {
-      // the whole chain in one CTA per transform: n1 rows of n2 points in
-      // shared memory (blue4.cuh)
+    if (M && one_pass && one_pass((int)n1, (int)(M / n1)) && fixed_sequence(M / n1, &seq) && seq == row_radices) {
+      // the whole chain in one CTA (or CTA pair) per transform: n1 rows of
+      // n2 points in shared memory (blue4.cuh)
       const int64_t n2 = M / n1;
       CoreSpec sc{CoreKind::Conv, n2, n2, row_radices, nullptr};
       auto *p = bld.add_pass(sc, IoKind::C2C, true, batch, 1, idist, 0, 1, odist, 0, 1, src, dst, n);
       TileArgs<T> &a = p->a;
       a.blue_cols = (int)n1;
+      a.blue_pair = pair ? 1 : 0;
       a.G = 1;
       a.W = 1;
       a.n = (int)n;
@@ -1100,8 +1120,9 @@ void lower_c2c(Builder<T> &bld, Program &prog, const NodePtr &root, bool inverse
       a.kern = bld.table_bluestein_rows(n, row_radices, n1, n2, inverse, true);
       a.kern_stride = n2;
       bld.set_post_twiddle(a, M);
-      p->smem = blue4_smem((int)n1, (int)n2, sizeof(cpx<T>));
-      p->note = "bluestein one pass: " + std::to_string(n1) + " x " + std::to_string(n2) + " four-step in one CTA";
+      p->smem = blue4_smem((int)n1, (int)n2, sizeof(cpx<T>), pair);
+      p->note = "bluestein one pass: " + std::to_string(n1) + " x " + std::to_string(n2) +
+                (pair ? " four-step in a two-CTA cluster" : " four-step in one CTA");
       return;
     }
     if (M) {

@@ -71,13 +71,13 @@ struct TilePass final : PassBase {
 
   std::string describe() const override {
     std::ostringstream o;
-    o << (a.regcol ? "register-columns" : a.blue_cols ? "bluestein-four-step" : kind_name(kind)) << "/" << io_name(io)
+    o << (a.regcol ? "register-columns" : a.blue_pair ? "bluestein-four-step-pair" : a.blue_cols ? "bluestein-four-step" : kind_name(kind)) << "/" << io_name(io)
       << " "
       << (sizeof(T) == 4 ? "f32" : "f64") << " L=" << a.core.L
       << " radices=[";
     for (int s = 0; s < a.core.nst; ++s) o << (s ? "," : "") << a.core.radix[s];
     o << "] n=" << a.n << " transforms=" << a.nbatch << "x" << a.G << " per_cta=" << a.W
-      << " threads=" << (a.blue_cols ? blue4_threads(a.blue_cols, a.core.L) : a.tiles ? a.tpt : a.W * a.tpt)
+      << " threads=" << (a.blue_cols ? blue4_threads(a.blue_cols, a.core.L, a.blue_pair != 0) : a.tiles ? a.tpt : a.W * a.tpt)
       << (a.tiles ? " tiles" : "") << " smem=" << tile_smem<T>(a, kind, io, smem) << " " << buf_name(src) << "->"
       << buf_name(dst);
     if (a.tcols) o << " tma-columns(threads=" << a.tc_threads << " smem=" << a.tc_smem << ")";

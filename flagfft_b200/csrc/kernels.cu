@@ -414,7 +414,7 @@ template <typename T>
 size_t tile_smem(const TileArgs<T> &a, CoreKind kind, IoKind io, size_t smem) {
   const int k = (int)kind;
   if (a.regcol) return 0;
-  if (a.blue_cols) return blue4_smem(a.blue_cols, a.core.L, sizeof(cpx<T>));
+  if (a.blue_cols) return blue4_smem(a.blue_cols, a.core.L, sizeof(cpx<T>), a.blue_pair != 0);
   if (a.tiles) return smem;
   if (a.pp && io == IoKind::C2C && (k == 0 || k == 1 || k == 3)) {
     const size_t r = k == 0 ? rows::rows_smem_any<T, 0>(a) : k == 1 ? rows::rows_smem_any<T, 1>(a)

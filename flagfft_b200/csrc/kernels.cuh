@@ -56,6 +56,18 @@ enum class IoKind : int {
   X(12, 2048, 16, 16, 8) X(13, 2048, 16, 16, 8) X(13, 1024, 16, 16, 4) X(15, 1024, 16, 16, 4)            \
   X(16, 1024, 16, 16, 4)
 
+// Shapes of the pair form (blue4.cuh k_blue4_pair): N1 even, N1 / 2 padded
+// rows per CTA (double precision: 139-209 KB).
+#define FFB_BLUE4_PAIR_SHAPES(X) X(8, 2048, 16, 16, 8) X(10, 2048, 16, 16, 8) X(12, 2048, 16, 16, 8)
+
+inline bool blue4_pair_shape(int n1, int L2) {
+#define FFB_B4P_HAS(N1, L2_, ...) \
+  if (n1 == (N1) && L2 == (L2_)) return true;
+  FFB_BLUE4_PAIR_SHAPES(FFB_B4P_HAS)
+#undef FFB_B4P_HAS
+  return false;
+}
+
 inline bool blue4_shape(int n1, int L2) {
 #define FFB_B4_HAS(N1, L2_, ...) \
   if (n1 == (N1) && L2 == (L2_)) return true;
@@ -110,8 +122,10 @@ struct TileArgs {
   // C2C, transforms contiguous in memory on both sides: ig == og == 1).
   int regcol;
   // > 0: one-pass four-step Bluestein (blue4.cuh) with this many columns
-  // (rows of the core's sequence); one CTA per transform.
+  // (rows of the core's sequence); one CTA per transform, or with blue_pair
+  // a cluster of two CTAs holding half of the rows each.
   int blue_cols;
+  int blue_pair;
   // 1: strided tile kernel of a compile-time sequence (tiles.cuh): W is its
   // fixed tile width, one shared buffer per transform.
   int tiles;
@@ -238,13 +252,13 @@ bool tcols_eligible(int L, long long nbatch, long long G, long long ib, long lon
 template <typename T>
 long long tcols_wait_failures();
 
-// One-pass four-step Bluestein (TileArgs::blue_cols); defined in
-// k_f32_blue4.cu (single precision only).
+// One-pass four-step Bluestein (TileArgs::blue_cols, blue_pair); defined in
+// k_f32_blue4.cu and k_f64_blue4.cu.
 template <typename T>
 cudaError_t launch_blue4(const TileArgs<T> &a, cudaStream_t stream);
-// Its dynamic shared memory and threads per CTA.
-size_t blue4_smem(int n1, int L2, size_t elem_bytes);
-int blue4_threads(int n1, int L2);
+// Its dynamic shared memory and threads per CTA (pair: per CTA of the pair).
+size_t blue4_smem(int n1, int L2, size_t elem_bytes, bool pair);
+int blue4_threads(int n1, int L2, bool pair);
 
 // Register column pass (TileArgs::regcol); defined in regcol.cu.
 template <typename T>

@@ -82,6 +82,28 @@ def test_long_bluestein_and_nested_trees(ffb, torch_cuda, n, batch, double):
             _bounds(O.error_stats(yd.cpu().numpy(), O.c2c(x.astype(np.complex128), d)), ftype, n)
 
 
+# The one-pass Bluestein in its pair form ($FLAGFFT_BLUESTEIN_PAIR=1, read at
+# plan time): the N1 x 2048 convolution rows split over a two-CTA cluster
+# exchanging through distributed shared memory, N1 = 8 (8009), 10 (10007,
+# 8501) and 12 (11003); batch 300 is more transforms than pairs resident at
+# once, so pairs walk several transforms.
+@pytest.mark.parametrize("n,batch,double", [(8009, 3, True), (10007, 300, True), (8501, 2, True),
+                                            (11003, 5, True), (10007, 300, False), (11003, 5, False)])
+def test_bluestein_pair(ffb, torch_cuda, monkeypatch, n, batch, double):
+    torch = torch_cuda
+    monkeypatch.setenv("FLAGFFT_BLUESTEIN_PAIR", "1")
+    ftype = O.Z2Z if double else O.C2C
+    x = O.random_complex(n * batch, O.accuracy_seed(ftype, n, batch), double).reshape(batch, n)
+    with ffb.plan1d(n, ffb.Z2Z if double else ffb.C2C, batch) as p:
+        assert "bluestein-four-step-pair" in p.description()
+        for d in (ffb.FORWARD, ffb.INVERSE):
+            xd = torch.from_numpy(x).cuda()
+            yd = torch.empty_like(xd)
+            p.execute(xd, yd, d)
+            torch.cuda.synchronize()
+            _bounds(O.error_stats(yd.cpu().numpy(), O.c2c(x.astype(np.complex128), d)), ftype, n)
+
+
 # The plan tree's own lowerings (FLAGFFT_TREE_LOWERING=1, read at plan time):
 # the reference's generic four-step over a multi-pass child (60022 = 2 x
 # Bluestein(30011), M = 60021 = 19 x 3159) and its Rader chain over a

@@ -134,6 +134,21 @@ def test_tree_lowering(monkeypatch, n, batch, double, marker):
         assert _rel(got, ref) < _bound(n, double), (direction, _rel(got, ref))
 
 
+# The one-pass Bluestein's pair form (FLAGFFT_BLUESTEIN_PAIR=1): the two
+# CTAs of the cluster emulated phase by phase, each writing half of its
+# columns' rows into the other's buffer; N1 = 8, 10 and 12 rows of 2048.
+@pytest.mark.parametrize("n,batch,double", [(8009, 2, True), (10007, 2, True), (11003, 1, True), (10007, 2, False)])
+def test_bluestein_pair(monkeypatch, n, batch, double):
+    monkeypatch.setenv("FLAGFFT_BLUESTEIN_PAIR", "1")
+    x = O.random_complex(n * batch, O.accuracy_seed(C2C, n, batch), double=True).reshape(batch, n)
+    d = _describe(lambda: H.plan1d(n, Z2Z if double else C2C, batch))
+    assert "bluestein-four-step-pair" in d, d
+    for direction in (-1, 1):
+        got = H.c2c(x, direction, double)
+        ref = np.stack([O.c2c(r, direction) for r in x])
+        assert _rel(got, ref) < _bound(n, double), (direction, _rel(got, ref))
+
+
 def test_server_multi_pass_lengths():
     """Server templates lower their four-step and Bluestein-chain passes in
     the persistent kernel's form (no strided tile / TMA column kernels):
