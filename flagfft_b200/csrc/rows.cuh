@@ -76,6 +76,25 @@ FFB_HD constexpr int rows_tpt() {
                                                                            : tile::TileBounds<T>::kMaxThreads;
 }
 
+// The wide form of a sequence with a radix that is not a power of two: one
+// butterfly of its smallest radix of at least 5 per thread, so that no such
+// stage takes a second round (1701 = 9 9 7 3: 243 -> 256 threads instead of
+// 189 -> 192, whose radix-7 stage runs two rounds).  Equal to rows_tpt for
+// powers of two.  The executor takes it for small batches (exec.cpp
+// wide_tpt).
+template <int... Rs>
+FFB_HD constexpr int thread_radix() {
+  constexpr bool pow2 = (((Rs & (Rs - 1)) == 0) && ...);
+  int m = Seq<Rs...>::rmax();
+  if (!pow2) ((Rs >= 5 && Rs < m ? (void)(m = Rs) : (void)0), ...);
+  return m;
+}
+template <typename T, int L, int... Rs>
+FFB_HD constexpr int rows_tpt_wide() {
+  return tpt_of(L, thread_radix<Rs...>()) < tile::TileBounds<T>::kMaxThreads ? tpt_of(L, thread_radix<Rs...>())
+                                                                             : tile::TileBounds<T>::kMaxThreads;
+}
+
 // Thread policy: DevT runs a phase's body once as this CUDA thread; HostT
 // (host emulation of the index arithmetic) runs it for every thread in turn.
 struct DevT {
@@ -509,21 +528,19 @@ FFB_HD void rows_body(const TileArgs<T> &a, long long bx, long long by, cpx<T> *
   }
 }
 
-template <typename T, int KIND, bool INV, int MB, int L, int... Rs>
+template <typename T, int KIND, bool INV, int MB, int L, int TPT, int... Rs>
 __global__ void __launch_bounds__(tile::TileBounds<T>::kMaxThreads, MB) k_rows(const __grid_constant__ TileArgs<T> a) {
   pdl_entry();
   extern __shared__ __align__(16) unsigned char smraw[];
-  constexpr int TPT = rows_tpt<T, L, Rs...>();
   rows_body<T, KIND, INV, L, TPT, DevT, Rs...>(a, (long long)blockIdx.x, (long long)blockIdx.y,
                                                reinterpret_cast<cpx<T> *>(smraw), DevT{});
 }
 
-// True when the pass can run as rows of this sequence: contiguous rows on
-// both sides, the executor's threads per transform, and (convolutions) the
-// same sequence for the inverse core.
-template <typename T, int KIND, int L, int... Rs>
+// True when the pass can run as rows of this sequence with TPT threads a
+// row: contiguous rows on both sides, the executor's threads per transform,
+// and (convolutions) the same sequence for the inverse core.
+template <typename T, int KIND, int L, int TPT, int... Rs>
 FFB_HD bool rows_fit(const TileArgs<T> &a) {
-  constexpr int TPT = rows_tpt<T, L, Rs...>();
   return a.pp && !a.wfast && a.ii == 1 && a.ok == 1 && a.tpt == TPT &&
          a.W * TPT <= tile::TileBounds<T>::kMaxThreads && tile::core_is<L, Rs...>(a.core) &&
          (KIND == 0 || tile::core_is<L, Rs...>(a.core2));
@@ -536,16 +553,15 @@ size_t rows_smem(const TileArgs<T> &a) {
 }
 
 #ifndef FFB_HOST_EMULATION
-template <typename T, int KIND, bool INV, int MB, int L, int... Rs>
+template <typename T, int KIND, bool INV, int MB, int L, int TPT, int... Rs>
 cudaError_t launch_rows_mb(const TileArgs<T> &a, cudaStream_t s) {
   {
-    cudaError_t e = set_smem_limit_once<k_rows<T, KIND, INV, MB, L, Rs...>>(232448);
+    cudaError_t e = set_smem_limit_once<k_rows<T, KIND, INV, MB, L, TPT, Rs...>>(232448);
     if (e != cudaSuccess) return e;
   }
-  constexpr int TPT = rows_tpt<T, L, Rs...>();
   dim3 grid((unsigned)((a.G + a.W - 1) / a.W), (unsigned)a.nbatch, 1);
   dim3 block((unsigned)(a.W * TPT), 1, 1);
-  return launch_pdl(k_rows<T, KIND, INV, MB, L, Rs...>, grid, block, rows_smem<T, L>(a), s, a);
+  return launch_pdl(k_rows<T, KIND, INV, MB, L, TPT, Rs...>, grid, block, rows_smem<T, L>(a), s, a);
 }
 // Double-precision transforms of up to 4096 points are compiled for two
 // CTAs per SM (at most 128 registers, no spills): without the bound the
@@ -556,14 +572,13 @@ template <typename T, int KIND, int L>
 constexpr int rows_min_blocks() {
   return sizeof(T) == 8 && KIND == 0 && L <= 4096 ? 2 : 1;
 }
-template <typename T, int KIND, bool INV, int L, int... Rs>
+template <typename T, int KIND, bool INV, int L, int TPT, int... Rs>
 cudaError_t launch_rows(const TileArgs<T> &a, cudaStream_t s) {
-  return launch_rows_mb<T, KIND, INV, rows_min_blocks<T, KIND, L>(), L, Rs...>(a, s);
+  return launch_rows_mb<T, KIND, INV, rows_min_blocks<T, KIND, L>(), L, TPT, Rs...>(a, s);
 }
 #else
-template <typename T, int KIND, bool INV, int L, int... Rs>
+template <typename T, int KIND, bool INV, int L, int TPT, int... Rs>
 cudaError_t launch_rows(const TileArgs<T> &a, cudaStream_t) {
-  constexpr int TPT = rows_tpt<T, L, Rs...>();
   std::vector<unsigned char> buf(rows_smem<T, L>(a) + 64);
   cpx<T> *sm = reinterpret_cast<cpx<T> *>(buf.data());
   const long long tiles = (a.G + a.W - 1) / a.W;
@@ -580,8 +595,10 @@ cudaError_t launch_rows(const TileArgs<T> &a, cudaStream_t) {
 // not rows of a compile-time sequence.
 template <typename T, int KIND>
 size_t rows_smem_any(const TileArgs<T> &a) {
-#define FFB_ROWS_SMEM(L, ...) \
-  if (rows_fit<T, KIND, L, __VA_ARGS__>(a)) return rows_smem<T, L>(a);
+#define FFB_ROWS_SMEM(L, ...)                                                                 \
+  if (rows_fit<T, KIND, L, rows_tpt<T, L, __VA_ARGS__>(), __VA_ARGS__>(a) ||                 \
+      rows_fit<T, KIND, L, rows_tpt_wide<T, L, __VA_ARGS__>(), __VA_ARGS__>(a))              \
+    return rows_smem<T, L>(a);
   FFB_FIXED_SEQUENCES(FFB_ROWS_SMEM)
 #undef FFB_ROWS_SMEM
   return 0;
@@ -591,8 +608,13 @@ size_t rows_smem_any(const TileArgs<T> &a) {
 // the pass is not rows of a compile-time sequence.
 template <typename T, int KIND, bool INV>
 cudaError_t launch_rows_any(const TileArgs<T> &a, size_t, cudaStream_t s) {
-#define FFB_TRY_ROWS(L, ...) \
-  if (rows_fit<T, KIND, L, __VA_ARGS__>(a)) return launch_rows<T, KIND, INV, L, __VA_ARGS__>(a, s);
+#define FFB_TRY_ROWS(L, ...)                                                                              \
+  if (rows_fit<T, KIND, L, rows_tpt<T, L, __VA_ARGS__>(), __VA_ARGS__>(a))                                \
+    return launch_rows<T, KIND, INV, L, rows_tpt<T, L, __VA_ARGS__>(), __VA_ARGS__>(a, s);                \
+  if constexpr (rows_tpt_wide<T, L, __VA_ARGS__>() != rows_tpt<T, L, __VA_ARGS__>()) {                    \
+    if (rows_fit<T, KIND, L, rows_tpt_wide<T, L, __VA_ARGS__>(), __VA_ARGS__>(a))                         \
+      return launch_rows<T, KIND, INV, L, rows_tpt_wide<T, L, __VA_ARGS__>(), __VA_ARGS__>(a, s);         \
+  }
   FFB_FIXED_SEQUENCES(FFB_TRY_ROWS)
 #undef FFB_TRY_ROWS
   return cudaErrorNotSupported;

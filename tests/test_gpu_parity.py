@@ -251,3 +251,19 @@ def test_lowering_policies(ffb, torch_cuda, plans, monkeypatch, policy, double, 
     for direction in (-1, 1):
         got = _run_c2c(ffb, torch_cuda, x, direction, double)
         _check(O.error_stats(got, O.c2c(x.astype(np.complex128), direction, plan)), ftype, n)
+
+
+# 1701 = 9 9 7 3 has two row-kernel forms: up to 2048 transforms a pass the
+# wide one (one radix-7 butterfly per thread, 256 threads a row), above that
+# the default (one radix-9 butterfly per thread, 192 threads).
+@pytest.mark.parametrize("batch,double,threads", [(5, False, 256), (2048, False, 256), (2049, False, 192),
+                                                  (3, True, 256), (3000, True, 192)])
+def test_1701_row_forms(ffb, torch_cuda, batch, double, threads):
+    n = 1701
+    ftype = O.Z2Z if double else O.C2C
+    x = O.random_complex(n * batch, O.accuracy_seed(ftype, n, batch), double).reshape(batch, n)
+    with ffb.plan1d(n, ffb.Z2Z if double else ffb.C2C, batch) as p:
+        assert f"threads={threads} " in p.description(), p.description()
+    for direction in (-1, 1):
+        got = _run_c2c(ffb, torch_cuda, x, direction, double)
+        _check(O.error_stats(got, O.c2c(x.astype(np.complex128), direction)), ftype, n)

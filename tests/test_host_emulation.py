@@ -149,6 +149,21 @@ def test_bluestein_pair(monkeypatch, n, batch, double):
         assert _rel(got, ref) < _bound(n, double), (direction, _rel(got, ref))
 
 
+# 1701's two row-kernel forms: 256 threads a row up to 2048 transforms a
+# pass (every radix-9 and radix-7 stage one round), 192 above.
+@pytest.mark.parametrize("double", [False, True])
+def test_1701_row_forms(double):
+    n, batch = 1701, 3
+    code = Z2Z if double else C2C
+    assert "threads=256 " in _describe(lambda: H.plan1d(n, code, batch))
+    assert "threads=192 " in _describe(lambda: H.plan1d(n, code, 2049))
+    x = O.random_complex(n * batch, O.accuracy_seed(code, n, batch), double=True).reshape(batch, n)
+    for direction in (-1, 1):
+        got = H.c2c(x, direction, double)
+        ref = np.stack([O.c2c(r, direction) for r in x])
+        assert _rel(got, ref) < _bound(n, double), (direction, _rel(got, ref))
+
+
 def test_server_multi_pass_lengths():
     """Server templates lower their four-step and Bluestein-chain passes in
     the persistent kernel's form (no strided tile / TMA column kernels):
