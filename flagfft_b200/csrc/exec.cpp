@@ -277,9 +277,10 @@ thread_local bool t_no_one_pass = false;
 // plan time): the N1 convolution rows split over a two-CTA cluster, in both
 // precisions, instead of one CTA (single precision) or the three-pass chain
 // (double precision).  Off by default: on B200 it measured slower at the
-// benchmark lengths (C2C 10007 x 1024: 208.8 us against 176.7 us for one CTA;
-// Z2Z 10007 x 256: 123.2 us against 102 us for three passes) -- a pair CTA
-// runs 12 warps, and its row phase is no more efficient than the chain's.
+// benchmark lengths (C2C 10007 x 1024: 208.8 us against 176.7 us for one CTA,
+// both before the product-form column twiddles they share; Z2Z 10007 x 256:
+// 123.2 us against 102 us for three passes) -- a pair CTA runs 12 warps, and
+// its row phase is no more efficient than the chain's.
 bool bluestein_pair() {
   const char *v = std::getenv("FLAGFFT_BLUESTEIN_PAIR");
   return v && v[0] == '1';
