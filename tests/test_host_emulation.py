@@ -180,6 +180,21 @@ def test_server_multi_pass_lengths():
         assert _rel(y, ref) < _bound(n, code == Z2Z), (code, n, _rel(y, ref))
 
 
+def test_server_1701_wide_items():
+    """1701 requests (their wide 256-thread form) in one persistent launch
+    with lengths of other thread counts, both precisions and directions."""
+    reqs = []
+    for code, n, b, d, seed in [(C2C, 1701, 3, -1, 41), (C2C, 4096, 2, 1, 42), (Z2Z, 1701, 2, 1, 43),
+                                (C2C, 1009, 1, -1, 44), (Z2Z, 1701, 1, -1, 45)]:
+        dbl = code == Z2Z
+        x = O.random_complex(n * b, seed, double=True).reshape(b, n).astype(np.complex128 if dbl else np.complex64)
+        reqs.append((code, n, b, d, x))
+    outs = _server_run(reqs)
+    for (code, n, b, d, x), y in zip(reqs, outs):
+        ref = np.stack([O.c2c(r.astype(np.complex128), d) for r in x])
+        assert _rel(y, ref) < _bound(n, code == Z2Z), (code, n, _rel(y, ref))
+
+
 def test_server_real_on_chip_items():
     """Real requests whose transform fits one CTA: the persistent launch runs
     their pack / Hermitian post (R2C) and pre / unpack (C2R) tiles."""
